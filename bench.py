@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Throughput of the Stable Cosserat Rods substep on B200: vertex-substeps/s.
+
+Workload (config 2): RopeBatch.from_positions with 4096 ropes x 64 vertices per GPU (seg 0.02 m,
+straight down + N(0, 1e-3) m jitter, vertex 0 pinned), density 0.117 kg/m, EA 11473 N,
+EI 4.48e-3 N m^2, h = 1/6000 s, 8 iterations, 100 substeps per 1/60 s control frame, plane
+z = 0 (radius 6.35 mm), roots on the second-order program: p0 in a 1 m cube (z in [1.4, 2.4]),
+v0 ~ N(0, 0.5) m/s, p1 = p0 + N(0, 0.05) m. Damping 0 and drag 0.2 /s set explicitly.
+One step = one control frame (one persistent kernel launch). Synthetic seeded inputs.
+
+  value   device time of the K timed frames (CUDA events on the solver stream, inputs already
+          resident; L2 flushed between frames outside the events), max over ranks
+  e2e     the same frames through the public API with host buffers: every step copies its
+          root program from pinned host memory and reads the resulting positions back
+  --impl reference: the CPU restatement of the reference's algorithm (the reference itself
+          does not build here: GLM is absent) timed on all host cores, bounded sample.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cosserat-rod-solver-cuda_b200")
+for p in (PKG, os.path.join(ROOT, "tests")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "vertex-substeps/s"
+N_ROPES, V, S, ITERS, DT = 4096, 64, 100, 8, 1.0 / 60.0
+H = 1.0 / 6000.0
+
+
+def c2_inputs(n_ropes, frames, seed):
+    import scenarios as Sc
+
+    pos, roots = Sc.c2_positions(n_ropes, V, seed)
+    rng = np.random.default_rng(seed + 1000)
+    p0 = np.empty((frames, n_ropes, 3), np.float32)
+    v0 = rng.normal(0, 0.5, (frames, n_ropes, 3)).astype(np.float32)
+    p1 = np.empty_like(p0)
+    cur = roots.copy()
+    for f in range(frames):
+        p0[f] = cur
+        p1[f] = (cur + rng.normal(0, 0.05, (n_ropes, 3))).astype(np.float32)
+        cur = p1[f]
+    return pos, p0, v0, p1
+
+
+def configure(b):
+    b.set_gravity(np.array([0, 0, -9.81], np.float32))
+    b.damping = 0.0
+    b.drag = 0.2
+    b.set_planes(np.array([[0, 0, 1, 0]], np.float32), radius=0.00635)
+
+
+def read_flops():
+    path = os.path.join(ROOT, "profiles", "flop_count_config2.txt")
+    for line in open(path):
+        if line.startswith("flops_per_vertex_substep:"):
+            return float(line.split(":")[1])
+    raise RuntimeError("flops_per_vertex_substep missing in " + path)
+
+
+def read_traffic():
+    path = os.path.join(ROOT, "profiles", "frame_kernel_config2.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return json.load(open(path)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.dev)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_leg(seconds_target=15.0, threads=None):
+    """The CPU restatement (FP32 instantiation of the oracle) on all host cores: bounded sample
+    of the config-2 workload, ropes split over threads (ropes are independent)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ropesim_oracle
+
+    threads = threads or os.cpu_count() or 1
+
+    def run(n_ropes, frames):
+        pos, p0, v0, p1 = c2_inputs(n_ropes, frames, 7)
+        chunks = np.array_split(np.arange(n_ropes), threads)
+        sims = []
+        for c in chunks:
+            if len(c) == 0:
+                continue
+            b = ropesim_oracle.RopeBatch.from_positions(pos[c], 0.117, 11473.0, 4.48e-3, H, ITERS, precision="f32")
+            configure(b)
+            sims.append((b, c))
+        t0 = time.perf_counter()
+
+        def work(b, c):
+            for f in range(frames):
+                b.step(p0[f][c], v0[f][c], DT, S, root_pos_end=p1[f][c])
+
+        ts = [threading.Thread(target=work, args=bc) for bc in sims]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return time.perf_counter() - t0
+
+    probe_ropes = threads
+    t = run(probe_ropes, 1)
+    per = t / (probe_ropes * V * S)
+    n_ropes = int(max(threads, min(N_ROPES, seconds_target / max(per, 1e-12) / (V * S) / 2)))
+    frames = 2
+    t = run(n_ropes, frames)
+    value = n_ropes * V * S * frames / t
+    return {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{n_ropes} of the {N_ROPES} config-2 ropes x {frames} frames x {S} substeps "
+                      f"(FP32 CPU restatement, {threads} threads, {t:.1f} s)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ropesim_oracle
+
+    threads = os.cpu_count() or 1
+    n_ropes = max(threads, int(os.environ.get("RS_REF_ROPES", str(8 * threads))))
+    pos, p0, v0, p1 = c2_inputs(n_ropes, args.warmup + args.steps, 11)
+    chunks = [c for c in np.array_split(np.arange(n_ropes), threads) if len(c)]
+    sims = []
+    for c in chunks:
+        b = ropesim_oracle.RopeBatch.from_positions(pos[c], 0.117, 11473.0, 4.48e-3, H, ITERS, precision="f32")
+        configure(b)
+        sims.append((b, c))
+
+    def frame(f):
+        def work(b, c):
+            b.step(p0[f][c], v0[f][c], DT, S, root_pos_end=p1[f][c])
+
+        ts = [threading.Thread(target=work, args=bc) for bc in sims]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+
+    for f in range(args.warmup):
+        frame(f)
+    t0 = time.perf_counter()
+    for f in range(args.warmup, args.warmup + args.steps):
+        frame(f)
+    el = time.perf_counter() - t0
+    value = n_ropes * V * S * args.steps / el
+    sample = (f"{n_ropes} of the {N_ROPES} config-2 ropes per step (64 verts, {S} substeps, {ITERS} itr), "
+              f"FP32 CPU restatement of the reference's algorithm on {threads} threads")
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config2-program-4096x64 (bounded CPU sample)", "ropes_per_step": n_ropes,
+                       "verts_per_rope": V, "substeps": S, "num_itr": ITERS},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference CUDA build unavailable (GLM headers absent); the reference arm is the oracle port"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    import ctypes
+
+    import ropesim
+
+    lib = ctypes.CDLL(os.path.join(PKG, "ropesim", "libropesim_b200.so"))
+    frames = args.warmup + args.steps
+    pos, p0, v0, p1 = c2_inputs(N_ROPES, frames, 1234 + rank)
+    b = ropesim.RopeBatch.from_positions(pos, 0.117, 11473.0, 4.48e-3, H, ITERS, deterministic=True)
+    configure(b)
+    b.set_timing(True)
+    dev = torch.device("cuda", local)
+    P0 = torch.as_tensor(p0, device=dev)
+    V0 = torch.as_tensor(v0, device=dev)
+    P1 = torch.as_tensor(p1, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    torch.cuda.synchronize()
+
+    # ---- device-timed leg: one persistent launch per frame
+    for f in range(args.warmup):
+        b.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    kernel_ms = []
+    frame_ms = []
+    stream = torch.cuda.ExternalStream(b.stream_ptr())
+    sampler = ClockSampler(local)
+    with sampler:
+        for f in range(args.warmup, frames):
+            flush.fill_(float(f))
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
+            e1.record(stream)
+            e1.synchronize()
+            frame_ms.append(e0.elapsed_time(e1))
+            kernel_ms.append(b.last_frame_ms())
+    torch.cuda.synchronize()
+    total_ms = float(sum(frame_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    vs_per_rank = N_ROPES * V * S * args.steps
+    value = world * vs_per_rank / (total_ms * 1e-3)
+
+    # ---- end-to-end leg: host inputs in, host positions out, through the public API
+    hp0 = torch.as_tensor(p0).pin_memory()
+    hv0 = torch.as_tensor(v0).pin_memory()
+    hp1 = torch.as_tensor(p1).pin_memory()
+    out = torch.empty((N_ROPES, V, 3), dtype=torch.float32).pin_memory()
+    view = torch.as_tensor(b.positions())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for f in range(args.warmup, frames):
+        a0 = hp0[f].to(dev, non_blocking=True)
+        a1 = hv0[f].to(dev, non_blocking=True)
+        a2 = hp1[f].to(dev, non_blocking=True)
+        b.step(a0, a1, DT, S, root_pos_end=a2)
+        out.copy_(view)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * vs_per_rank / e2e_s
+    h2d = 3 * N_ROPES * 3 * 4
+    d2h = N_ROPES * V * 3 * 4
+
+    if rank == 0:
+        peaks, source = measured_peaks()
+        tf = ctypes.c_double(0)
+        lib.rs_probe_fp32_peak(ctypes.byref(tf), None)
+        fp32_peak = tf.value
+        flops_vs = read_flops()
+        avg_kernel_ms = float(np.mean(kernel_ms))
+        flops_launch = flops_vs * N_ROPES * V * S
+        achieved = flops_launch / (avg_kernel_ms * 1e-3) / 1e12
+        state_bytes = N_ROPES * V * (6 * 16 + 4 * 16 + 40)  # state in (6 float4), out (4 float4), views
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 ropes and root programs)",
+            "config": {"workload": "config2-program-4096x64", "ropes_per_gpu": N_ROPES, "verts_per_rope": V,
+                       "substeps": S, "num_itr": ITERS, "h": H, "planes": 1, "l2": "flushed between frames (256 MB write)",
+                       "bins": list(b.layout()), "parallelism": f"replicas x{world} (ropes independent)"},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": read_traffic(),
+                         "peak_source": "measured FP32 FMA probe (rs_probe_fp32_peak) on this GPU",
+                         "flops_per_vertex_substep": flops_vs,
+                         "hbm_view": {"algorithmic_bytes_per_launch": state_bytes,
+                                      "achieved_gbs": state_bytes / (avg_kernel_ms * 1e-3) / 1e9,
+                                      "peak_gbs": peaks.get("hbm_gbs"), "peak_source": source}},
+            "kernel_ms_per_frame": avg_kernel_ms,
+            "clocks": sampler.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_leg()
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+"""Build the engine in-tree.
+
+1. libropesim_b200.so: the sm_100a kernels, the C++ driver and the extern "C" boundary
+   (include/ropesim_b200.h), compiled by nvcc for `-gencode arch=compute_100a,code=sm_100a`
+   only, IEEE division / square root (no fast math), static CUDA runtime.
+2. ropesim/_ropesim*.so: the pybind11 module (RopeSim, RopeBatch, CudaView) linked against (1)
+   with an $ORIGIN rpath, so the package directory is self-contained.
+
+Usage: python cosserat-rod-solver-cuda_b200/build.py [--force] [-v]
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+import sysconfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+PKG = os.path.join(HERE, "ropesim")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CU_SOURCES = ["rs_frame.cu"]
+CPP_SOURCES = ["rs_batch.cpp", "rs_capi.cpp"]
+HEADERS = ["rs_types.h", "rs_device.cuh", "rs_kernels.h", "rs_batch.h"]
+
+
+def lib_path() -> str:
+    return os.path.join(PKG, "libropesim_b200.so")
+
+
+def ext_path() -> str:
+    return os.path.join(PKG, "_ropesim" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
+def _nvcc() -> str:
+    cand = [os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"]
+    for c in cand:
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found: the engine needs the CUDA toolkit to build")
+
+
+def _stale(out: str, deps) -> bool:
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    nvcc = _nvcc()
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "ropesim_b200.h")]
+    common = ["-std=c++17", "-O3", "-I", CSRC, "-I", INCLUDE, "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off"]
+    objs = []
+    for src in CU_SOURCES + CPP_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(objdir, src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            extra = ARCH + ["-lineinfo", "-Xptxas", "-v"] if src.endswith(".cu") else ARCH
+            cmd = [nvcc] + common + extra + ["-c", s, "-o", o]
+            if src.endswith(".cu") and not verbose:
+                cmd.remove("-Xptxas"); cmd.remove("-v")
+            _run(cmd, verbose)
+    lib = lib_path()
+    if force or _stale(lib, objs):
+        _run([nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", lib + ".tmp"] + objs, verbose)
+        os.replace(lib + ".tmp", lib)
+
+    import pybind11
+
+    ext = ext_path()
+    src = os.path.join(CSRC, "rs_pybind.cpp")
+    if force or _stale(ext, [src, lib, os.path.join(INCLUDE, "ropesim_b200.h")]):
+        cxx = os.environ.get("CXX", "g++")
+        cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
+               "-I", sysconfig.get_paths()["include"], "-I", pybind11.get_include(), "-I", INCLUDE,
+               src, "-o", ext + ".tmp", "-L", PKG, "-lropesim_b200", "-Wl,-rpath,$ORIGIN"]
+        _run(cmd, verbose)
+        os.replace(ext + ".tmp", ext)
+    return ext
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

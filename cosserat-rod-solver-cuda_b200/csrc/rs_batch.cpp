@@ -1,0 +1,723 @@
+// rs_batch.cpp -- host driver: setup, packing, staging, mesh pose machine, frame launch.
+#include "rs_batch.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+
+#include "rs_kernels.h"
+
+namespace rs {
+
+namespace {
+
+// Single-precision rotor helpers for the host setup. The setup follows YarnBall.cu:112-259
+// operation by operation (same order, IEEE float, no contraction) so that initial frames and
+// rest rotations are the reference's.
+V4 qmul(const V4& a, const V4& b) {
+    // (a.w b.v + b.w a.v + a.v x b.v, a.w b.w - a.v . b.v), Rotor.h:185-188
+    const float cx = a.y * b.z - a.z * b.y, cy = a.z * b.x - a.x * b.z, cz = a.x * b.y - a.y * b.x;
+    V4 r;
+    r.x = (a.w * b.x + b.w * a.x) + cx;
+    r.y = (a.w * b.y + b.w * a.y) + cy;
+    r.z = (a.w * b.z + b.w * a.z) + cz;
+    r.w = a.w * b.w - ((a.x * b.x + a.y * b.y) + a.z * b.z);
+    return r;
+}
+V4 qconj(const V4& a) { return V4{-a.x, -a.y, -a.z, a.w}; }
+float dot4(const V4& a, const V4& b) { return (a.x * b.x + a.y * b.y) + (a.z * b.z + a.w * b.w); }
+V4 scale4(const V4& a, float s) { return V4{a.x * s, a.y * s, a.z * s, a.w * s}; }
+V4 normalize4(const V4& a) { return scale4(a, 1.f / std::sqrt(dot4(a, a))); }
+
+int next_pow2(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+}  // namespace
+
+void Batch::check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw cuda_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+Batch::Batch(int num_ropes, const int* rope_verts, const float* positions, const uint8_t* pinned, float density,
+             float k_stretch, float k_bend, float max_h_in, int num_itr_in, bool fix_root_orientation,
+             bool straight_rest, float dead_radius, float dead_barrier) {
+    if (num_ropes < 1) throw std::invalid_argument("num_ropes must be >= 1");
+    R_ = num_ropes;
+    ustart_.assign(R_ + 1, 0);
+    for (int r = 0; r < R_; r++) {
+        if (rope_verts[r] < 3) throw std::invalid_argument("every rope needs >= 3 vertices");
+        if (rope_verts[r] > 1024) throw std::invalid_argument("ropes longer than 1024 vertices are not supported");
+        ustart_[r + 1] = ustart_[r] + rope_verts[r];
+        if (rope_verts[r] != rope_verts[0]) uniform_ = false;
+    }
+    n_ = ustart_[R_];
+    im_.assign(n_, 1.f); lr_.assign(n_, 1.f); ks_.assign(n_, 100.f); fl_.assign(n_, F_NEXT);
+    qrest_.assign(n_, V4{0.f, 0.f, 0.f, 5.f});
+    pos_.assign(n_, V4{0, 0, 0, 0}); vel_.assign(n_, V4{0, 0, 0, 0}); lvel_.assign(n_, V4{0, 0, 0, 0});
+    q_.assign(n_, V4{0, 0, 0, 1});
+    for (int i = 0; i < n_; i++) pos_[i] = V4{positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], 0.f};
+    fl_[n_ - 1] = 0;
+    // RopeBatch ctor, batch.cu:344-361
+    for (int r = 0; r < R_; r++) {
+        fl_[ustart_[r + 1] - 1] = 0;
+        for (int i = ustart_[r]; i < ustart_[r + 1]; i++)
+            if (pinned ? pinned[i] != 0 : i == ustart_[r]) im_[i] = 0.f;
+        if (fix_root_orientation) fl_[ustart_[r]] |= F_FIX_ORIENT;
+    }
+    configure(density);
+    // dead collision radii gate the segment-length check of uploadMeta (YarnBall.cu:268)
+    if (2.f * min_seg_ < 2.f * dead_radius + dead_barrier)
+        throw std::invalid_argument("Use thinner yarn or use longer segments (2 * min segment >= 2 * radius + barrier)");
+    if (straight_rest)
+        for (int r = 0; r < R_; r++)
+            for (int i = ustart_[r]; i + 1 < ustart_[r + 1]; i++) qrest_[i] = V4{0.f, 0.f, 0.f, 1.f};
+    for (int i = 0; i < n_; i++) ks_[i] = k_stretch * lr_[i];       // setKStretch
+    const float kb4 = k_bend * 4.f;                                   // setKBend
+    for (int i = 0; i < n_; i++) qrest_[i] = scale4(normalize4(qrest_[i]), kb4 / lr_[i]);
+    for (int r = 0; r < R_; r++) fl_[ustart_[r]] |= F_ROOT;
+    max_h = max_h_in;
+    h_ = max_h_in;   // seed lastH like a fresh sim (bindings.cpp:249-253)
+    num_itr = num_itr_in;
+    init_pos_ = pos_;
+    init_q_ = q_;
+
+    check(cudaStreamCreate(&stream_), "cudaStreamCreate");
+    check(cudaEventCreate(&ev0_), "cudaEventCreate");
+    check(cudaEventCreate(&ev1_), "cudaEventCreate");
+    host_dyn_valid_ = true;
+    device_valid_ = false;
+    layout_valid_ = false;
+    ensure_device();
+    gather();   // views are valid before the first step (batch.cu:411)
+    check(cudaStreamSynchronize(stream_), "construct");
+}
+
+Batch::~Batch() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (auto& g : grids_) cudaFree(const_cast<float*>(g.v));
+    void* bufs[] = {d_bins_, d_ropes_, d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, d_qrest_, d_init_pos_, d_init_q_,
+                    d_out_pos_, d_out_vel_, d_out_q_, d_prog_, d_status_, d_ranges_, d_boxes_, d_cur_, d_tgt_,
+                    d_tele_, d_motion_, d_poses_, d_stage_, d_stage_tele_, d_force_, d_wrench_};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    if (h_prog_) cudaFreeHost(h_prog_);
+    if (h_status_) cudaFreeHost(h_status_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+// Sim::configure, YarnBall.cu:112-182. Frames are transported along the whole caller-order
+// array, so each rope's initial frames continue from the previous rope's last frame.
+void Batch::configure(float density) {
+    max_seg_ = 0.f;
+    min_seg_ = std::numeric_limits<float>::max();
+    V4 lastQ{0.f, 0.f, 0.f, 1.f};
+    for (int i = 0; i < n_; i++) {
+        if (i < n_ - 1) {
+            const bool hasNext = fl_[i] & F_NEXT;
+            fl_[i + 1] = hasNext ? (fl_[i + 1] | F_PREV) : (fl_[i + 1] & ~F_PREV);
+            const bool hasNextNext = hasNext && (fl_[i + 1] & F_NEXT);
+            fl_[i] = hasNextNext ? (fl_[i] | F_NEXT_ORIENT) : (fl_[i] & ~F_NEXT_ORIENT);
+            if (!hasNext) fl_[i] |= F_FIX_ORIENT;
+        }
+        if (!(fl_[i] & F_PREV) && !(fl_[i] & F_NEXT))
+            throw std::invalid_argument("Dangling segment. Yarns must be atleast 2 segments long");
+        lr_[i] = 1.f / (float)n_;
+        float mass = 0.f;
+        if (fl_[i] & F_PREV) mass += lr_[i - 1];
+        if (fl_[i] & F_NEXT) {
+            const float sx = pos_[i + 1].x - pos_[i].x, sy = pos_[i + 1].y - pos_[i].y, sz = pos_[i + 1].z - pos_[i].z;
+            const float d2 = (sx * sx + sy * sy) + sz * sz;
+            lr_[i] = std::sqrt(d2);
+            if (lr_[i] == 0.f || !std::isfinite(lr_[i])) throw std::invalid_argument("0 length segment");
+            const float inv = 1.f / std::sqrt(d2);
+            const float dx = sx * inv, dy = sy * inv, dz = sz * inv;
+            V4 qq;
+            if (dx < -0.999999f) {
+                qq = V4{0.f, 0.f, 1.f, 0.f};
+            } else {  // Rotor::fromTo(e1, d), Rotor.h:57-64
+                float hx = (1.f + dx) * 0.5f, hy = (0.f + dy) * 0.5f, hz = (0.f + dz) * 0.5f;
+                const float l = (hx * hx + hy * hy) + hz * hz;
+                if (l > 0.f) {
+                    const float s = 1.f / std::sqrt(l);
+                    hx *= s; hy *= s; hz *= s;
+                } else {
+                    hx = 0.f; hy = 1.f; hz = 0.f;
+                }
+                // cross(e1, h), dot(e1, h)
+                qq = V4{0.f * hz - 0.f * hy, 0.f * hx - 1.f * hz, 1.f * hy - 0.f * hx, (1.f * hx + 0.f * hy) + 0.f * hz};
+            }
+            V4 t = qmul(qconj(qq), lastQ);
+            const V4 tw{t.x, 0.f, 0.f, t.w};
+            t = (dot4(tw, tw) > 1e-12f) ? normalize4(tw) : V4{0.f, 0.f, 0.f, 1.f};
+            lastQ = qmul(qq, t);
+            mass += lr_[i];
+            max_seg_ = std::max(max_seg_, lr_[i]);
+            min_seg_ = std::min(min_seg_, lr_[i]);
+        }
+        q_[i] = lastQ;
+        mass *= 0.5f * density;
+        im_[i] = (mass != 0.f) ? im_[i] * (1.f / mass) : 0.f;
+    }
+    for (int i = 0; i < n_ - 1; i++) qrest_[i] = scale4(qmul(qconj(q_[i]), q_[i + 1]), std::sqrt(dot4(qrest_[i], qrest_[i])));
+}
+
+bool Batch::roots_pinned() const {
+    for (int r = 0; r < R_; r++)
+        if (im_[ustart_[r]] != 0.f) return false;
+    return true;
+}
+
+int Batch::pose_cache_entries() const { return std::max(1, max_rcount_ * (int)grids_.size()); }
+
+// Whole ropes into bins of `block_` threads: first-fit decreasing by length; a bin also
+// holds at most max_ropes_per_bin_ ropes (bounded by the per-CTA mesh pose cache).
+void Batch::pack() {
+    int maxV = 0;
+    for (int r = 0; r < R_; r++) maxV = std::max(maxV, rope_verts(r));
+    int blk = block_override;
+    if (blk == 0) {
+        blk = std::max(64, next_pow2(maxV));
+        if (blk < 256 && (long long)n_ > 148LL * blk) blk = 256;
+    }
+    if (blk < maxV) blk = next_pow2(maxV);
+    if (blk > 1024) throw std::invalid_argument("rope longer than the largest CTA (1024)");
+    block_ = blk;
+    const int M = (int)grids_.size();
+    int cap = max_ropes_per_bin_;
+    if (M > 0) cap = std::min(cap, std::max(1, (96 * 1024) / (2 * M * (int)sizeof(Pose))));
+    std::vector<int> order(R_);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rope_verts(a) > rope_verts(b); });
+    struct Open { int used, rc; std::vector<int> ropes; };
+    std::vector<Open> open;
+    int first_open = 0;
+    for (int r : order) {
+        const int L = rope_verts(r);
+        int b = -1;
+        for (int k = first_open; k < (int)open.size(); k++)
+            if (open[k].used + L <= blk && open[k].rc < cap) { b = k; break; }
+        if (b < 0) { open.push_back(Open{0, 0, {}}); b = (int)open.size() - 1; }
+        open[b].used += L;
+        open[b].rc++;
+        open[b].ropes.push_back(r);
+        while (first_open < (int)open.size() && (open[first_open].used + 3 > blk || open[first_open].rc >= cap)) first_open++;
+    }
+    bins_.clear();
+    dropes_.clear();
+    u2d_.assign(n_, 0);
+    int dv = 0;
+    max_rcount_ = 1;
+    for (auto& o : open) {
+        Bin b{dv, 0, (int)dropes_.size(), (int)o.ropes.size()};
+        for (int r : o.ropes) {
+            Rope rp{dv, rope_verts(r), ustart_[r], r};
+            for (int i = 0; i < rp.count; i++) u2d_[rp.ustart + i] = dv + i;
+            dv += rp.count;
+            dropes_.push_back(rp);
+        }
+        b.vcount = dv - b.vstart;
+        bins_.push_back(b);
+        max_rcount_ = std::max(max_rcount_, b.rcount);
+    }
+}
+
+void Batch::alloc_device() {
+    auto alloc = [&](void** p, size_t bytes, const char* what) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        check(cudaMalloc(p, bytes), what);
+    };
+    alloc((void**)&d_bins_, sizeof(Bin) * bins_.size(), "cudaMalloc(bins)");
+    alloc((void**)&d_ropes_, sizeof(Rope) * dropes_.size(), "cudaMalloc(ropes)");
+    if (!d_pos_) {
+        const size_t n4 = sizeof(float4) * n_;
+        alloc((void**)&d_topo_, sizeof(int4) * n_, "cudaMalloc(topo)");
+        alloc((void**)&d_pos_, n4, "cudaMalloc(pos)");
+        alloc((void**)&d_vel_, n4, "cudaMalloc(vel)");
+        alloc((void**)&d_lvel_, n4, "cudaMalloc(lvel)");
+        alloc((void**)&d_q_, n4, "cudaMalloc(q)");
+        alloc((void**)&d_qrest_, n4, "cudaMalloc(qrest)");
+        alloc((void**)&d_init_pos_, n4, "cudaMalloc(init pos)");
+        alloc((void**)&d_init_q_, n4, "cudaMalloc(init q)");
+        alloc((void**)&d_out_pos_, sizeof(float) * 3 * n_, "cudaMalloc(view pos)");
+        alloc((void**)&d_out_vel_, sizeof(float) * 3 * n_, "cudaMalloc(view vel)");
+        alloc((void**)&d_out_q_, sizeof(float) * 4 * n_, "cudaMalloc(view quat)");
+        alloc((void**)&d_prog_, sizeof(float) * 17 * R_, "cudaMalloc(program)");
+        alloc((void**)&d_status_, sizeof(int) * 4, "cudaMalloc(status)");
+        alloc((void**)&d_ranges_, sizeof(int2) * R_, "cudaMalloc(reset ranges)");
+        check(cudaMemset(d_status_, 0, sizeof(int) * 4), "memset(status)");
+        check(cudaMemset(d_prog_, 0, sizeof(float) * 17 * R_), "memset(program)");
+        check(cudaMallocHost((void**)&h_prog_, sizeof(float) * 17 * R_), "cudaMallocHost(program)");
+        check(cudaMallocHost((void**)&h_status_, sizeof(int) * 4), "cudaMallocHost(status)");
+        const size_t slots = (size_t)R_ * kMaxSdf;
+        alloc((void**)&d_boxes_, sizeof(float) * 6 * kMaxSdf, "cudaMalloc(sdf boxes)");
+        alloc((void**)&d_cur_, sizeof(Pose7) * slots, "cudaMalloc(sdf cur)");
+        alloc((void**)&d_tgt_, sizeof(Pose7) * slots, "cudaMalloc(sdf tgt)");
+        alloc((void**)&d_tele_, slots, "cudaMalloc(sdf tele)");
+        alloc((void**)&d_motion_, sizeof(Motion) * slots, "cudaMalloc(sdf motion)");
+        alloc((void**)&d_poses_, sizeof(Pose) * slots, "cudaMalloc(sdf poses)");
+        alloc((void**)&d_stage_, sizeof(float) * 7 * slots, "cudaMalloc(sdf stage)");
+        alloc((void**)&d_stage_tele_, R_, "cudaMalloc(sdf stage flags)");
+        std::vector<Pose7> ident(slots, Pose7{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f});
+        check(cudaMemcpy(d_cur_, ident.data(), sizeof(Pose7) * slots, cudaMemcpyHostToDevice), "upload(sdf cur)");
+        check(cudaMemcpy(d_tgt_, ident.data(), sizeof(Pose7) * slots, cudaMemcpyHostToDevice), "upload(sdf tgt)");
+        check(cudaMemset(d_tele_, 0, slots), "memset(sdf tele)");
+        check(cudaMemset(d_poses_, 0, sizeof(Pose) * slots), "memset(sdf poses)");
+        check(cudaMemset(d_motion_, 0, sizeof(Motion) * slots), "memset(sdf motion)");
+        check(cudaMemset(d_boxes_, 0, sizeof(float) * 6 * kMaxSdf), "memset(sdf boxes)");
+    }
+}
+
+void Batch::ensure_device() {
+    if (!layout_valid_) {
+        ensure_host();
+        pack();
+        alloc_device();
+        std::vector<int4> topo(n_);
+        std::vector<float4> ip(n_), iq(n_);
+        for (const Bin& b : bins_)
+            for (int r = b.rstart; r < b.rstart + b.rcount; r++) {
+                const Rope& rp = dropes_[r];
+                for (int i = 0; i < rp.count; i++) {
+                    const int u = rp.ustart + i, d = rp.dstart + i;
+                    topo[d] = make_int4((int)fl_[u], r - b.rstart, u, rp.user);
+                    ip[d] = make_float4(init_pos_[u].x, init_pos_[u].y, init_pos_[u].z, 0.f);
+                    iq[d] = make_float4(init_q_[u].x, init_q_[u].y, init_q_[u].z, init_q_[u].w);
+                }
+            }
+        check(cudaMemcpy(d_bins_, bins_.data(), sizeof(Bin) * bins_.size(), cudaMemcpyHostToDevice), "upload(bins)");
+        check(cudaMemcpy(d_ropes_, dropes_.data(), sizeof(Rope) * dropes_.size(), cudaMemcpyHostToDevice), "upload(ropes)");
+        check(cudaMemcpy(d_topo_, topo.data(), sizeof(int4) * n_, cudaMemcpyHostToDevice), "upload(topo)");
+        check(cudaMemcpy(d_init_pos_, ip.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(init pos)");
+        check(cudaMemcpy(d_init_q_, iq.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(init q)");
+        layout_valid_ = true;
+        device_valid_ = false;
+    }
+    if (!device_valid_) {
+        std::vector<float4> P(n_), Vv(n_), L(n_), Q(n_), QR(n_);
+        std::vector<int4> topo(n_);
+        for (int u = 0; u < n_; u++) {
+            const int d = u2d_[u];
+            P[d] = make_float4(pos_[u].x, pos_[u].y, pos_[u].z, im_[u]);
+            Vv[d] = make_float4(vel_[u].x, vel_[u].y, vel_[u].z, lr_[u]);
+            L[d] = make_float4(lvel_[u].x, lvel_[u].y, lvel_[u].z, ks_[u]);
+            Q[d] = make_float4(q_[u].x, q_[u].y, q_[u].z, q_[u].w);
+            QR[d] = make_float4(qrest_[u].x, qrest_[u].y, qrest_[u].z, qrest_[u].w);
+        }
+        for (const Bin& b : bins_)
+            for (int r = b.rstart; r < b.rstart + b.rcount; r++) {
+                const Rope& rp = dropes_[r];
+                for (int i = 0; i < rp.count; i++) topo[rp.dstart + i] = make_int4((int)fl_[rp.ustart + i], r - b.rstart, rp.ustart + i, rp.user);
+            }
+        check(cudaMemcpy(d_topo_, topo.data(), sizeof(int4) * n_, cudaMemcpyHostToDevice), "upload(topo)");
+        check(cudaMemcpy(d_pos_, P.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(pos)");
+        check(cudaMemcpy(d_vel_, Vv.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(vel)");
+        check(cudaMemcpy(d_lvel_, L.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(lvel)");
+        check(cudaMemcpy(d_q_, Q.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(q)");
+        check(cudaMemcpy(d_qrest_, QR.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(qrest)");
+        device_valid_ = true;
+    }
+}
+
+void Batch::ensure_host() {
+    if (host_dyn_valid_) return;
+    std::vector<float4> P(n_), Vv(n_), L(n_), Q(n_);
+    check(cudaStreamSynchronize(stream_), "sync");
+    check(cudaMemcpy(P.data(), d_pos_, sizeof(float4) * n_, cudaMemcpyDeviceToHost), "download(pos)");
+    check(cudaMemcpy(Vv.data(), d_vel_, sizeof(float4) * n_, cudaMemcpyDeviceToHost), "download(vel)");
+    check(cudaMemcpy(L.data(), d_lvel_, sizeof(float4) * n_, cudaMemcpyDeviceToHost), "download(lvel)");
+    check(cudaMemcpy(Q.data(), d_q_, sizeof(float4) * n_, cudaMemcpyDeviceToHost), "download(q)");
+    for (int u = 0; u < n_; u++) {
+        const int d = u2d_[u];
+        pos_[u] = V4{P[d].x, P[d].y, P[d].z, 0.f};
+        vel_[u] = V4{Vv[d].x, Vv[d].y, Vv[d].z, 0.f};
+        lvel_[u] = V4{L[d].x, L[d].y, L[d].z, 0.f};
+        q_[u] = V4{Q[d].x, Q[d].y, Q[d].z, Q[d].w};
+    }
+    host_dyn_valid_ = true;
+}
+
+// ------------------------------------------------------------------ host edits
+void Batch::set_vertex_inv_mass(int u, float im) {
+    ensure_host();
+    if (im_[u] != 0.f) im_[u] = im;
+    device_valid_ = false;
+}
+void Batch::set_vertex_ea(int u, float ea) {
+    ensure_host();
+    ks_[u] = ea * lr_[u];
+    device_valid_ = false;
+}
+void Batch::set_vertex_ei(int u, float ei) {
+    ensure_host();
+    const float k = 4.f * ei / lr_[u];
+    qrest_[u] = scale4(normalize4(qrest_[u]), k);
+    device_valid_ = false;
+}
+void Batch::set_root_host(int rope, const float* p, const float* v, const float* q) {
+    ensure_host();
+    const int u = ustart_[rope];
+    pos_[u] = V4{p[0], p[1], p[2], 0.f};
+    vel_[u] = V4{v[0], v[1], v[2], 0.f};
+    if (q) q_[u] = V4{q[0], q[1], q[2], q[3]};
+    device_valid_ = false;
+}
+void Batch::set_velocities_host(const float* v) {
+    ensure_host();
+    for (int u = 0; u < n_; u++) vel_[u] = V4{v[3 * u], v[3 * u + 1], v[3 * u + 2], 0.f};
+    device_valid_ = false;
+}
+void Batch::unpin_root(int rope) {
+    ensure_host();
+    const int u = ustart_[rope];
+    im_[u] = 2.f * im_[u + 1];
+    vel_[u] = V4{0.f, 0.f, 0.f, 0.f};
+    device_valid_ = false;
+}
+void Batch::reset_all() {
+    ensure_host();
+    for (int u = 0; u < n_; u++) {
+        pos_[u] = init_pos_[u];
+        q_[u] = init_q_[u];
+        vel_[u] = V4{0.f, 0.f, 0.f, 0.f};
+        lvel_[u] = V4{0.f, 0.f, 0.f, 0.f};
+    }
+    time_ = 0.f;
+    h_ = max_h;
+    last_error_ = last_warning_ = 0;
+    device_valid_ = false;
+    ensure_device();
+    gather();
+}
+void Batch::reset_ropes(const int* ids, int count) {
+    if (count <= 0) return;
+    ensure_device();
+    std::vector<int2> rg(count);
+    int maxv = 0;
+    for (int c = 0; c < count; c++) {
+        const int u = ustart_[ids[c]];
+        rg[c] = make_int2(u2d_[u], rope_verts(ids[c]));
+        maxv = std::max(maxv, rg[c].y);
+    }
+    check(cudaMemcpyAsync(d_ranges_, rg.data(), sizeof(int2) * count, cudaMemcpyHostToDevice, stream_), "upload(reset ids)");
+    check(launch_reset(d_pos_, d_vel_, d_lvel_, d_q_, d_init_pos_, d_init_q_, d_ranges_, count, maxv, stream_), "reset");
+    host_dyn_valid_ = false;
+    gather();
+    check(cudaStreamSynchronize(stream_), "reset");
+}
+void Batch::gather() {
+    ensure_device();
+    FrameArgs a{};
+    a.topo = d_topo_; a.pos = d_pos_; a.vel = d_vel_; a.q = d_q_;
+    a.out_pos = d_out_pos_; a.out_vel = d_out_vel_; a.out_q = d_out_q_;
+    check(launch_gather(a, n_, stream_), "gather");
+}
+void Batch::download(float* p, float* v, float* q) {
+    ensure_host();
+    for (int u = 0; u < n_; u++) {
+        if (p) { p[3 * u] = pos_[u].x; p[3 * u + 1] = pos_[u].y; p[3 * u + 2] = pos_[u].z; }
+        if (v) { v[3 * u] = vel_[u].x; v[3 * u + 1] = vel_[u].y; v[3 * u + 2] = vel_[u].z; }
+        if (q) { q[4 * u] = q_[u].x; q[4 * u + 1] = q_[u].y; q[4 * u + 2] = q_[u].z; q[4 * u + 3] = q_[u].w; }
+    }
+}
+
+// ------------------------------------------------------------------ stepping
+// Root rows [R, 17] = (p0, v0, p1, q0, q1) staged into library memory before the launch
+// (batch.cu:327-346): callers may free their tensors as soon as the call returns.
+void Batch::stage_rows(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1, bool host) {
+    if (host) {
+        // the previous frame's upload from this pinned buffer must be done before reuse
+        check(cudaStreamSynchronize(stream_), "sync(program staging)");
+        for (int r = 0; r < R_; r++) {
+            float* row = h_prog_ + (size_t)r * 17;
+            for (int k = 0; k < 3; k++) {
+                row[k] = p0[3 * r + k];
+                row[3 + k] = v0[3 * r + k];
+                row[6 + k] = p1 ? p1[3 * r + k] : 0.f;
+            }
+            for (int k = 0; k < 4; k++) {
+                row[9 + k] = q0 ? q0[4 * r + k] : 0.f;
+                row[13 + k] = q1 ? q1[4 * r + k] : 0.f;
+            }
+        }
+        check(cudaMemcpyAsync(d_prog_, h_prog_, sizeof(float) * 17 * R_, cudaMemcpyHostToDevice, stream_), "upload(program)");
+        return;
+    }
+    const size_t rowb = 17 * sizeof(float);
+    check(cudaMemcpy2DAsync(d_prog_, rowb, p0, 3 * sizeof(float), 3 * sizeof(float), R_, cudaMemcpyDeviceToDevice, stream_), "stage p0");
+    check(cudaMemcpy2DAsync(d_prog_ + 3, rowb, v0, 3 * sizeof(float), 3 * sizeof(float), R_, cudaMemcpyDeviceToDevice, stream_), "stage v0");
+    if (p1) check(cudaMemcpy2DAsync(d_prog_ + 6, rowb, p1, 3 * sizeof(float), 3 * sizeof(float), R_, cudaMemcpyDeviceToDevice, stream_), "stage p1");
+    if (q0) check(cudaMemcpy2DAsync(d_prog_ + 9, rowb, q0, 4 * sizeof(float), 4 * sizeof(float), R_, cudaMemcpyDeviceToDevice, stream_), "stage q0");
+    if (q1) check(cudaMemcpy2DAsync(d_prog_ + 13, rowb, q1, 4 * sizeof(float), 4 * sizeof(float), R_, cudaMemcpyDeviceToDevice, stream_), "stage q1");
+}
+
+void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int steps, float h) {
+    // uploadMeta bookkeeping, batch.cu:57-62 / step.cpp:41-42
+    last_h_ = h_;
+    h_ = h;
+    FrameArgs a{};
+    a.bins = d_bins_; a.ropes = d_ropes_; a.topo = d_topo_;
+    a.pos = d_pos_; a.vel = d_vel_; a.lvel = d_lvel_; a.q = d_q_; a.qrest = d_qrest_;
+    a.out_pos = d_out_pos_; a.out_vel = d_out_vel_; a.out_q = d_out_q_;
+    a.out_force = d_force_; a.wrench = d_wrench_; a.status = d_status_;
+    a.prog = d_prog_; a.root_mode = root_mode; a.has_q0 = has_q0; a.has_q1 = has_q1;
+    a.h = h_; a.last_h = last_h_; a.dt = dt; a.substeps = steps; a.iters = num_itr;
+    a.gx = gravity[0]; a.gy = gravity[1]; a.gz = gravity[2];
+    a.damping = damping; a.drag = drag; a.drag_quad = drag_quad; a.drag_quad_t = drag_quad_t; a.accel = accel;
+    a.num_planes = num_planes_;
+    for (int p = 0; p < num_planes_; p++) a.planes[p] = make_float4(planes_[p][0], planes_[p][1], planes_[p][2], planes_[p][3]);
+    a.c_radius = c_radius_; a.c_kappa = c_kappa_; a.c_mu_s = c_mu_s_; a.c_mu_k = c_mu_k_; a.c_vslip = c_vslip_;
+    a.num_sdf = (int)grids_.size();
+    a.sdf_moving = sdf_moving_ ? 1 : 0;
+    a.forces_on = forces_on_ ? 1 : 0;
+    a.pose_cache = pose_cache_entries();
+    a.poses = d_poses_; a.motion = d_motion_;
+    for (int m = 0; m < (int)grids_.size(); m++) a.grids[m] = grids_[m];
+    if (timing_) check(cudaEventRecord(ev0_, stream_), "event");
+    check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
+    if (timing_) check(cudaEventRecord(ev1_, stream_), "event");
+    host_dyn_valid_ = false;
+}
+
+void Batch::sdf_begin() {
+    if (pending_set_) {
+        check(launch_stage_motion(d_cur_, d_tgt_, d_tele_, d_motion_, R_ * kMaxSdf, stream_), "stage motion");
+        sdf_moving_ = true;
+        moving_ = true;
+    } else {
+        sdf_moving_ = false;
+    }
+    if (forces_on_) {
+        check(cudaMemsetAsync(d_force_, 0, sizeof(float) * 3 * n_, stream_), "zero(contact forces)");
+        check(cudaMemsetAsync(d_wrench_, 0, sizeof(float) * 6 * (size_t)R_ * kMaxSdf, stream_), "zero(mesh wrenches)");
+    }
+}
+
+void Batch::sdf_end(int substeps) {
+    last_substeps_ = substeps > 0 ? substeps : 1;
+    if (moving_) {
+        check(launch_commit(d_cur_, d_tgt_, d_tele_, d_poses_, d_boxes_, (int)grids_.size(), -1, R_, stream_), "commit poses");
+        moving_ = false;
+        pending_set_ = false;
+    }
+    if (forces_on_)
+        check(launch_scale(d_wrench_, 6 * R_ * kMaxSdf, 1.f / (float)last_substeps_, stream_), "average wrenches");
+}
+
+void Batch::step_program(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1, float dt,
+                         int substeps, bool host_inputs) {
+    ensure_device();
+    stage_rows(p0, v0, p1, q0, q1, host_inputs);
+    sdf_begin();
+    run_frame(ROOT_PROGRAM, q0 != nullptr, q1 != nullptr, dt, substeps, dt / (float)substeps);
+    time_ += dt;
+    sdf_end(substeps);
+    if (sync_every_frame) {
+        check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
+        check(cudaStreamSynchronize(stream_), "frame");
+        if (h_status_[0] || h_status_[1] || h_status_[2]) {
+            if (h_status_[2]) nonfinite_ = 1;
+            if (h_status_[1]) last_warning_ = h_status_[1];
+            const int err = h_status_[0];
+            check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
+            if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
+        }
+    }
+    if (timing_) {
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed");
+        last_frame_ms_ = ms;
+    }
+}
+
+void Batch::step_legacy(const float* p, const float* v, const float* q, float dt, int substeps, bool host_inputs) {
+    ensure_device();
+    stage_rows(p, v, nullptr, q, nullptr, host_inputs);
+    sdf_begin();
+    // exactly `substeps` substeps through the biased max_h of batch.cu:444-452 (float ceil)
+    const float mh = (dt / (float)substeps) * 1.000001f;
+    int steps = (int)std::ceil(dt / mh);
+    if (steps < 1) steps = 1;
+    run_frame(ROOT_SET, q != nullptr, false, dt, steps, dt / (float)steps);
+    time_ += dt;
+    sdf_end(substeps);
+    if (sync_every_frame) {
+        check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
+        check(cudaStreamSynchronize(stream_), "frame");
+        if (h_status_[2]) { nonfinite_ = 1; check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status"); }
+    }
+    if (timing_) {
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed");
+        last_frame_ms_ = ms;
+    }
+}
+
+void Batch::step_free(float dt, int substeps) {
+    ensure_device();
+    sdf_begin();
+    run_frame(ROOT_NONE, false, false, dt, substeps, dt / (float)substeps);
+    time_ += dt;
+    sdf_end(substeps);
+    if (sync_every_frame) {
+        check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
+        check(cudaStreamSynchronize(stream_), "frame");
+        if (h_status_[2]) { nonfinite_ = 1; check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status"); }
+    }
+}
+
+// Sim::advance (step.cpp:37-57) with bindings.cpp:274-295's explicit-substep bias.
+void Batch::advance(float dt, int substeps) {
+    if (!(dt > 0.f)) return;
+    ensure_device();
+    sdf_begin();
+    const float mh = substeps > 0 ? (dt / (float)substeps) * 1.000001f : max_h;
+    int steps = (int)std::ceil(dt / mh);
+    if (steps < 1) steps = 1;
+    run_frame(ROOT_NONE, false, false, dt, steps, dt / (float)steps);
+    time_ += dt;
+    sdf_end(substeps > 0 ? substeps : steps);
+    if (sync_every_frame) {
+        check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
+        check(cudaStreamSynchronize(stream_), "frame");
+        if (h_status_[2]) { nonfinite_ = 1; check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status"); }
+    }
+}
+
+void Batch::set_block(int block) {
+    if (block == block_override) return;
+    ensure_host();
+    block_override = block;
+    layout_valid_ = false;
+    device_valid_ = false;
+    ensure_device();
+    gather();
+}
+
+// ------------------------------------------------------------------ contact
+void Batch::set_contact(float radius, float mu_s, float mu_k, float v_slip, float kappa) {
+    c_radius_ = radius; c_mu_s_ = mu_s; c_mu_k_ = mu_k; c_vslip_ = v_slip; c_kappa_ = kappa;
+}
+void Batch::set_planes(int count, const float* rows) {
+    for (int p = 0; p < count; p++)
+        for (int k = 0; k < 4; k++) planes_[p][k] = rows[4 * p + k];
+    num_planes_ = count;
+}
+
+int Batch::add_mesh(const float* values, int nx, int ny, int nz, const float* origin, float spacing, float mu_s,
+                    float mu_k, const float* pos, const float* quat, int rows) {
+    if ((int)grids_.size() >= kMaxSdf) throw std::invalid_argument("at most 64 meshes per sim");
+    ensure_device();
+    const size_t cnt = (size_t)nx * ny * nz;
+    float* d = nullptr;
+    check(cudaMalloc(&d, sizeof(float) * cnt), "cudaMalloc(sdf grid)");
+    const cudaError_t e = cudaMemcpy(d, values, sizeof(float) * cnt, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(d); check(e, "upload(sdf grid)"); }
+    GridDesc g{};
+    g.v = d; g.nx = nx; g.ny = ny; g.nz = nz;
+    g.ox = origin[0]; g.oy = origin[1]; g.oz = origin[2];
+    g.h = spacing; g.invH = 1.f / spacing; g.muS = mu_s; g.muK = mu_k;
+    grids_.push_back(g);
+    const float bx[6] = {origin[0], origin[1], origin[2], origin[0] + float(nx - 1) * spacing,
+                         origin[1] + float(ny - 1) * spacing, origin[2] + float(nz - 1) * spacing};
+    boxes_.insert(boxes_.end(), bx, bx + 6);
+    const int idx = (int)grids_.size() - 1;
+    check(cudaMemcpyAsync(d_boxes_, boxes_.data(), sizeof(float) * boxes_.size(), cudaMemcpyHostToDevice, stream_), "upload(boxes)");
+    const bool pending = pending_set_;
+    set_mesh_targets(idx, pos, quat, rows, nullptr, true, false);
+    check(launch_commit(d_cur_, d_tgt_, d_tele_, d_poses_, d_boxes_, (int)grids_.size(), idx, R_, stream_), "commit mesh");
+    check(cudaStreamSynchronize(stream_), "add_mesh");
+    pending_set_ = pending;
+    // the per-CTA pose cache must still fit: repack with fewer ropes per bin if needed
+    const int M = (int)grids_.size();
+    const int cap = std::max(1, (96 * 1024) / (2 * M * (int)sizeof(Pose)));
+    if (max_rcount_ > cap) {
+        ensure_host();
+        layout_valid_ = false;
+        device_valid_ = false;
+        ensure_device();
+    }
+    return idx;
+}
+
+void Batch::set_mesh_friction(int index, float mu_s, float mu_k) {
+    if (index < 0 || index >= (int)grids_.size()) throw std::invalid_argument("mesh index out of range");
+    grids_[index].muS = mu_s;
+    grids_[index].muK = mu_k;
+}
+
+void Batch::set_mesh_targets(int index, const float* pos, const float* quat, int rows, const uint8_t* tele, bool tele_all,
+                             bool on_device) {
+    const int M = (int)grids_.size();
+    if (index >= M || (index < 0 && M == 0)) throw std::invalid_argument("mesh index out of range");
+    ensure_device();
+    const float* dp = pos;
+    const float* dq = quat;
+    const uint8_t* dt = tele;
+    const int nrows = index < 0 ? R_ * M : rows;
+    if (!on_device) {
+        float* sq = d_stage_ + 3 * (size_t)R_ * kMaxSdf;
+        check(cudaMemcpyAsync(d_stage_, pos, sizeof(float) * 3 * nrows, cudaMemcpyHostToDevice, stream_), "upload(target pos)");
+        check(cudaMemcpyAsync(sq, quat, sizeof(float) * 4 * nrows, cudaMemcpyHostToDevice, stream_), "upload(target quat)");
+        dp = d_stage_;
+        dq = sq;
+        if (tele && !tele_all) {
+            check(cudaMemcpyAsync(d_stage_tele_, tele, R_, cudaMemcpyHostToDevice, stream_), "upload(teleport flags)");
+            dt = d_stage_tele_;
+        } else {
+            dt = nullptr;
+        }
+        // pageable sources: wait so the caller's arrays may die after the call
+        check(cudaStreamSynchronize(stream_), "stage targets");
+    }
+    check(launch_scatter_targets(d_tgt_, d_tele_, index, dp, dq, rows, M, tele_all ? nullptr : dt, tele_all ? 1 : 0, R_,
+                                 stream_),
+          "set_mesh_poses");
+    pending_set_ = true;
+}
+
+void Batch::clear_meshes() {
+    check(cudaStreamSynchronize(stream_), "clear_meshes");
+    for (auto& g : grids_) cudaFree(const_cast<float*>(g.v));
+    grids_.clear();
+    boxes_.clear();
+    pending_set_ = false;
+    moving_ = false;
+}
+
+void Batch::enable_forces(bool on) {
+    if (on && !d_force_) {
+        check(cudaMalloc(&d_force_, sizeof(float) * 3 * n_), "cudaMalloc(contact forces)");
+        check(cudaMalloc(&d_wrench_, sizeof(float) * 6 * (size_t)R_ * kMaxSdf), "cudaMalloc(mesh wrenches)");
+        check(cudaMemset(d_force_, 0, sizeof(float) * 3 * n_), "memset(contact forces)");
+        check(cudaMemset(d_wrench_, 0, sizeof(float) * 6 * (size_t)R_ * kMaxSdf), "memset(mesh wrenches)");
+    }
+    forces_on_ = on;
+}
+
+void Batch::contact_forces_host(float* out) {
+    if (!forces_on_ || !d_force_) throw std::invalid_argument("enable_contact_forces(True) first");
+    check(cudaStreamSynchronize(stream_), "sync");
+    check(cudaMemcpy(out, d_force_, sizeof(float) * 3 * n_, cudaMemcpyDeviceToHost), "download(contact forces)");
+}
+
+void Batch::wrenches_host(float* out) {
+    if (!forces_on_ || !d_wrench_) throw std::invalid_argument("enable_contact_forces(True) first");
+    std::vector<float> w(6 * (size_t)R_ * kMaxSdf);
+    check(cudaStreamSynchronize(stream_), "sync");
+    check(cudaMemcpy(w.data(), d_wrench_, sizeof(float) * w.size(), cudaMemcpyDeviceToHost), "download(mesh wrenches)");
+    const int M = (int)grids_.size();
+    for (int e = 0; e < R_; e++)
+        for (int m = 0; m < M; m++)
+            for (int k = 0; k < 6; k++) out[((size_t)e * M + m) * 6 + k] = w[((size_t)e * kMaxSdf + m) * 6 + k];
+}
+
+}  // namespace rs

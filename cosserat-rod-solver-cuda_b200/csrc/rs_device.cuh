@@ -1,0 +1,195 @@
+// rs_device.cuh -- device arithmetic of the substep: vectors, rotors, the symmetric 3x3
+// local solve, the surface contact law and the trilinear SDF sample.
+//
+// Every function keeps the operation order of the reference routine it cites so that a
+// single-precision run tracks the reference within rounding (IEEE div/sqrt, no fast math).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "rs_types.h"
+
+namespace rsd {
+
+struct f3 {
+    float x, y, z;
+};
+__device__ __forceinline__ f3 mk3(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ f3 zero3() { return f3{0.f, 0.f, 0.f}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return f3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return f3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a) { return f3{-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return f3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ f3 operator*(float s, f3 a) { return f3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ f3 operator/(f3 a, float s) { return f3{a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ f3& operator+=(f3& a, f3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+__device__ __forceinline__ f3& operator-=(f3& a, f3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
+__device__ __forceinline__ f3& operator*=(f3& a, float s) { a.x *= s; a.y *= s; a.z *= s; return a; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ f3 lerp3(f3 a, f3 b, float t) { return a * (1.f - t) + b * t; }
+__device__ __forceinline__ f3 xyz(float4 v) { return f3{v.x, v.y, v.z}; }
+__device__ __forceinline__ float4 f4(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// Rotor (x, y, z = bivector part, w = scalar) products, Rotor.h:96-105 and :185-188.
+__device__ __forceinline__ float4 qmul(float4 a, float4 b) {
+    const f3 av = xyz(a), bv = xyz(b);
+    const f3 v = bv * a.w + av * b.w + cross(av, bv);
+    return make_float4(v.x, v.y, v.z, a.w * b.w - dot(av, bv));
+}
+__device__ __forceinline__ float4 qconj(float4 a) { return make_float4(-a.x, -a.y, -a.z, a.w); }
+__device__ __forceinline__ float dot4(float4 a, float4 b) { return (a.x * b.x + a.y * b.y) + (a.z * b.z + a.w * b.w); }
+__device__ __forceinline__ float4 scale4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 normalize4(float4 a) { return scale4(a, 1.f / sqrtf(dot4(a, a))); }
+__device__ __forceinline__ f3 qrot(float4 q, f3 v) {
+    const f3 qv = xyz(q);
+    const f3 a = v * q.w + cross(qv, v);
+    const float c = dot(v, qv);
+    return a * q.w + cross(qv, a) + qv * c;
+}
+// q * e1: the tangent of the segment frame.
+__device__ __forceinline__ f3 qtangent(float4 q) { return qrot(q, mk3(1.f, 0.f, 0.f)); }
+
+// Symmetric 3x3: diag (xx, yy, zz), upper (xy, xz, yz).
+struct sym3 {
+    float xx, yy, zz, xy, xz, yz;
+};
+__device__ __forceinline__ sym3 sym_diag(float d) { return sym3{d, d, d, 0.f, 0.f, 0.f}; }
+__device__ __forceinline__ sym3 sym_zero() { return sym3{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}; }
+__device__ __forceinline__ void sym_add(sym3& a, const sym3& b) {
+    a.xx += b.xx; a.yy += b.yy; a.zz += b.zz; a.xy += b.xy; a.xz += b.xz; a.yz += b.yz;
+}
+__device__ __forceinline__ void sym_add_scaled_outer(sym3& a, f3 n, float s) {  // a += (n n^T) * s
+    a.xx += (n.x * n.x) * s; a.yy += (n.y * n.y) * s; a.zz += (n.z * n.z) * s;
+    a.xy += (n.x * n.y) * s; a.xz += (n.x * n.z) * s; a.yz += (n.y * n.z) * s;
+}
+// a -= (n n^T - I) * s
+__device__ __forceinline__ void sym_sub_scaled_outer_minus_I(sym3& a, f3 n, float s) {
+    a.xx -= (n.x * n.x - 1.f) * s; a.yy -= (n.y * n.y - 1.f) * s; a.zz -= (n.z * n.z - 1.f) * s;
+    a.xy -= (n.x * n.y) * s; a.xz -= (n.x * n.z) * s; a.yz -= (n.y * n.z) * s;
+}
+// x = H^-1 f through the adjugate of the symmetric matrix (cofactor expansion).
+__device__ __forceinline__ f3 sym_solve(const sym3& H, f3 f) {
+    const float c00 = H.yy * H.zz - H.yz * H.yz, c01 = H.xz * H.yz - H.xy * H.zz, c02 = H.xy * H.yz - H.xz * H.yy;
+    const float c11 = H.xx * H.zz - H.xz * H.xz, c12 = H.xy * H.xz - H.xx * H.yz, c22 = H.xx * H.yy - H.xy * H.xy;
+    const float idet = 1.f / (H.xx * c00 + H.xy * c01 + H.xz * c02);
+    return f3{(c00 * f.x + c01 * f.y + c02 * f.z) * idet, (c01 * f.x + c11 * f.y + c12 * f.z) * idet,
+              (c02 * f.x + c12 * f.y + c22 * f.z) * idet};
+}
+
+// Closest points of segments a0a1 / b0b1 as (u, v), Common.h:327-345.
+__device__ __forceinline__ void seg_closest(f3 a0, f3 a1, f3 b0, f3 b1, float& u, float& v) {
+    const f3 A0 = a1 - a0, A1 = b1 - b0;
+    const float a = dot(A0, A0), b = dot(A0, A1), c = dot(A1, A1);
+    const f3 diff = b0 - a0;
+    v = (b * dot(A0, diff) - a * dot(A1, diff)) / (a * c - b * b);
+    if (!isfinite(v)) v = 0.5f;
+    v = fminf(fmaxf(v, 0.f), 1.f);
+    u = fminf(fmaxf(dot(lerp3(b0, b1, v) - a0, A0) / a, 0.f), 1.f);
+    v = fminf(fmaxf(dot(lerp3(a0, a1, u) - b0, A1) / c, 0.f), 1.f);
+}
+
+// One surface contact at a vertex: penalty k (|gap| along n) + regularised Coulomb friction
+// on the tangential displacement d (relative to the surface), contact.cuh:27-46.
+__device__ __forceinline__ void surface_contact(f3 n, float gap, f3 d, float k, float h, float muS, float muK,
+                                                float vslip, f3& f, sym3& H) {
+    const float N = -k * gap;
+    f += n * N;
+    sym_add_scaled_outer(H, n, k);
+    const f3 ut = d - n * dot(n, d);
+    const float ul = len(ut);
+    const float vt = ul / h;
+    float kt;
+    if (vt <= vslip) kt = muS * N / (vslip * h);
+    else {
+        const float s = 1.f - fminf(1.f, vt / vslip - 1.f);
+        kt = (s * muS + (1.f - s) * muK) * N / ul;
+    }
+    f -= ut * kt;
+    sym_sub_scaled_outer_minus_I(H, n, kt);
+}
+
+// Trilinear phi and its exact gradient at object-frame point p, contact.cuh:57-76.
+__device__ __forceinline__ bool sdf_sample(const rs::GridDesc& g, f3 p, float& phi, f3& grad) {
+    const f3 o = mk3(g.ox, g.oy, g.oz);
+    const f3 u = (p - o) * g.invH;
+    if (!(u.x >= 0.f && u.y >= 0.f && u.z >= 0.f && u.x < float(g.nx - 1) && u.y < float(g.ny - 1) &&
+          u.z < float(g.nz - 1)))
+        return false;
+    const int i = (int)u.x, j = (int)u.y, k = (int)u.z;
+    const f3 fr = (p - (o + mk3(float(i), float(j), float(k)) * g.h)) * g.invH;
+    const float fx = fminf(fmaxf(fr.x, 0.f), 1.f), fy = fminf(fmaxf(fr.y, 0.f), 1.f), fz = fminf(fmaxf(fr.z, 0.f), 1.f);
+    const int sy = g.nz, sx = g.ny * g.nz;
+    const float* c = g.v + (size_t)i * sx + (size_t)j * sy + k;
+    const float c000 = __ldg(c), c001 = __ldg(c + 1), c010 = __ldg(c + sy), c011 = __ldg(c + sy + 1);
+    const float c100 = __ldg(c + sx), c101 = __ldg(c + sx + 1), c110 = __ldg(c + sx + sy), c111 = __ldg(c + sx + sy + 1);
+    const float dx00 = c100 - c000, dx01 = c101 - c001, dx10 = c110 - c010, dx11 = c111 - c011;
+    const float c00 = c000 + fx * dx00, c01 = c001 + fx * dx01, c10 = c010 + fx * dx10, c11 = c011 + fx * dx11;
+    const float dy0 = c10 - c00, dy1 = c11 - c01;
+    const float c0 = c00 + fy * dy0, c1 = c01 + fy * dy1;
+    phi = c0 + fz * (c1 - c0);
+    const float gx0 = dx00 + fy * (dx10 - dx00), gx1 = dx01 + fy * (dx11 - dx01);
+    grad = mk3(gx0 + fz * (gx1 - gx0), dy0 + fz * (dy1 - dy0), c1 - c0) * g.invH;
+    return true;
+}
+
+// Pose cache entry accessors (rs::Pose is 5 float4).
+struct PoseV {
+    f3 pos, vel, om, lo, hi;
+    float4 q;
+};
+__device__ __forceinline__ PoseV load_pose(const float4* e) {
+    const float4 a = e[0], b = e[1], c = e[2], d = e[3], f = e[4];
+    PoseV P;
+    P.pos = mk3(a.x, a.y, a.z);
+    P.vel = mk3(a.w, c.x, c.y);
+    P.q = b;
+    P.om = mk3(c.z, c.w, d.x);
+    P.lo = mk3(d.y, d.z, d.w);
+    P.hi = mk3(f.x, f.y, f.z);
+    return P;
+}
+__device__ __forceinline__ void store_pose(float4* e, f3 pos, float4 q, f3 vel, f3 om, f3 lo, f3 hi) {
+    e[0] = make_float4(pos.x, pos.y, pos.z, vel.x);
+    e[1] = q;
+    e[2] = make_float4(vel.y, vel.z, om.x, om.y);
+    e[3] = make_float4(om.z, lo.x, lo.y, lo.z);
+    e[4] = make_float4(hi.x, hi.y, hi.z, 0.f);
+}
+
+// World AABB of the lattice box [lo_o, hi_o] under (pos, q), contact.cuh:79-87.
+__device__ __forceinline__ void world_box(f3 lo_o, f3 hi_o, f3 pos, float4 q, f3& lo, f3& hi) {
+    lo = mk3(INFINITY, INFINITY, INFINITY);
+    hi = mk3(-INFINITY, -INFINITY, -INFINITY);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const f3 corner = mk3((c & 1) ? hi_o.x : lo_o.x, (c & 2) ? hi_o.y : lo_o.y, (c & 4) ? hi_o.z : lo_o.z);
+        const f3 w = qrot(q, corner) + pos;
+        lo = mk3(fminf(lo.x, w.x), fminf(lo.y, w.y), fminf(lo.z, w.z));
+        hi = mk3(fmaxf(hi.x, w.x), fmaxf(hi.y, w.y), fmaxf(hi.z, w.z));
+    }
+}
+
+// Contact of a vertex with one posed lattice at probe (pos - P.pos) + d, contact.cuh:94-110.
+__device__ __forceinline__ bool sdf_contact_at(const rs::GridDesc& g, const PoseV& P, f3 pos, f3 d, float h, float R,
+                                               bool moving, f3& n, float& gap, f3& dRel) {
+    float phi;
+    f3 gr;
+    if (!sdf_sample(g, qrot(qconj(P.q), (pos - P.pos) + d), phi, gr)) return false;
+    gap = phi - R;
+    if (gap >= 0.f) return false;
+    const float gl = len(gr);
+    if (!(gl > 0.f)) return false;
+    n = qrot(P.q, gr / gl);
+    dRel = d;
+    if (moving) dRel -= (P.vel + cross(P.om, pos - P.pos)) * h;
+    return true;
+}
+
+}  // namespace rsd

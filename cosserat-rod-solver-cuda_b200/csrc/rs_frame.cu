@@ -1,0 +1,566 @@
+// rs_frame.cu -- the persistent per-control-frame kernel and the small pose/view kernels.
+//
+// One CTA owns one bin of whole ropes, one thread per vertex. The CTA runs every substep of
+// the frame without leaving the SM: vertex state lives in registers, neighbour data moves
+// through shared memory, and the only global-memory traffic is the state in/out at the frame
+// boundary, the caller-order views and the SDF lattice samples (L2-resident). This replaces the
+// reference's 3 + 2*num_itr launches per substep (batch.cu:352-358, step.cpp:11-25).
+//
+// Per substep (reference kernels restated, deterministic Jacobi ordering):
+//   root program / legacy root         batch.cu:90-159
+//   mesh poses of this substep         iteration.cu:12-33
+//   inertial prediction, initial guess iteration.cu:34-68
+//   num_itr x { position step          cosserat.cu:23-225 (SNAPSHOT)
+//               frame step }           cosserat.cu:227-273 (SNAPSHOT)
+//   velocity, drag, readout, advect,   iteration.cu:77-129
+//   broad phase
+// Barriers per substep: 2 * num_itr + 2 (the position step's neighbour force exchange and the
+// displacement publish; the frame step reads a double-buffered rotor array and needs none).
+#include <cuda_runtime.h>
+
+#include "rs_device.cuh"
+#include "rs_kernels.h"
+#include "rs_types.h"
+
+using namespace rsd;
+
+namespace rs {
+
+template <int BLOCK>
+struct FrameSmem {
+    float4 dx[BLOCK];     // current displacement iterate
+    float4 p[BLOCK];      // positions at the substep start
+    float4 q[2][BLOCK];   // frame rotors, double buffered across frame steps
+    float4 fa[BLOCK];     // segment force on the next vertex (xyz) + H2.xx
+    float4 fb[BLOCK];     // H2.yy, H2.zz, H2.xy, H2.xz
+    float fc[BLOCK];      // H2.yz
+};
+
+constexpr int kPoseF4 = 5;  // float4 per cached pose
+
+__device__ __forceinline__ uint64_t all_meshes(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
+
+// Shortest-arc SLERP with an nlerp fallback above dot 0.9995, batch.cu:106-114.
+__device__ __forceinline__ float4 slerp4(float4 a, float4 b, float t) {
+    float d = dot4(a, b);
+    if (d < 0.f) { b = scale4(b, -1.f); d = -d; }
+    if (d > 0.9995f) return normalize4(add4(scale4(a, 1.f - t), scale4(b, t)));
+    const float th = acosf(fminf(d, 1.f));
+    const float s = sinf(th);
+    return add4(scale4(a, sinf((1.f - t) * th) / s), scale4(b, sinf(t * th) / s));
+}
+__device__ __forceinline__ float4 unit_or_identity(const float* q) {
+    float4 a = make_float4(q[0], q[1], q[2], q[3]);
+    const float l = dot4(a, a);
+    return (l > 0.f) ? scale4(a, rsqrtf(l)) : make_float4(0.f, 0.f, 0.f, 1.f);
+}
+
+// Surfaces (planes, then candidate meshes in ascending index) at one probe point,
+// contact.cuh:141-163; `wr` != nullptr turns it into the readout (contact.cuh:172-204).
+__device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
+                                         float h, f3& f, sym3& H, float* wr, f3* facc) {
+    for (int pl = 0; pl < a.num_planes; pl++) {
+        const float4 P = a.planes[pl];
+        const f3 n = mk3(P.x, P.y, P.z);
+        const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
+        if (gap >= 0.f) continue;
+        surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
+    }
+    for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
+        const int m = __ffsll((long long)mm) - 1;
+        const PoseV P = load_pose(cache + m * kPoseF4);
+        f3 n, dRel;
+        float gap;
+        if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, n, gap, dRel)) continue;
+        if (wr) {
+            f3 fm = zero3();
+            sym3 Hs = sym_zero();
+            surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, fm, Hs);
+            *facc += fm;
+            const f3 r = (pos - P.pos) + d - n * a.c_radius;
+            const f3 tq = cross(r, -fm);
+            float* w = wr + m * 6;
+            atomicAdd(w + 0, -fm.x); atomicAdd(w + 1, -fm.y); atomicAdd(w + 2, -fm.z);
+            atomicAdd(w + 3, tq.x); atomicAdd(w + 4, tq.y); atomicAdd(w + 5, tq.z);
+        } else {
+            surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, f, H);
+        }
+    }
+}
+
+template <int BLOCK, bool SURF>
+__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(const FrameArgs a) {
+    extern __shared__ float4 dyn_smem[];  // FrameSmem<BLOCK>, then the pose cache [2][pose_cache][kPoseF4]
+    FrameSmem<BLOCK>& sm = *reinterpret_cast<FrameSmem<BLOCK>*>(dyn_smem);
+    float4* pose_smem = dyn_smem + sizeof(FrameSmem<BLOCK>) / sizeof(float4);
+
+    const Bin bin = a.bins[blockIdx.x];
+    const int t = threadIdx.x;
+    const bool act = t < bin.vcount;
+    const int dv = bin.vstart + t;
+
+    // ---- load this vertex (registers for the whole frame)
+    f3 p = zero3(), v = zero3(), lv = zero3();
+    float im = 0.f, lr = 1.f, ks = 0.f;
+    float4 q = make_float4(0.f, 0.f, 0.f, 1.f), qrp = q, qro = q;
+    uint32_t fl = 0;
+    int lrope = 0, uidx = 0, env = 0;
+    if (act) {
+        const float4 a0 = a.pos[dv], a1 = a.vel[dv], a2 = a.lvel[dv];
+        const int4 tp = a.topo[dv];
+        p = xyz(a0); im = a0.w;
+        v = xyz(a1); lr = a1.w;
+        lv = xyz(a2); ks = a2.w;
+        q = a.q[dv];
+        qro = a.qrest[dv];
+        fl = (uint32_t)tp.x; lrope = tp.y; uidx = tp.z; env = tp.w;
+        if (fl & F_PREV) qrp = a.qrest[dv - 1];
+    }
+    const bool hasNext = fl & F_NEXT, hasPrev = fl & F_PREV;
+    const bool isRoot = (fl & F_ROOT) != 0;
+
+    const float h = a.h;
+    const float invl = 1.f / lr;
+    const float Hd = 1.f / (im * h * h);
+    const float fm = 1.f / (h * h * im);
+    const float damp = a.damping / h;
+    const float invH = 1.f / h;
+    const f3 g = mk3(a.gx, a.gy, a.gz);
+    const float g2 = dot(g, g);
+    const float kap = a.c_kappa / h;
+    const float kc = kap * kap / im;
+    const int S = a.substeps, I = a.iters;
+
+    // ---- root driving inputs (caller rope order)
+    f3 P0 = zero3(), V0 = zero3(), A = zero3();
+    float4 qa = q, qb = q;
+    if (isRoot && a.root_mode != ROOT_NONE) {
+        const float* row = a.prog + (size_t)env * 17;
+        P0 = mk3(row[0], row[1], row[2]);
+        V0 = mk3(row[3], row[4], row[5]);
+        if (a.root_mode == ROOT_PROGRAM) {
+            const f3 P1 = mk3(row[6], row[7], row[8]);
+            A = 2.f / (a.dt * a.dt) * ((P1 - P0) - V0 * a.dt);
+            if (a.has_q0) qa = unit_or_identity(row + 9);
+            if (a.has_q1) qb = unit_or_identity(row + 13);
+        } else {  // ROOT_SET: constant-velocity frame, batch.cu:90-104
+            p = P0;
+            v = V0;
+            if (a.has_q0) q = unit_or_identity(row + 9);
+        }
+    }
+
+    // ---- mesh pose cache (per CTA: its ropes x meshes)
+    const int nsdf = SURF ? a.num_sdf : 0;
+    const int nPose = bin.rcount * nsdf;
+    float4* cache0 = pose_smem;
+    float4* cache1 = pose_smem + (size_t)a.pose_cache * kPoseF4;
+    if constexpr (SURF) if (nsdf > 0 && !a.sdf_moving) {
+        for (int e = t; e < nPose; e += BLOCK) {
+            const int r = e / nsdf, m = e % nsdf;
+            const int en = a.ropes[bin.rstart + r].user;
+            const float4* src = reinterpret_cast<const float4*>(a.poses + (size_t)en * kMaxSdf + m);
+#pragma unroll
+            for (int k = 0; k < kPoseF4; k++) { cache0[e * kPoseF4 + k] = src[k]; cache1[e * kPoseF4 + k] = src[k]; }
+        }
+    }
+    uint64_t cand = all_meshes(nsdf);  // the first substep of a frame visits every mesh
+    f3 facc = zero3();
+    float* wrow = (SURF && a.forces_on && nsdf > 0) ? a.wrench + (size_t)env * kMaxSdf * 6 : nullptr;
+
+    int cur = 0;
+    if (act) sm.q[0][t] = q;
+
+    for (int s = 0; s < S; s++) {
+        // ---- root program of this substep, batch.cu:122-159
+        if (isRoot && a.root_mode == ROOT_PROGRAM) {
+            const float tau = float(s) * h;
+            p = P0 + V0 * tau + 0.5f * tau * tau * A;
+            v = V0 + (tau + 0.5f * h) * A;
+            if (a.has_q0) {
+                float4 qq = a.has_q1 ? slerp4(qa, qb, float(s + 1) / float(S)) : qa;
+                const float l2 = dot4(qq, qq);
+                q = (l2 > 0.f) ? scale4(qq, rsqrtf(l2)) : make_float4(0.f, 0.f, 0.f, 1.f);
+                sm.q[cur][t] = q;
+            }
+        }
+        // ---- kinematic mesh poses of this substep, iteration.cu:12-33
+        float4* cache = (SURF && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
+        if constexpr (SURF) if (nsdf > 0 && a.sdf_moving) {
+            const float al = float(s + 1) / float(S);
+            const float invDt = 1.f / (float(S) * h);
+            for (int e = t; e < nPose; e += BLOCK) {
+                const int r = e / nsdf, m = e % nsdf;
+                const int en = a.ropes[bin.rstart + r].user;
+                const Motion M = a.motion[(size_t)en * kMaxSdf + m];
+                const f3 p0 = mk3(M.p0x, M.p0y, M.p0z), dp = mk3(M.dpx, M.dpy, M.dpz), rot = mk3(M.rx, M.ry, M.rz);
+                const float4 q0 = make_float4(M.qx, M.qy, M.qz, M.qw);
+                f3 Pp, Pv, Pw;
+                float4 Pq;
+                const float th = len(rot);
+                if (th > 0.f || dp.x != 0.f || dp.y != 0.f || dp.z != 0.f) {
+                    Pp = p0 + al * dp;
+                    float4 dq = make_float4(0.f, 0.f, 0.f, 1.f);
+                    if (th > 0.f) {
+                        const f3 ax = rot / th;
+                        const float hr = (al * th) * 0.5f;
+                        const float sn = sinf(hr);
+                        dq = make_float4(sn * ax.x, sn * ax.y, sn * ax.z, cosf(hr));
+                    }
+                    Pq = normalize4(qmul(dq, q0));
+                    Pv = dp * invDt;
+                    Pw = rot * invDt;
+                } else {
+                    Pp = p0; Pq = q0; Pv = zero3(); Pw = zero3();
+                }
+                const GridDesc& gd = a.grids[m];
+                const f3 lo_o = mk3(gd.ox, gd.oy, gd.oz);
+                const f3 hi_o = lo_o + mk3(float(gd.nx - 1), float(gd.ny - 1), float(gd.nz - 1)) * gd.h;
+                f3 lo, hi;
+                world_box(lo_o, hi_o, Pp, Pq, lo, hi);
+                store_pose(cache + e * kPoseF4, Pp, Pq, Pv, Pw, lo, hi);
+            }
+        }
+        const float4* mycache = cache + lrope * nsdf * kPoseF4;
+
+        // ---- inertial prediction and initial guess, iteration.cu:34-68
+        const f3 vel0 = v;
+        f3 dx = vel0 * h;
+        const f3 lv_old = lv;
+        lv = vel0;
+        const f3 y = dx + g * (h * h);
+        if (im != 0.f && g2 > 0.f) {
+            const f3 acc = (vel0 - lv_old) / a.last_h;
+            const float sg = fminf(fmaxf(dot(acc, g) / g2, 0.f), 1.f);
+            dx += g * (h * h * sg);
+        }
+        if (act) {
+            sm.p[t] = f4(p, 0.f);
+            sm.dx[t] = f4(dx, 0.f);
+        }
+        __syncthreads();  // B0
+        const f3 p1 = hasNext ? xyz(sm.p[t + 1]) : zero3();
+
+        for (int it = 0; it < I; it++) {
+            // ---- position step, cosserat.cu:37-193
+            f3 f = (y - dx) * fm;
+            sym3 H = sym_diag(Hd);
+            if (SURF && im != 0.f && (a.num_planes > 0 || nsdf > 0))
+                surfaces(a, mycache, cand, p, dx, kc, h, f, H, nullptr, nullptr);
+            f3 f2 = zero3();
+            sym3 H2 = sym_zero();
+            if (hasNext) {
+                const f3 p1dx = xyz(sm.dx[t + 1]);
+                const f3 c = ((p1 - p) + (p1dx - dx)) * invl - qtangent(q);
+                const float k = ks * invl;
+                float dd = k * invl;
+                f += c * k - dx * (damp * dd);
+                f2 += c * (-k) - p1dx * (damp * dd);
+                dd *= 1.f + damp;
+                H.xx += dd; H.yy += dd; H.zz += dd;
+                H2.xx += dd; H2.yy += dd; H2.zz += dd;
+            }
+            if (act) {
+                sm.fa[t] = f4(f2, H2.xx);
+                sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
+                sm.fc[t] = H2.yz;
+            }
+            __syncthreads();  // B1
+            if (hasPrev) {
+                const float4 fa = sm.fa[t - 1], fb = sm.fb[t - 1];
+                f += xyz(fa);
+                H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
+            }
+            if (im != 0.f) dx += sym_solve(H, f) * a.accel;
+            if (act) sm.dx[t] = f4(dx, 0.f);
+            __syncthreads();  // B2
+
+            // ---- frame step, cosserat.cu:242-272
+            if (!(fl & F_FIX_ORIENT) && hasNext) {
+                const f3 p1dx = xyz(sm.dx[t + 1]);
+                f3 vv = ((p1 - p) + (p1dx - dx)) / lr;
+                vv *= -2.f * ks;
+                float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 q0 = q;
+                if (hasPrev) {
+                    const float4 qq = sm.q[cur][t - 1];
+                    const float sg = dot4(qmul(qconj(qq), q0), qrp) > 0.f ? 1.f : -1.f;
+                    b = add4(b, scale4(qmul(qq, qrp), sg));
+                }
+                if (fl & F_NEXT_ORIENT) {
+                    const float4 qq = sm.q[cur][t + 1];
+                    const float sg = dot4(qmul(qconj(q0), qq), qro) > 0.f ? 1.f : -1.f;
+                    b = add4(b, scale4(qmul(qq, qconj(qro)), sg));
+                }
+                const float lambda = len(vv) + sqrtf(dot4(b, b));
+                const float4 m = qmul(qmul(f4(vv, 0.f), b), make_float4(1.f, 0.f, 0.f, 0.f));
+                q = normalize4(add4(m, scale4(b, lambda)));
+            }
+            if (act) sm.q[cur ^ 1][t] = q;
+            cur ^= 1;
+        }
+        __syncthreads();  // B3
+
+        // ---- velocity, drag, readout, advection, broad phase; iteration.cu:85-128
+        if (im != 0.f) {
+            f3 vv = dx * invH;
+            const float kn = a.drag_quad;
+            if (kn > 0.f) {
+                const f3 tg = hasNext ? qtangent(q) : qtangent(sm.q[cur][t - 1]);
+                const f3 vt = tg * dot(tg, vv);
+                f3 vn = vv - vt;
+                vn = vn / (1.f + kn * len(vn) * h);
+                const f3 vt2 = vt / (1.f + a.drag_quad_t * len(vt) * h);
+                vv = vn + vt2;
+            }
+            v = vv * (1.f - a.drag * h);
+            if (SURF && a.forces_on && (a.num_planes > 0 || nsdf > 0)) {
+                // planes accumulate into fv; each mesh's force is added to fv and its wrench
+                // goes to the (env, mesh) row, contact.cuh:172-204
+                f3 fv = zero3();
+                sym3 Hs = sym_zero();
+                surfaces(a, mycache, cand, p, dx, kc, h, fv, Hs, wrow, &fv);
+                facc += fv;
+            }
+        }
+        p += dx;
+        if (SURF && nsdf > 0) {
+            if (im != 0.f) {
+                const float pad = 2.f * len(dx) + 0.02f;
+                uint64_t mask = 0ull;
+                int cnt = 0;
+                for (int m = 0; m < nsdf; m++) {
+                    const PoseV P = load_pose(mycache + m * kPoseF4);
+                    const float pm = pad + (a.sdf_moving ? h * (len(P.vel) + len(P.om) * 0.5f * len(P.hi - P.lo)) : 0.f);
+                    if (p.x >= P.lo.x - pm && p.x <= P.hi.x + pm && p.y >= P.lo.y - pm && p.y <= P.hi.y + pm &&
+                        p.z >= P.lo.z - pm && p.z <= P.hi.z + pm) {
+                        mask |= 1ull << m;
+                        cnt++;
+                    }
+                }
+                cand = cnt <= kMaxCand ? mask : all_meshes(nsdf);
+            } else {
+                cand = 0ull;
+            }
+        }
+    }
+
+    // ---- write back: device-order state and caller-order views
+    if (act) {
+        a.pos[dv] = f4(p, im);
+        a.vel[dv] = f4(v, lr);
+        a.lvel[dv] = f4(lv, ks);
+        a.q[dv] = q;
+        float* op = a.out_pos + (size_t)uidx * 3;
+        op[0] = p.x; op[1] = p.y; op[2] = p.z;
+        float* ov = a.out_vel + (size_t)uidx * 3;
+        ov[0] = v.x; ov[1] = v.y; ov[2] = v.z;
+        reinterpret_cast<float4*>(a.out_q)[uidx] = q;
+        if (SURF && a.forces_on && a.out_force) {
+            const float k = 1.f / float(S);
+            float* of = a.out_force + (size_t)uidx * 3;
+            of[0] = facc.x * k; of[1] = facc.y * k; of[2] = facc.z * k;
+        }
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicOr(a.status + 2, 1);
+    }
+}
+
+// ------------------------------------------------------------------ launch
+template <int BLOCK, bool SURF>
+static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_bytes, cudaStream_t s) {
+    auto k = frame_kernel<BLOCK, SURF>;
+    const size_t dyn_smem = sizeof(FrameSmem<BLOCK>) + pose_bytes;
+    if (dyn_smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<num_bins, BLOCK, dyn_smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s) {
+    const bool surf = a.num_planes > 0 || a.num_sdf > 0;
+    const size_t dyn = surf && a.num_sdf > 0 ? (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4) : 0;
+    switch (block) {
+        case 64: return surf ? launch_frame_t<64, true>(a, num_bins, dyn, s) : launch_frame_t<64, false>(a, num_bins, dyn, s);
+        case 128: return surf ? launch_frame_t<128, true>(a, num_bins, dyn, s) : launch_frame_t<128, false>(a, num_bins, dyn, s);
+        case 256: return surf ? launch_frame_t<256, true>(a, num_bins, dyn, s) : launch_frame_t<256, false>(a, num_bins, dyn, s);
+        case 512: return surf ? launch_frame_t<512, true>(a, num_bins, dyn, s) : launch_frame_t<512, false>(a, num_bins, dyn, s);
+        case 1024: return surf ? launch_frame_t<1024, true>(a, num_bins, dyn, s) : launch_frame_t<1024, false>(a, num_bins, dyn, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ------------------------------------------------------------------ views and resets
+// Device state -> caller-order views, batch.cu:163-175.
+__global__ void gather_kernel(const float4* pos, const float4* vel, const float4* q, const int4* topo, float* out_pos,
+                              float* out_vel, float* out_q, int n) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const int u = topo[d].z;
+    const float4 p = pos[d], v = vel[d];
+    out_pos[3 * (size_t)u] = p.x; out_pos[3 * (size_t)u + 1] = p.y; out_pos[3 * (size_t)u + 2] = p.z;
+    out_vel[3 * (size_t)u] = v.x; out_vel[3 * (size_t)u + 1] = v.y; out_vel[3 * (size_t)u + 2] = v.z;
+    reinterpret_cast<float4*>(out_q)[u] = q[d];
+}
+
+cudaError_t launch_gather(const FrameArgs& a, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    gather_kernel<<<(n + 255) / 256, 256, 0, s>>>(a.pos, a.vel, a.q, a.topo, a.out_pos, a.out_vel, a.out_q, n);
+    return cudaGetLastError();
+}
+
+// Restore the construction state of listed ropes (device ranges), batch.cu:178-189.
+__global__ void reset_kernel(float4* pos, float4* vel, float4* lvel, float4* q, const float4* init_pos,
+                             const float4* init_q, const int2* ranges, int count, int maxv) {
+    const int r = blockIdx.y;
+    if (r >= count) return;
+    const int2 rg = ranges[r];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rg.y && i < maxv; i += gridDim.x * blockDim.x) {
+        const int d = rg.x + i;
+        const float4 p0 = init_pos[d];
+        pos[d] = make_float4(p0.x, p0.y, p0.z, pos[d].w);
+        vel[d] = make_float4(0.f, 0.f, 0.f, vel[d].w);
+        lvel[d] = make_float4(0.f, 0.f, 0.f, lvel[d].w);
+        q[d] = init_q[d];
+    }
+}
+
+cudaError_t launch_reset(float4* pos, float4* vel, float4* lvel, float4* q, const float4* init_pos, const float4* init_q,
+                         const int2* ranges, int count, int maxv, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    dim3 grid((maxv + 255) / 256, count);
+    reset_kernel<<<grid, 256, 0, s>>>(pos, vel, lvel, q, init_pos, init_q, ranges, count, maxv);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ mesh pose machine (sdf.cu)
+// Rotation vector taking unit q0 to unit q1 (world, shortest arc), sdf.cu:25-33. A target
+// bitwise equal to the current pose gives exactly zero motion.
+__device__ __forceinline__ f3 rotvec(float4 q0, float4 q1) {
+    if (q0.x == q1.x && q0.y == q1.y && q0.z == q1.z && q0.w == q1.w) return zero3();
+    const f3 av = mk3(q1.x, q1.y, q1.z), bv = mk3(-q0.x, -q0.y, -q0.z);
+    f3 vv = q1.w * bv + q0.w * av + cross(av, bv);
+    float w = q1.w * q0.w - dot(av, bv);
+    if (w < 0.f) { vv = -vv; w = -w; }
+    const float sl = len(vv);
+    if (!(sl > 1e-9f)) return zero3();
+    return vv * (2.f * atan2f(sl, w) / sl);
+}
+
+// Caller rows -> targets: one mesh for every env (index >= 0, rows 1 or N) or a dense
+// [N, M] block (index < 0), sdf.cu:37-51.
+__global__ void scatter_targets_kernel(Pose7* tgt, uint8_t* tele, int index, const float* pos, const float* quat, int rows,
+                                       int M, const uint8_t* tele_flags, int tele_all, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int per = index < 0 ? M : 1;
+    if (i >= N * per) return;
+    const int e = i / per, m = index < 0 ? i % per : index;
+    const int r = index < 0 ? i : (rows == 1 ? 0 : e);
+    float4 qq = make_float4(quat[4 * r], quat[4 * r + 1], quat[4 * r + 2], quat[4 * r + 3]);
+    const float l = sqrtf(dot4(qq, qq));
+    qq = l > 0.f ? make_float4(qq.x / l, qq.y / l, qq.z / l, qq.w / l) : make_float4(0.f, 0.f, 0.f, 1.f);
+    const size_t slot = (size_t)e * kMaxSdf + m;
+    Pose7 P;
+    P.px = pos[3 * r]; P.py = pos[3 * r + 1]; P.pz = pos[3 * r + 2];
+    P.qx = qq.x; P.qy = qq.y; P.qz = qq.z; P.qw = qq.w; P.pad_ = 0.f;
+    tgt[slot] = P;
+    tele[slot] = tele_all ? 1 : (tele_flags ? tele_flags[e] : 0);
+}
+
+cudaError_t launch_scatter_targets(Pose7* tgt, uint8_t* tele, int index, const float* pos, const float* quat, int rows,
+                                   int M, const uint8_t* tele_flags, int tele_all, int N, cudaStream_t s) {
+    const int threads = index < 0 ? N * M : N;
+    if (threads <= 0) return cudaSuccess;
+    scatter_targets_kernel<<<(threads + 255) / 256, 256, 0, s>>>(tgt, tele, index, pos, quat, rows, M, tele_flags, tele_all, N);
+    return cudaGetLastError();
+}
+
+// This frame's motion per (env, mesh); teleported slots jump first, sdf.cu:55-63.
+__global__ void stage_motion_kernel(Pose7* cur, const Pose7* tgt, uint8_t* tele, Motion* motion, int total) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    if (tele[i]) { cur[i] = tgt[i]; tele[i] = 0; }
+    const Pose7 c = cur[i], g = tgt[i];
+    Motion M;
+    M.p0x = c.px; M.p0y = c.py; M.p0z = c.pz;
+    M.qx = c.qx; M.qy = c.qy; M.qz = c.qz; M.qw = c.qw;
+    M.dpx = g.px - c.px; M.dpy = g.py - c.py; M.dpz = g.pz - c.pz;
+    const f3 r = rotvec(make_float4(c.qx, c.qy, c.qz, c.qw), make_float4(g.qx, g.qy, g.qz, g.qw));
+    M.rx = r.x; M.ry = r.y; M.rz = r.z;
+    M.pad0 = M.pad1 = M.pad2 = 0.f;
+    motion[i] = M;
+}
+
+cudaError_t launch_stage_motion(Pose7* cur, const Pose7* tgt, uint8_t* tele, Motion* motion, int total, cudaStream_t s) {
+    if (total <= 0) return cudaSuccess;
+    stage_motion_kernel<<<(total + 255) / 256, 256, 0, s>>>(cur, tgt, tele, motion, total);
+    return cudaGetLastError();
+}
+
+// Targets become current static poses with world boxes, sdf.cu:67-87. `only` >= 0 commits a
+// single mesh index (a newly added mesh).
+__global__ void commit_kernel(Pose7* cur, const Pose7* tgt, uint8_t* tele, Pose* poses, const float* boxes, int num_sdf,
+                              int only, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int per = only >= 0 ? 1 : kMaxSdf;
+    if (i >= N * per) return;
+    const int e = i / per, m = only >= 0 ? only : i % per;
+    if (m >= num_sdf) return;
+    const size_t slot = (size_t)e * kMaxSdf + m;
+    cur[slot] = tgt[slot];
+    tele[slot] = 0;
+    const Pose7 c = cur[slot];
+    const f3 lo_o = mk3(boxes[6 * m], boxes[6 * m + 1], boxes[6 * m + 2]);
+    const f3 hi_o = mk3(boxes[6 * m + 3], boxes[6 * m + 4], boxes[6 * m + 5]);
+    const float4 qq = make_float4(c.qx, c.qy, c.qz, c.qw);
+    f3 lo, hi;
+    const f3 pp = mk3(c.px, c.py, c.pz);
+    world_box(lo_o, hi_o, pp, qq, lo, hi);
+    store_pose(reinterpret_cast<float4*>(poses + slot), pp, qq, zero3(), zero3(), lo, hi);
+}
+
+cudaError_t launch_commit(Pose7* cur, const Pose7* tgt, uint8_t* tele, Pose* poses, const float* boxes, int num_sdf,
+                          int only, int N, cudaStream_t s) {
+    const int threads = only >= 0 ? N : N * kMaxSdf;
+    if (threads <= 0) return cudaSuccess;
+    commit_kernel<<<(threads + 255) / 256, 256, 0, s>>>(cur, tgt, tele, poses, boxes, num_sdf, only, N);
+    return cudaGetLastError();
+}
+
+__global__ void scale_kernel(float* x, int n, float k) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] *= k;
+}
+
+cudaError_t launch_scale(float* x, int n, float k, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    scale_kernel<<<(n + 255) / 256, 256, 0, s>>>(x, n, k);
+    return cudaGetLastError();
+}
+
+}  // namespace rs
+
+// ------------------------------------------------------------------ measurement probe
+namespace rs {
+// FP32 FMA throughput probe: every thread runs `iters` rounds of 8 independent FMA chains, so
+// the FMA pipe (not latency) is the limit. Used by bench.py as the measured FP32 peak.
+__global__ void fp32_probe_kernel(float* out, int iters, float a, float b) {
+    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1e-7f, x2 = x0 + 2e-7f, x3 = x0 + 3e-7f;
+    float x4 = x0 + 4e-7f, x5 = x0 + 5e-7f, x6 = x0 + 6e-7f, x7 = x0 + 7e-7f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    const float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
+}
+
+cudaError_t launch_fp32_probe(float* out, int blocks, int threads, int iters, cudaStream_t s) {
+    fp32_probe_kernel<<<blocks, threads, 0, s>>>(out, iters, 0.999999f, 1e-7f);
+    return cudaGetLastError();
+}
+}  // namespace rs

@@ -1,0 +1,27 @@
+// rs_kernels.h -- host-side launchers of the kernels in rs_frame.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "rs_types.h"
+
+namespace rs {
+
+// One persistent launch that runs every substep of one control frame for every bin.
+cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s);
+// Device state -> caller-order views.
+cudaError_t launch_gather(const FrameArgs& a, int n, cudaStream_t s);
+// Restore construction state of device vertex ranges (x = start, y = count).
+cudaError_t launch_reset(float4* pos, float4* vel, float4* lvel, float4* q, const float4* init_pos, const float4* init_q,
+                         const int2* ranges, int count, int maxv, cudaStream_t s);
+// Mesh pose machine.
+cudaError_t launch_scatter_targets(Pose7* tgt, uint8_t* tele, int index, const float* pos, const float* quat, int rows,
+                                   int M, const uint8_t* tele_flags, int tele_all, int N, cudaStream_t s);
+cudaError_t launch_stage_motion(Pose7* cur, const Pose7* tgt, uint8_t* tele, Motion* motion, int total, cudaStream_t s);
+cudaError_t launch_commit(Pose7* cur, const Pose7* tgt, uint8_t* tele, Pose* poses, const float* boxes, int num_sdf,
+                          int only, int N, cudaStream_t s);
+cudaError_t launch_scale(float* x, int n, float k, cudaStream_t s);
+// FP32 FMA throughput probe (16 * 8 FMAs per thread per iteration).
+cudaError_t launch_fp32_probe(float* out, int blocks, int threads, int iters, cudaStream_t s);
+
+}  // namespace rs

@@ -1,0 +1,125 @@
+// rs_types.h -- plain-old-data shared by the host driver and the sm_100a kernels.
+//
+// Device layout ("packed order"): ropes are packed whole into bins; one bin is one CTA of
+// BLOCK threads, one thread per vertex, and a rope never straddles two bins. Device vertex
+// arrays are in bin order; `uidx` maps every device vertex back to the caller's flat order
+// (rope-major, as in the reference's RopeBatch: rope e owns [start_e, start_e + V_e)).
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define RS_HD __host__ __device__
+#else
+#define RS_HD
+#endif
+
+namespace rs {
+
+// Vertex flags. Bits 0-3 keep the meaning of YarnBall's VertexFlags (YarnBall.h:52-58);
+// bit 5 marks a rope's first vertex (the driven root).
+enum : uint32_t {
+    F_PREV = 1u,         // has a previous vertex on the same rope
+    F_NEXT = 2u,         // has a next vertex (owns segment i -> i+1)
+    F_NEXT_ORIENT = 4u,  // segment i has a next segment (bending with i+1)
+    F_FIX_ORIENT = 8u,   // frame of segment i is held (clamped root, rope end)
+    F_ROOT = 32u,        // first vertex of its rope
+};
+
+constexpr int kMaxSdf = 64;      // meshes per solver (YarnBall.h:153)
+constexpr int kMaxCand = 8;      // broad-phase list length before "visit every mesh"
+constexpr int kMaxPlanes = 8;
+constexpr int kMaxCols = 128;    // rope-rope candidates per segment (YarnBall.h:38)
+
+// Solver status words (YarnBall.h:204-208).
+enum : int { ERR_NONE = 0, ERR_MAX_COLLISIONS = 1, WARN_INTERPENETRATION = 2 };
+
+// One bin = one CTA: a contiguous range of device vertices and of device ropes.
+struct Bin {
+    int vstart, vcount;   // device vertices [vstart, vstart + vcount)
+    int rstart, rcount;   // device ropes [rstart, rstart + rcount)
+};
+
+// One rope in device order.
+struct Rope {
+    int dstart, count;    // device vertices
+    int ustart;           // first vertex in the caller's flat order
+    int user;             // caller's rope index (= env of its meshes, row of its root program)
+};
+
+// A signed-distance lattice: values[nx, ny, nz] (C order) at origin + ijk * h, object frame.
+struct GridDesc {
+    const float* v;
+    int nx, ny, nz;
+    float ox, oy, oz;
+    float h, invH;
+    float muS, muK;
+    float pad_;
+};
+
+// Kinematic pose of (env, mesh) at the end of a substep: position, rotor (x, y, z, w),
+// velocity of the origin, angular velocity (world), world AABB of the lattice.
+struct Pose {
+    float px, py, pz, vx;
+    float qx, qy, qz, qw;
+    float vy, vz, wx, wy;
+    float wz, lox, loy, loz;
+    float hix, hiy, hiz, pad_;
+};
+
+// One frame of motion of (env, mesh): start pose, translation, world rotation vector.
+struct Motion {
+    float p0x, p0y, p0z, dpx;
+    float qx, qy, qz, qw;
+    float dpy, dpz, rx, ry;
+    float rz, pad0, pad1, pad2;
+};
+
+// Host staging of a caller-side pose target: position + rotor.
+struct Pose7 {
+    float px, py, pz, qx, qy, qz, qw, pad_;
+};
+
+// Root driving of one frame.
+enum : int { ROOT_NONE = 0, ROOT_PROGRAM = 1, ROOT_SET = 2 };
+
+// Everything one persistent frame launch needs, passed by value.
+struct FrameArgs {
+    // topology (device order)
+    const Bin* bins;
+    const Rope* ropes;
+    const int4* topo;        // (flags, local rope within the bin, uidx, env)
+    // state (device order), updated in place
+    float4* pos;             // (x, y, z, invMass)
+    float4* vel;             // (vx, vy, vz, lRest)
+    float4* lvel;            // (last substep's start velocity xyz, kStretch)
+    float4* q;               // segment frame rotor
+    const float4* qrest;     // rest rotation (scaled by the bending stiffness)
+    // caller-order outputs (the zero-copy views)
+    float* out_pos;          // [n, 3]
+    float* out_vel;          // [n, 3]
+    float* out_q;            // [n, 4]
+    float* out_force;        // [n, 3] contact force readout (forces on)
+    float* wrench;           // [envs, 64, 6] mesh wrench readout (forces on)
+    int* status;             // [2] error, warning
+    // root program rows [R, 17] = (p0, v0, p1, q0, q1), caller rope order
+    const float* prog;
+    int root_mode, has_q0, has_q1;
+    // step
+    float h, last_h, dt;
+    int substeps, iters;
+    // physics
+    float gx, gy, gz;
+    float damping, drag, drag_quad, drag_quad_t, accel;
+    // surface contact
+    int num_planes;
+    float4 planes[kMaxPlanes];
+    float c_radius, c_kappa, c_mu_s, c_mu_k, c_vslip;
+    int num_sdf, sdf_moving, forces_on;
+    int pose_cache;          // pose cache entries per buffer (= max ropes per bin * num_sdf)
+    const Pose* poses;       // [envs * 64] committed static poses
+    const Motion* motion;    // [envs * 64] this frame's motion (sdf_moving)
+    GridDesc grids[kMaxSdf];
+};
+
+}  // namespace rs

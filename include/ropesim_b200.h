@@ -1,0 +1,179 @@
+/* ropesim_b200.h -- C-ABI of the B200 Stable Cosserat Rods substep engine.
+ *
+ * The boundary the reference's Python module binds (csrc/bindings.cpp of
+ * DeformX/Cosserat-Rod-Solver-CUDA, pybind11 `_ropesim`) is re-expressed as plain C: opaque
+ * handles, host or device float pointers with explicit sizes, `int` status codes and a
+ * thread-local error string. No torch or pybind11 types cross it. The pybind11 module
+ * `ropesim._ropesim` of this repository is one client; ctypes / cffi clients work the same way
+ * (see INTEGRATION.md).
+ *
+ * Layout conventions: "caller order" is the reference's flat order (rope r owns its vertices
+ * consecutively, ropes in index order). Rotors are (x, y, z, w). All device pointers are
+ * float32, C-contiguous. Every call is serialised by a per-handle mutex; device work runs on
+ * the handle's own blocking stream (ordered with the legacy default stream, as the
+ * reference's solver stream is: csrc/batch.h:9-14).
+ */
+#ifndef ROPESIM_B200_H
+#define ROPESIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define RS_API __declspec(dllexport)
+#else
+#define RS_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. RS_EINVAL maps to the reference's ValueError (bindings.cpp throws
+ * py::value_error before any state change), RS_ECUDA to its RuntimeError (Common.h:17-30),
+ * RS_ESOLVER to Sim::checkErrors' solver errors (YarnBall.cu:311-339). */
+#define RS_OK 0
+#define RS_EINVAL 1
+#define RS_ECUDA 2
+#define RS_ESOLVER 3
+
+typedef struct rs_batch rs_batch;
+
+/* Last error message of the calling thread ("" when none). */
+RS_API const char* rs_last_error_string(void);
+/* Library version string. */
+RS_API const char* rs_version(void);
+
+/* ---------------------------------------------------------------- construction
+ * Replaces RopeBatch::RopeBatch + Sim::configure/setKStretch/setKBend (csrc/batch.cu:330-413,
+ * YarnBall.cu:112-259) and RopeSim::RopeSim (bindings.cpp:196-265).
+ * rope_verts[num_ropes] (each >= 3, <= 1024; uneven lengths allowed), positions host
+ * [sum(rope_verts), 3], pinned host [sum(rope_verts)] or NULL (each rope's first vertex).
+ * dead_radius / dead_barrier: the rope-rope radii used only by the segment-length validity
+ * check (batch.cu:363-375: 0.01 / 0.08 of the shortest segment). */
+RS_API int rs_batch_create(rs_batch** out, int num_ropes, const int* rope_verts, const float* positions,
+                    const uint8_t* pinned, float density, float k_stretch, float k_bend, float max_h,
+                    int num_itr, int fix_root_orientation, int straight_rest, float dead_radius,
+                    float dead_barrier);
+/* Straight ropes from roots (RopeBatch(num_envs, verts_per_rope, root_pos, seg_len, dir, ...),
+ * bindings.cpp:736-767 / batch.cu:343-350): vertex v of rope e at root_e + v * seg_len * dir. */
+RS_API int rs_batch_create_straight(rs_batch** out, int num_ropes, int verts_per_rope, const float* root_pos,
+                             float seg_len, const float* dir3, float density, float k_stretch, float k_bend,
+                             float max_h, int num_itr, int fix_root_orientation, float dead_radius,
+                             float dead_barrier);
+RS_API int rs_batch_destroy(rs_batch* b);
+
+/* ---------------------------------------------------------------- knobs (MetaData fields)
+ * Replaces the property setters/getters of bindings.cpp:535-579 and :860-886. */
+enum rs_param {
+    RS_P_DRAG = 0,        /* linear velocity decay [1/s]            (meta.drag) */
+    RS_P_DRAG_QUAD = 1,   /* quadratic normal drag [1/m]            (meta.dragQuad) */
+    RS_P_DRAG_QUAD_T = 2, /* quadratic tangential drag [1/m]        (meta.dragQuadT) */
+    RS_P_DAMPING = 3,     /* YarnBall damping (enters as damping/h) (meta.damping) */
+    RS_P_ACCEL = 4,       /* local-solve relaxation                 (meta.accelerationRatio) */
+    RS_P_MAX_H = 5,       /* largest substep of advance()           (Sim::maxH) */
+    RS_P_TIME = 6         /* read-only accumulated time             (meta.time) */
+};
+RS_API int rs_batch_set_param(rs_batch* b, int which, float value);
+RS_API int rs_batch_get_param(rs_batch* b, int which, float* value);
+RS_API int rs_batch_set_num_itr(rs_batch* b, int num_itr);
+RS_API int rs_batch_get_num_itr(rs_batch* b, int* num_itr);
+RS_API int rs_batch_set_gravity(rs_batch* b, const float* g3);
+RS_API int rs_batch_get_gravity(rs_batch* b, float* g3);
+/* Bin size (CTA threads) of the packed layout; 0 = automatic. Used by the autotuner. */
+RS_API int rs_batch_set_block(rs_batch* b, int block);
+RS_API int rs_batch_layout(rs_batch* b, int* block, int* num_bins);
+/* 1 (default) = synchronise and read the status words after every frame (checkErrors). */
+RS_API int rs_batch_set_sync(rs_batch* b, int every_frame);
+
+/* ---------------------------------------------------------------- geometry / host state
+ * Replaces RopeSim's host getters and setters (bindings.cpp:303-462, :525-532) and RopeBatch's
+ * per-vertex property API (bindings.cpp:1109-1201). Arrays are caller order. */
+RS_API int rs_batch_num_verts(rs_batch* b, int* n, int* num_ropes);
+RS_API int rs_batch_rope_verts(rs_batch* b, int* rope_verts /* [num_ropes] */);
+RS_API int rs_batch_download(rs_batch* b, float* pos /*[n,3] or NULL*/, float* vel /*[n,3] or NULL*/,
+                      float* quat /*[n,4] or NULL*/);
+RS_API int rs_batch_inv_masses(rs_batch* b, float* out /* [n] */);
+RS_API int rs_batch_rest_lengths(rs_batch* b, float* out /* [n]; entry of a rope's last vertex unused */);
+RS_API int rs_batch_min_segment(rs_batch* b, float* out);
+/* per-vertex arrays [n]; entries of pinned vertices (masses) or of each rope's last vertex
+ * (EA, EI) are ignored */
+RS_API int rs_batch_set_masses(rs_batch* b, const float* masses);
+RS_API int rs_batch_set_stretch_stiffnesses(rs_batch* b, const float* ea);
+RS_API int rs_batch_set_bend_stiffnesses(rs_batch* b, const float* ei);
+RS_API int rs_batch_set_velocities(rs_batch* b, const float* vel /* host [n,3] */);
+/* RopeSim::set_root (bindings.cpp:324-350): q (already unit) may be NULL */
+RS_API int rs_batch_set_root(rs_batch* b, int rope, const float* pos3, const float* vel3, const float* q4);
+RS_API int rs_batch_unpin_root(rs_batch* b, int rope);
+RS_API int rs_batch_roots_pinned(rs_batch* b, int* pinned);
+
+/* ---------------------------------------------------------------- stepping
+ * One control frame = ONE persistent kernel launch over every substep.
+ * step_program replaces RopeBatch::step_program (batch.cu:321-363): p0, v0, p1 [R,3], q0, q1
+ * [R,4] or NULL; `on_host` = 1 when the pointers are host memory (copied in), else device.
+ * step_legacy replaces RopeBatch::step (batch.cu:288-319): p, v [R,3], q [R,4] or NULL.
+ * step_free replaces RopeBatch::step_free (batch.cu:388-398).
+ * advance replaces RopeSim::advance / Sim::advance (bindings.cpp:274-295, step.cpp:37-57):
+ * substeps = 0 runs the float ceil(dt / max_h) substeps. */
+RS_API int rs_batch_step_program(rs_batch* b, const float* p0, const float* v0, const float* p1, const float* q0,
+                          const float* q1, float dt, int substeps, int on_host);
+RS_API int rs_batch_step_legacy(rs_batch* b, const float* p, const float* v, const float* q, float dt, int substeps,
+                         int on_host);
+RS_API int rs_batch_step_free(rs_batch* b, float dt, int substeps);
+RS_API int rs_batch_advance(rs_batch* b, float dt, int substeps);
+/* RopeBatch::reset_envs (batch.cu:400-413): host ids[count] (rope indices) */
+RS_API int rs_batch_reset_ropes(rs_batch* b, const int* ids, int count);
+/* RopeSim::reset (bindings.cpp:303-316) */
+RS_API int rs_batch_reset_all(rs_batch* b);
+/* RopeBatch::gather (batch.cu:420-425) */
+RS_API int rs_batch_gather(rs_batch* b);
+/* Device views [n,3], [n,3], [n,4] (caller order), refreshed by every step/reset/gather;
+ * stable for the handle's life (RopeBatch::positions_ptr etc., batch.h:79-81). */
+RS_API int rs_batch_views(rs_batch* b, float** pos, float** vel, float** quat);
+/* Solver status (Sim::lastErrorCode / lastWarningCode, bindings.cpp:578-579) and a sticky
+ * flag raised when a frame produced a non-finite position. */
+RS_API int rs_batch_status(rs_batch* b, int* last_error, int* last_warning, int* nonfinite);
+/* CUDA stream the handle's device work runs on. */
+RS_API int rs_batch_stream(rs_batch* b, void** stream);
+/* Device time of the last frame kernel in ms (after rs_batch_set_timing(b, 1)). */
+RS_API int rs_batch_set_timing(rs_batch* b, int on);
+RS_API int rs_batch_last_frame_ms(rs_batch* b, double* ms);
+
+/* ---------------------------------------------------------------- surface contact
+ * set_contact / set_planes replace write_contact / write_planes (bindings.cpp:51-80): rows are
+ * [count <= 8, 4] = (n, w) half-spaces n.x >= w, normalised here. */
+RS_API int rs_batch_set_contact(rs_batch* b, float radius, float mu_s, float mu_k, float v_slip, float kappa);
+RS_API int rs_batch_get_contact(rs_batch* b, float* radius, float* mu_s, float* mu_k);
+RS_API int rs_batch_set_planes(rs_batch* b, int count, const float* rows);
+/* SdfStore::add (sdf.cu:137-158): values host [nx,ny,nz], pose rows host [rows,3]/[rows,4]
+ * (rows 1 or num_ropes). Returns the mesh index in *index. */
+RS_API int rs_batch_add_mesh(rs_batch* b, const float* values, int nx, int ny, int nz, const float* origin3,
+                      float spacing, float mu_s, float mu_k, const float* pos, const float* quat, int rows,
+                      int* index);
+RS_API int rs_batch_set_mesh_friction(rs_batch* b, int index, float mu_s, float mu_k);
+/* SdfStore::set_targets / set_targets_host (sdf.cu:165-189): index >= 0 with rows 1 or
+ * num_ropes, or index = -1 with [num_ropes, M] rows; tele [num_ropes] or NULL; tele_all;
+ * on_device = 1 when pos/quat/tele are device memory. */
+RS_API int rs_batch_set_mesh_poses(rs_batch* b, int index, const float* pos, const float* quat, int rows,
+                            const uint8_t* tele, int tele_all, int on_device);
+RS_API int rs_batch_clear_meshes(rs_batch* b);
+RS_API int rs_batch_num_meshes(rs_batch* b, int* count);
+RS_API int rs_batch_enable_contact_forces(rs_batch* b, int on);
+/* averaged over the last frame: forces [n,3] ON each vertex; wrenches [num_ropes, M, 6] BY the
+ * rope ON each mesh (SdfStore::contact_forces / wrenches, sdf.cu:255-270) */
+RS_API int rs_batch_contact_forces(rs_batch* b, float* out);
+RS_API int rs_batch_mesh_wrenches(rs_batch* b, float* out);
+/* device views [n,3] and [num_ropes, 64, 6] (contact_forces_view / mesh_wrenches_view) */
+RS_API int rs_batch_contact_views(rs_batch* b, float** forces, float** wrenches);
+
+/* ---------------------------------------------------------------- measurement
+ * Measured FP32 FMA throughput of the current device in TFLOP/s (2 FLOP per FMA), from a
+ * kernel of independent FMA chains (no counterpart in the reference; bench.py uses it as the
+ * roofline peak of the FP32-bound frame kernel). */
+RS_API int rs_probe_fp32_peak(double* tflops, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROPESIM_B200_H */
