@@ -297,6 +297,8 @@ def run_ours(args):
     value = world * vs_per_rank / (total_ms * 1e-3)
 
     # ---- end-to-end leg: host inputs in, host positions out, through the public API
+    if args.no_e2e:
+        frames = args.warmup  # no e2e frames
     hp0 = torch.as_tensor(p0).pin_memory()
     hv0 = torch.as_tensor(v0).pin_memory()
     hp1 = torch.as_tensor(p1).pin_memory()
@@ -318,7 +320,7 @@ def run_ours(args):
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * vs_per_rank / e2e_s
+    e2e_value = world * vs_per_rank / e2e_s if not args.no_e2e else None
     h2d = 3 * N_ROPES * 3 * 4
     d2h = N_ROPES * V * 3 * 4
 
@@ -360,15 +362,19 @@ def run_ours(args):
 
 
 def main():
+    global N_ROPES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ropes", type=int, default=N_ROPES, help="ropes per GPU (profiling of smaller cases)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    N_ROPES = args.ropes
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -53,8 +53,21 @@ __device__ __forceinline__ f3 qrot(float4 q, f3 v) {
     const float c = dot(v, qv);
     return a * q.w + cross(qv, a) + qv * c;
 }
-// q * e1: the tangent of the segment frame.
-__device__ __forceinline__ f3 qtangent(float4 q) { return qrot(q, mk3(1.f, 0.f, 0.f)); }
+// q * e1, the tangent of the segment frame: qrot(q, e1) with the zero terms of e1 dropped
+// (a = (w, z, -y), c = x; exact, as multiplying by 1 and adding 0 are).
+__device__ __forceinline__ f3 qtangent(float4 q) {
+    const f3 qv = xyz(q);
+    const f3 a = mk3(q.w, q.z, -q.y);
+    return a * q.w + cross(qv, a) + qv * q.x;
+}
+// (v, 0) * b for a pure vector v: the rotor product with the zero scalar's terms dropped.
+__device__ __forceinline__ float4 qmul_pure(f3 v, float4 b) {
+    const f3 bv = xyz(b);
+    const f3 r = v * b.w + cross(v, bv);
+    return make_float4(r.x, r.y, r.z, -dot(v, bv));
+}
+// c * (1, 0, 0, 0): a signed permutation of c's components.
+__device__ __forceinline__ float4 qmul_e1(float4 c) { return make_float4(c.w, c.z, -c.y, -c.x); }
 
 // Symmetric 3x3: diag (xx, yy, zz), upper (xy, xz, yz).
 struct sym3 {

@@ -38,6 +38,15 @@ struct FrameSmem {
 
 constexpr int kPoseF4 = 5;  // float4 per cached pose
 
+// Surface-contact variants of the frame kernel: none, planes only, planes + SDF meshes.
+enum : int { SURF_NONE = 0, SURF_PLANES = 1, SURF_MESHES = 2 };
+
+// Resident CTAs per SM the register allocation targets: 768 threads per SM (<= 85
+// registers) without meshes, 512 threads per SM (<= 128 registers) with meshes.
+#ifndef RS_MIN_BLOCKS
+#define RS_MIN_BLOCKS(B, SURF) ((B) <= 256 ? (((SURF) == SURF_MESHES ? 512 : 768) / (B)) : 1)
+#endif
+
 __device__ __forceinline__ uint64_t all_meshes(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
 
 // Shortest-arc SLERP with an nlerp fallback above dot 0.9995, batch.cu:106-114.
@@ -57,6 +66,7 @@ __device__ __forceinline__ float4 unit_or_identity(const float* q) {
 
 // Surfaces (planes, then candidate meshes in ascending index) at one probe point,
 // contact.cuh:141-163; `wr` != nullptr turns it into the readout (contact.cuh:172-204).
+template <int SURF>
 __device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
                                          float h, f3& f, sym3& H, float* wr, f3* facc) {
     for (int pl = 0; pl < a.num_planes; pl++) {
@@ -66,6 +76,7 @@ __device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache
         if (gap >= 0.f) continue;
         surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
     }
+    if constexpr (SURF != SURF_MESHES) return;
     for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
         const int m = __ffsll((long long)mm) - 1;
         const PoseV P = load_pose(cache + m * kPoseF4);
@@ -88,8 +99,8 @@ __device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache
     }
 }
 
-template <int BLOCK, bool SURF>
-__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(const FrameArgs a) {
+template <int BLOCK, int SURF>
+__global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kernel(const FrameArgs a) {
     extern __shared__ float4 dyn_smem[];  // FrameSmem<BLOCK>, then the pose cache [2][pose_cache][kPoseF4]
     FrameSmem<BLOCK>& sm = *reinterpret_cast<FrameSmem<BLOCK>*>(dyn_smem);
     float4* pose_smem = dyn_smem + sizeof(FrameSmem<BLOCK>) / sizeof(float4);
@@ -131,31 +142,21 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
     const float kc = kap * kap / im;
     const int S = a.substeps, I = a.iters;
 
-    // ---- root driving inputs (caller rope order)
-    f3 P0 = zero3(), V0 = zero3(), A = zero3();
-    float4 qa = q, qb = q;
-    if (isRoot && a.root_mode != ROOT_NONE) {
-        const float* row = a.prog + (size_t)env * 17;
-        P0 = mk3(row[0], row[1], row[2]);
-        V0 = mk3(row[3], row[4], row[5]);
-        if (a.root_mode == ROOT_PROGRAM) {
-            const f3 P1 = mk3(row[6], row[7], row[8]);
-            A = 2.f / (a.dt * a.dt) * ((P1 - P0) - V0 * a.dt);
-            if (a.has_q0) qa = unit_or_identity(row + 9);
-            if (a.has_q1) qb = unit_or_identity(row + 13);
-        } else {  // ROOT_SET: constant-velocity frame, batch.cu:90-104
-            p = P0;
-            v = V0;
-            if (a.has_q0) q = unit_or_identity(row + 9);
-        }
+    // ---- root driving (caller rope order). Program rows are re-read from L1 every substep
+    // instead of occupying registers of every thread for the whole frame.
+    const float* row = (isRoot && a.root_mode != ROOT_NONE) ? a.prog + (size_t)env * 17 : nullptr;
+    if (row && a.root_mode == ROOT_SET) {  // constant-velocity frame, batch.cu:90-104
+        p = mk3(row[0], row[1], row[2]);
+        v = mk3(row[3], row[4], row[5]);
+        if (a.has_q0) q = unit_or_identity(row + 9);
     }
 
     // ---- mesh pose cache (per CTA: its ropes x meshes)
-    const int nsdf = SURF ? a.num_sdf : 0;
+    const int nsdf = (SURF == SURF_MESHES) ? a.num_sdf : 0;
     const int nPose = bin.rcount * nsdf;
     float4* cache0 = pose_smem;
     float4* cache1 = pose_smem + (size_t)a.pose_cache * kPoseF4;
-    if constexpr (SURF) if (nsdf > 0 && !a.sdf_moving) {
+    if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && !a.sdf_moving) {
         for (int e = t; e < nPose; e += BLOCK) {
             const int r = e / nsdf, m = e % nsdf;
             const int en = a.ropes[bin.rstart + r].user;
@@ -166,27 +167,32 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
     }
     uint64_t cand = all_meshes(nsdf);  // the first substep of a frame visits every mesh
     f3 facc = zero3();
-    float* wrow = (SURF && a.forces_on && nsdf > 0) ? a.wrench + (size_t)env * kMaxSdf * 6 : nullptr;
+    float* wrow = (SURF == SURF_MESHES && a.forces_on && nsdf > 0) ? a.wrench + (size_t)env * kMaxSdf * 6 : nullptr;
 
     int cur = 0;
     if (act) sm.q[0][t] = q;
 
     for (int s = 0; s < S; s++) {
         // ---- root program of this substep, batch.cu:122-159
-        if (isRoot && a.root_mode == ROOT_PROGRAM) {
+        if (row && a.root_mode == ROOT_PROGRAM) {
+            const f3 P0 = mk3(__ldg(row), __ldg(row + 1), __ldg(row + 2));
+            const f3 V0 = mk3(__ldg(row + 3), __ldg(row + 4), __ldg(row + 5));
+            const f3 P1 = mk3(__ldg(row + 6), __ldg(row + 7), __ldg(row + 8));
+            const f3 A = 2.f / (a.dt * a.dt) * ((P1 - P0) - V0 * a.dt);
             const float tau = float(s) * h;
             p = P0 + V0 * tau + 0.5f * tau * tau * A;
             v = V0 + (tau + 0.5f * h) * A;
             if (a.has_q0) {
-                float4 qq = a.has_q1 ? slerp4(qa, qb, float(s + 1) / float(S)) : qa;
+                const float4 qa = unit_or_identity(row + 9);
+                float4 qq = a.has_q1 ? slerp4(qa, unit_or_identity(row + 13), float(s + 1) / float(S)) : qa;
                 const float l2 = dot4(qq, qq);
                 q = (l2 > 0.f) ? scale4(qq, rsqrtf(l2)) : make_float4(0.f, 0.f, 0.f, 1.f);
                 sm.q[cur][t] = q;
             }
         }
         // ---- kinematic mesh poses of this substep, iteration.cu:12-33
-        float4* cache = (SURF && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
-        if constexpr (SURF) if (nsdf > 0 && a.sdf_moving) {
+        float4* cache = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
+        if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_moving) {
             const float al = float(s + 1) / float(S);
             const float invDt = 1.f / (float(S) * h);
             for (int e = t; e < nPose; e += BLOCK) {
@@ -245,8 +251,8 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
             // ---- position step, cosserat.cu:37-193
             f3 f = (y - dx) * fm;
             sym3 H = sym_diag(Hd);
-            if (SURF && im != 0.f && (a.num_planes > 0 || nsdf > 0))
-                surfaces(a, mycache, cand, p, dx, kc, h, f, H, nullptr, nullptr);
+            if (SURF != SURF_NONE && im != 0.f)
+                surfaces<SURF>(a, mycache, cand, p, dx, kc, h, f, H, nullptr, nullptr);
             f3 f2 = zero3();
             sym3 H2 = sym_zero();
             if (hasNext) {
@@ -275,25 +281,24 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
             if (act) sm.dx[t] = f4(dx, 0.f);
             __syncthreads();  // B2
 
-            // ---- frame step, cosserat.cu:242-272
+            // ---- frame step, cosserat.cu:242-272. The reference's sign tests
+            // dot((q_{i-1}^-1 q_i), r_{i-1}) and dot((q_i^-1 q_{i+1}), r_i) equal
+            // dot(q_i, q_{i-1} r_{i-1}) and dot(q_i, q_{i+1} r_i^*) (Re(xy) = Re(yx) for
+            // quaternions), so they reuse the products that b needs.
             if (!(fl & F_FIX_ORIENT) && hasNext) {
                 const f3 p1dx = xyz(sm.dx[t + 1]);
-                f3 vv = ((p1 - p) + (p1dx - dx)) / lr;
-                vv *= -2.f * ks;
+                const f3 vv = (((p1 - p) + (p1dx - dx)) * invl) * (-2.f * ks);
                 float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
-                const float4 q0 = q;
                 if (hasPrev) {
-                    const float4 qq = sm.q[cur][t - 1];
-                    const float sg = dot4(qmul(qconj(qq), q0), qrp) > 0.f ? 1.f : -1.f;
-                    b = add4(b, scale4(qmul(qq, qrp), sg));
+                    const float4 pr = qmul(sm.q[cur][t - 1], qrp);
+                    b = scale4(pr, dot4(q, pr) > 0.f ? 1.f : -1.f);
                 }
                 if (fl & F_NEXT_ORIENT) {
-                    const float4 qq = sm.q[cur][t + 1];
-                    const float sg = dot4(qmul(qconj(q0), qq), qro) > 0.f ? 1.f : -1.f;
-                    b = add4(b, scale4(qmul(qq, qconj(qro)), sg));
+                    const float4 nx = qmul(sm.q[cur][t + 1], qconj(qro));
+                    b = add4(b, scale4(nx, dot4(q, nx) > 0.f ? 1.f : -1.f));
                 }
                 const float lambda = len(vv) + sqrtf(dot4(b, b));
-                const float4 m = qmul(qmul(f4(vv, 0.f), b), make_float4(1.f, 0.f, 0.f, 0.f));
+                const float4 m = qmul_e1(qmul_pure(vv, b));
                 q = normalize4(add4(m, scale4(b, lambda)));
             }
             if (act) sm.q[cur ^ 1][t] = q;
@@ -314,17 +319,17 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
                 vv = vn + vt2;
             }
             v = vv * (1.f - a.drag * h);
-            if (SURF && a.forces_on && (a.num_planes > 0 || nsdf > 0)) {
+            if (SURF != SURF_NONE && a.forces_on) {
                 // planes accumulate into fv; each mesh's force is added to fv and its wrench
                 // goes to the (env, mesh) row, contact.cuh:172-204
                 f3 fv = zero3();
                 sym3 Hs = sym_zero();
-                surfaces(a, mycache, cand, p, dx, kc, h, fv, Hs, wrow, &fv);
+                surfaces<SURF>(a, mycache, cand, p, dx, kc, h, fv, Hs, wrow, &fv);
                 facc += fv;
             }
         }
         p += dx;
-        if (SURF && nsdf > 0) {
+        if (SURF == SURF_MESHES && nsdf > 0) {
             if (im != 0.f) {
                 const float pad = 2.f * len(dx) + 0.02f;
                 uint64_t mask = 0ull;
@@ -356,7 +361,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
         float* ov = a.out_vel + (size_t)uidx * 3;
         ov[0] = v.x; ov[1] = v.y; ov[2] = v.z;
         reinterpret_cast<float4*>(a.out_q)[uidx] = q;
-        if (SURF && a.forces_on && a.out_force) {
+        if (SURF != SURF_NONE && a.forces_on && a.out_force) {
             const float k = 1.f / float(S);
             float* of = a.out_force + (size_t)uidx * 3;
             of[0] = facc.x * k; of[1] = facc.y * k; of[2] = facc.z * k;
@@ -366,7 +371,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 2 : 1)) frame_kernel(co
 }
 
 // ------------------------------------------------------------------ launch
-template <int BLOCK, bool SURF>
+template <int BLOCK, int SURF>
 static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_bytes, cudaStream_t s) {
     auto k = frame_kernel<BLOCK, SURF>;
     const size_t dyn_smem = sizeof(FrameSmem<BLOCK>) + pose_bytes;
@@ -378,15 +383,21 @@ static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_
     return cudaGetLastError();
 }
 
+template <int BLOCK>
+static cudaError_t launch_frame_b(const FrameArgs& a, int num_bins, cudaStream_t s) {
+    if (a.num_sdf > 0)
+        return launch_frame_t<BLOCK, SURF_MESHES>(a, num_bins, (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4), s);
+    if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES>(a, num_bins, 0, s);
+    return launch_frame_t<BLOCK, SURF_NONE>(a, num_bins, 0, s);
+}
+
 cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s) {
-    const bool surf = a.num_planes > 0 || a.num_sdf > 0;
-    const size_t dyn = surf && a.num_sdf > 0 ? (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4) : 0;
     switch (block) {
-        case 64: return surf ? launch_frame_t<64, true>(a, num_bins, dyn, s) : launch_frame_t<64, false>(a, num_bins, dyn, s);
-        case 128: return surf ? launch_frame_t<128, true>(a, num_bins, dyn, s) : launch_frame_t<128, false>(a, num_bins, dyn, s);
-        case 256: return surf ? launch_frame_t<256, true>(a, num_bins, dyn, s) : launch_frame_t<256, false>(a, num_bins, dyn, s);
-        case 512: return surf ? launch_frame_t<512, true>(a, num_bins, dyn, s) : launch_frame_t<512, false>(a, num_bins, dyn, s);
-        case 1024: return surf ? launch_frame_t<1024, true>(a, num_bins, dyn, s) : launch_frame_t<1024, false>(a, num_bins, dyn, s);
+        case 64: return launch_frame_b<64>(a, num_bins, s);
+        case 128: return launch_frame_b<128>(a, num_bins, s);
+        case 256: return launch_frame_b<256>(a, num_bins, s);
+        case 512: return launch_frame_b<512>(a, num_bins, s);
+        case 1024: return launch_frame_b<1024>(a, num_bins, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -344,11 +344,17 @@ class RopeBatch(_Common):
                                  int(group_ropes))
 
     def _per_vertex(self, arr, ncols):
+        """Per-rope rows of a per-vertex array: [V] (one profile for every rope) or [N, V] for
+        uniform batches, or a flat caller-order [total_verts] array for uneven ropes."""
         arr = np.asarray(arr, np.float32)
         N = len(self._verts)
+        uniform = len(set(self._verts)) == 1
         out = []
         for r in range(N):
-            row = arr if arr.ndim == 1 else arr[r]
+            if not uniform:
+                row = arr[self._starts[r]:self._starts[r + 1]]
+            else:
+                row = arr if arr.ndim == 1 else arr[r]
             out.append(row[:ncols(r)])
         return out
 

@@ -101,22 +101,24 @@ def test_program_config2_noise_floor(mods):
 
 
 def test_uneven_mesh_contact_noise_floor(mods):
+    """Uneven ropes teleport-hit by meshes in the first frame: contact-rich from the start, so
+    positions and the force/wrench readout are held to the FP32 noise floor of the oracle."""
     rs, orc = mods
     from ropesim import sdf
 
     g, gf, gw, _ = S.uneven(rs, sdf, to_dev=to_dev)
     o, of, ow, _ = S.uneven(orc, sdf, to_dev=host, precision="f64")
-    o32, _, _, _ = S.uneven(orc, sdf, to_dev=host, precision="f32")
+    o32, of32, ow32, _ = S.uneven(orc, sdf, to_dev=host, precision="f32")
     d, d32 = dev(g, o), dev(o32, o)
     print(f"\n  uneven ropes + planes + meshes (6 ropes, 10 frames): gpu-f64 {d:.2e} m, f32-f64 {d32:.2e} m, "
-          f"first frame {dev(g[0], o[0]):.2e} m; |F| max {np.abs(of).max():.1f} N")
-    assert dev(g[0], o[0]) <= TOL
+          f"first frame {dev(g[0], o[0]):.2e} m (f32 {dev(o32[0], o[0]):.2e}); |F| max {np.abs(of).max():.1f} N, "
+          f"force dev gpu {np.abs(gf - of).max():.3f} N (f32 {np.abs(of32 - of).max():.3f}), "
+          f"wrench dev gpu {np.abs(gw - ow).max():.3f} (f32 {np.abs(ow32 - ow).max():.3f})")
+    assert dev(g[0], o[0]) <= 4.0 * dev(o32[0], o[0]) + 1e-6
     assert d <= 4.0 * d32 + 1e-6
-    # readout of the first frame: forces and wrenches agree to the force scale's rounding
-    fscale = max(1.0, np.abs(of[0]).max())
-    assert np.abs(gf[0] - of[0]).max() <= 1e-3 * fscale
-    wscale = max(1.0, np.abs(ow[0]).max())
-    assert np.abs(gw[0] - ow[0]).max() <= 1e-3 * wscale
+    assert np.abs(gf[0] - of[0]).max() <= 4.0 * np.abs(of32[0] - of[0]).max() + 1e-3
+    assert np.abs(gw[0] - ow[0]).max() <= 4.0 * np.abs(ow32[0] - ow[0]).max() + 1e-3
+    assert np.abs(ow).max() > 0.0 and np.abs(of).max() > 0.0  # the readout saw contact
 
 
 def test_bitwise_replay_and_block_invariance(mods):
