@@ -256,6 +256,8 @@ def run_ours(args):
     pos, p0, v0, p1 = c2_inputs(N_ROPES, frames, 1234 + rank)
     b = ropesim.RopeBatch.from_positions(pos, 0.117, 11473.0, 4.48e-3, H, ITERS, deterministic=True)
     configure(b)
+    if args.block:
+        b.set_block(args.block)
     b.set_timing(True)
     dev = torch.device("cuda", local)
     P0 = torch.as_tensor(p0, device=dev)
@@ -324,6 +326,36 @@ def run_ours(args):
     h2d = 3 * N_ROPES * 3 * 4
     d2h = N_ROPES * V * 3 * 4
 
+    # ---- plain path: the same frames through the per-substep-launch engine (the reference's
+    # launch structure, in-repo), same inputs and device timing
+    plain = None
+    if not args.no_plain:
+        pb = ropesim.RopeBatch.from_positions(pos, 0.117, 11473.0, 4.48e-3, H, ITERS, deterministic=True)
+        configure(pb)
+        pb.set_engine("plain")
+        pstream = torch.cuda.ExternalStream(pb.stream_ptr())
+        for f in range(args.warmup):
+            pb.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
+        torch.cuda.synchronize()
+        pms = []
+        nplain = min(args.steps, 3)
+        for f in range(args.warmup, args.warmup + nplain):
+            flush.fill_(float(f))
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(pstream)
+            pb.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
+            e1.record(pstream)
+            e1.synchronize()
+            pms.append(e0.elapsed_time(e1))
+        pvalue = N_ROPES * V * S * nplain / (sum(pms) * 1e-3)
+        plain = {"value": pvalue, "unit": METRIC, "ms_per_step": sum(pms) / nplain, "steps": nplain,
+                 "launches_per_step": S * (3 + 2 * ITERS) + 1, "speedup_of_persistent": value / world / pvalue,
+                 "note": "per-substep-launch plain path (reference launch structure, in-repo; the reference's own "
+                         "CUDA build is unavailable)"}
+        del pb
+
     if rank == 0:
         peaks, source = measured_peaks()
         tf = ctypes.c_double(0)
@@ -351,6 +383,7 @@ def run_ours(args):
                                       "achieved_gbs": state_bytes / (avg_kernel_ms * 1e-3) / 1e9,
                                       "peak_gbs": peaks.get("hbm_gbs"), "peak_source": source}},
             "kernel_ms_per_frame": avg_kernel_ms,
+            "plain_path": plain,
             "clocks": sampler.summary(),
         }
         if world == 1 and not args.no_cpu:
@@ -371,6 +404,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ropes", type=int, default=N_ROPES, help="ropes per GPU (profiling of smaller cases)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
+    ap.add_argument("--block", type=int, default=0, help="bin size (CTA threads); 0 = the library's choice")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

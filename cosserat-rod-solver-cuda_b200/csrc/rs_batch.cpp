@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <numeric>
 
 #include "rs_kernels.h"
@@ -106,6 +107,11 @@ Batch::~Batch() {
                     d_tele_, d_motion_, d_poses_, d_stage_, d_stage_tele_, d_force_, d_wrench_};
     for (void* p : bufs)
         if (p) cudaFree(p);
+    if (pl_graph_) cudaGraphExecDestroy(pl_graph_);
+    void* pbufs[] = {pl_.dx, pl_.dxn, pl_.y, pl_.qprev, pl_.lpos, pl_.facc, pl_.cand, pl_.spose, d_pl_args_};
+    for (void* p : pbufs)
+        if (p) cudaFree(p);
+    if (h_pl_args_) cudaFreeHost(h_pl_args_);
     if (h_prog_) cudaFreeHost(h_prog_);
     if (h_status_) cudaFreeHost(h_status_);
     if (ev0_) cudaEventDestroy(ev0_);
@@ -182,7 +188,7 @@ int Batch::pose_cache_entries() const { return std::max(1, max_rcount_ * (int)gr
 void Batch::pack() {
     int maxV = 0;
     for (int r = 0; r < R_; r++) maxV = std::max(maxV, rope_verts(r));
-    int blk = block_override;
+    int blk = block_override ? block_override : tune_block_;
     if (blk == 0) {
         blk = std::max(64, next_pow2(maxV));
         if (blk < 256 && (long long)n_ > 148LL * blk) blk = 256;
@@ -481,10 +487,132 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     a.pose_cache = pose_cache_entries();
     a.poses = d_poses_; a.motion = d_motion_;
     for (int m = 0; m < (int)grids_.size(); m++) a.grids[m] = grids_[m];
-    if (timing_) check(cudaEventRecord(ev0_, stream_), "event");
-    check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
-    if (timing_) check(cudaEventRecord(ev1_, stream_), "event");
+    const bool timed = timing_ || tuning();
+    if (timed) check(cudaEventRecord(ev0_, stream_), "event");
+    if (engine_ == 1) run_frame_plain(a);
+    else check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
+    if (timed) check(cudaEventRecord(ev1_, stream_), "event");
     host_dyn_valid_ = false;
+}
+
+// ------------------------------------------------------------------ plain engine
+void Batch::set_engine(int e) {
+    if (e != 0 && e != 1) throw std::invalid_argument("engine must be 0 (persistent) or 1 (plain)");
+    engine_ = e;
+    if (e == 1) autotune_ = false;
+}
+
+void Batch::plain_alloc() {
+    if (pl_.dx) return;
+    const size_t n4 = sizeof(float4) * n_;
+    check(cudaMalloc(&pl_.dx, n4), "cudaMalloc(plain dx)");
+    check(cudaMalloc(&pl_.dxn, n4), "cudaMalloc(plain dxn)");
+    check(cudaMalloc(&pl_.y, n4), "cudaMalloc(plain y)");
+    check(cudaMalloc(&pl_.qprev, n4), "cudaMalloc(plain qprev)");
+    check(cudaMalloc(&pl_.lpos, n4), "cudaMalloc(plain lpos)");
+    check(cudaMalloc(&pl_.facc, n4), "cudaMalloc(plain facc)");
+    check(cudaMemset(pl_.facc, 0, n4), "memset(plain facc)");
+    check(cudaMalloc(&pl_.cand, sizeof(uint64_t) * n_), "cudaMalloc(plain cand)");
+    check(cudaMalloc(&pl_.spose, sizeof(Pose) * (size_t)R_ * kMaxSdf), "cudaMalloc(plain poses)");
+    check(cudaMalloc(&d_pl_args_, sizeof(FrameArgs)), "cudaMalloc(plain args)");
+    check(cudaMallocHost(&h_pl_args_, sizeof(FrameArgs)), "cudaMallocHost(plain args)");
+}
+
+// One frame of the plain path: parameters uploaded once (uploadMeta, YarnBall.cu:261-272),
+// then per substep the root / pose / init launches and one replay of the captured iterations.
+void Batch::run_frame_plain(const FrameArgs& a) {
+    plain_alloc();
+    check(cudaStreamSynchronize(stream_), "plain args reuse");  // the previous frame read h_pl_args_
+    *h_pl_args_ = a;
+    check(cudaMemcpyAsync(d_pl_args_, h_pl_args_, sizeof(FrameArgs), cudaMemcpyHostToDevice, stream_), "upload(args)");
+    const int surf = a.num_sdf > 0 ? 2 : (a.num_planes > 0 ? 1 : 0);
+    const std::string key = std::to_string(a.iters) + ":" + std::to_string(surf);
+    if (!pl_graph_ || key != pl_graph_key_) {
+        if (pl_graph_) { cudaGraphExecDestroy(pl_graph_); pl_graph_ = nullptr; }
+        cudaGraph_t graph;
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+        const cudaError_t rec = plain_record_inner(d_pl_args_, pl_, n_, a.iters, surf, stream_);
+        check(cudaStreamEndCapture(stream_, &graph), "end capture");
+        check(rec, "record plain iterations");
+        check(cudaGraphInstantiate(&pl_graph_, graph, 0), "instantiate plain graph");
+        cudaGraphDestroy(graph);
+        pl_graph_key_ = key;
+    }
+    for (int s = 0; s < a.substeps; s++) {
+        check(plain_launch_pre(d_pl_args_, pl_, n_, R_, R_, a.num_sdf, a.sdf_moving != 0, a.root_mode, s, stream_),
+              "plain substep prologue");
+        check(cudaGraphLaunch(pl_graph_, stream_), "plain graph launch");
+    }
+    check(plain_launch_finish(d_pl_args_, pl_, n_, stream_), "plain frame end");
+}
+
+// ------------------------------------------------------------------ autotuner
+namespace {
+std::mutex g_tune_mtx;
+std::map<std::string, int> g_tune_cache;  // workload signature -> bin size
+}  // namespace
+
+std::string Batch::tune_key() const {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int maxV = 0;
+    for (int r = 0; r < R_; r++) maxV = std::max(maxV, rope_verts(r));
+    const int surf = grids_.empty() ? (num_planes_ > 0 ? 1 : 0) : 2;
+    return std::to_string(dev) + ":" + std::to_string(n_) + ":" + std::to_string(R_) + ":" + std::to_string(maxV) + ":" +
+           std::to_string(surf) + ":" + std::to_string(grids_.size()) + ":" + std::to_string(num_itr);
+}
+
+void Batch::tune_before_frame() {
+    if (!tuning()) return;
+    if (tune_cands_.empty()) {
+        {
+            std::lock_guard<std::mutex> g(g_tune_mtx);
+            auto it = g_tune_cache.find(tune_key());
+            if (it != g_tune_cache.end()) {
+                tuned_ = true;
+                if (it->second != block_) { tune_block_ = it->second; ensure_host(); layout_valid_ = false; device_valid_ = false; ensure_device(); }
+                return;
+            }
+        }
+        int maxV = 0;
+        for (int r = 0; r < R_; r++) maxV = std::max(maxV, rope_verts(r));
+        const int lo = std::max(64, next_pow2(maxV));
+        const int hi = std::max(256, lo);
+        for (int b = lo; b <= hi && b <= 1024; b *= 2) tune_cands_.push_back(b);
+        if (tune_cands_.size() < 2) { tuned_ = true; return; }
+    }
+    const int k = (int)tune_log_.size();
+    if (k < (int)tune_cands_.size() && tune_cands_[k] != block_) {
+        tune_block_ = tune_cands_[k];
+        ensure_host();
+        layout_valid_ = false;
+        device_valid_ = false;
+        ensure_device();
+    }
+}
+
+void Batch::tune_after_frame() {
+    if (!tuning() || tune_cands_.empty()) return;
+    check(cudaEventSynchronize(ev1_), "tune sync");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed");
+    tune_log_.push_back({block_, (double)ms});
+    if (tune_log_.size() < tune_cands_.size()) return;
+    auto best = std::min_element(tune_log_.begin(), tune_log_.end(),
+                                 [](const std::pair<int, double>& x, const std::pair<int, double>& y) { return x.second < y.second; });
+    tuned_ = true;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mtx);
+        g_tune_cache[tune_key()] = best->first;
+    }
+    if (best->first != block_) {
+        tune_block_ = best->first;
+        ensure_host();
+        layout_valid_ = false;
+        device_valid_ = false;
+        ensure_device();
+        gather();
+    }
 }
 
 void Batch::sdf_begin() {
@@ -514,12 +642,14 @@ void Batch::sdf_end(int substeps) {
 
 void Batch::step_program(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1, float dt,
                          int substeps, bool host_inputs) {
+    tune_before_frame();
     ensure_device();
     stage_rows(p0, v0, p1, q0, q1, host_inputs);
     sdf_begin();
     run_frame(ROOT_PROGRAM, q0 != nullptr, q1 != nullptr, dt, substeps, dt / (float)substeps);
     time_ += dt;
     sdf_end(substeps);
+    tune_after_frame();
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");
@@ -539,6 +669,7 @@ void Batch::step_program(const float* p0, const float* v0, const float* p1, cons
 }
 
 void Batch::step_legacy(const float* p, const float* v, const float* q, float dt, int substeps, bool host_inputs) {
+    tune_before_frame();
     ensure_device();
     stage_rows(p, v, nullptr, q, nullptr, host_inputs);
     sdf_begin();
@@ -549,6 +680,7 @@ void Batch::step_legacy(const float* p, const float* v, const float* q, float dt
     run_frame(ROOT_SET, q != nullptr, false, dt, steps, dt / (float)steps);
     time_ += dt;
     sdf_end(substeps);
+    tune_after_frame();
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");
@@ -562,11 +694,13 @@ void Batch::step_legacy(const float* p, const float* v, const float* q, float dt
 }
 
 void Batch::step_free(float dt, int substeps) {
+    tune_before_frame();
     ensure_device();
     sdf_begin();
     run_frame(ROOT_NONE, false, false, dt, substeps, dt / (float)substeps);
     time_ += dt;
     sdf_end(substeps);
+    tune_after_frame();
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");
@@ -577,6 +711,7 @@ void Batch::step_free(float dt, int substeps) {
 // Sim::advance (step.cpp:37-57) with bindings.cpp:274-295's explicit-substep bias.
 void Batch::advance(float dt, int substeps) {
     if (!(dt > 0.f)) return;
+    tune_before_frame();
     ensure_device();
     sdf_begin();
     const float mh = substeps > 0 ? (dt / (float)substeps) * 1.000001f : max_h;
@@ -585,6 +720,7 @@ void Batch::advance(float dt, int substeps) {
     run_frame(ROOT_NONE, false, false, dt, steps, dt / (float)steps);
     time_ += dt;
     sdf_end(substeps > 0 ? substeps : steps);
+    tune_after_frame();
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");

@@ -58,7 +58,7 @@ public:
     float drag = 0.2f, drag_quad = 0.f, drag_quad_t = 0.f, damping = 1e-6f, accel = 1.f;
     int num_itr = 8;
     float max_h = 1e-3f;
-    int block_override = 0;  // 0 = automatic bin size
+    int block_override = 0;  // 0 = automatic bin size (autotuned over the first frames)
     bool sync_every_frame = true;
 
     // ---- host-side edits (download-modify-upload of the caller-order mirror)
@@ -122,6 +122,16 @@ public:
     int num_bins() const { return (int)bins_.size(); }
     double last_frame_ms() const { return last_frame_ms_; }
     void set_timing(bool on) { timing_ = on; }
+    // Autotuner: while on (default with an automatic bin size), the first frames run one
+    // candidate bin size each (results are bitwise identical across bin sizes), then the
+    // fastest is kept and remembered for this workload signature in this process.
+    void set_autotune(bool on) { autotune_ = on; }
+    // Engine: 0 = one persistent launch per frame (default), 1 = the per-substep-launch plain
+    // path (root, init, num_itr x (position, frame), end kernels per substep, graph-replayed).
+    void set_engine(int e);
+    int engine() const { return engine_; }
+    bool tuning() const { return autotune_ && block_override == 0 && !tuned_; }
+    const std::vector<std::pair<int, double>>& tune_log() const { return tune_log_; }
 
 private:
     void configure(float density);
@@ -177,6 +187,21 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     bool timing_ = false;
     double last_frame_ms_ = 0.0;
+    bool autotune_ = true, tuned_ = false;
+    int engine_ = 0;
+    PlainBufs pl_{};
+    FrameArgs* d_pl_args_ = nullptr;
+    FrameArgs* h_pl_args_ = nullptr;   // pinned staging of the frame parameters
+    cudaGraphExec_t pl_graph_ = nullptr;
+    std::string pl_graph_key_;
+    void plain_alloc();
+    void run_frame_plain(const FrameArgs& a);
+    std::vector<int> tune_cands_;
+    std::vector<std::pair<int, double>> tune_log_;
+    int tune_block_ = 0;            // bin size chosen by the autotuner (0 = none yet)
+    void tune_before_frame();
+    void tune_after_frame();
+    std::string tune_key() const;
 
     // solver bookkeeping (YarnBall MetaData)
     float h_ = 1e-3f, last_h_ = 1e-3f, time_ = 0.f;

@@ -195,6 +195,20 @@ int rs_batch_layout(rs_batch* b, int* block, int* num_bins) {
         if (num_bins) *num_bins = s.num_bins();
     });
 }
+int rs_batch_set_autotune(rs_batch* b, int on) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_autotune(on != 0);
+    });
+}
+int rs_batch_set_engine(rs_batch* b, int engine) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_engine(engine);
+    });
+}
 int rs_batch_set_sync(rs_batch* b, int every_frame) {
     return guarded([&] {
         rs::Batch& s = B(b);

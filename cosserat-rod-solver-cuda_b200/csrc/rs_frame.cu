@@ -20,6 +20,7 @@
 
 #include "rs_device.cuh"
 #include "rs_kernels.h"
+#include "rs_substep.cuh"
 #include "rs_types.h"
 
 using namespace rsd;
@@ -33,71 +34,16 @@ struct FrameSmem {
     float4 q[2][BLOCK];   // frame rotors, double buffered across frame steps
     float4 fa[BLOCK];     // segment force on the next vertex (xyz) + H2.xx
     float4 fb[BLOCK];     // H2.yy, H2.zz, H2.xy, H2.xz
+    float4 qr[BLOCK];     // rest rotation of segment i (vertex i reads slots i-1 and i)
+    float4 lv[BLOCK];     // velocity at the previous substep's start (initial-guess extrapolation)
     float fc[BLOCK];      // H2.yz
 };
 
-constexpr int kPoseF4 = 5;  // float4 per cached pose
-
-// Surface-contact variants of the frame kernel: none, planes only, planes + SDF meshes.
-enum : int { SURF_NONE = 0, SURF_PLANES = 1, SURF_MESHES = 2 };
-
-// Resident CTAs per SM the register allocation targets: 768 threads per SM (<= 85
-// registers) without meshes, 512 threads per SM (<= 128 registers) with meshes.
+// Resident CTAs per SM the register allocation targets: 28 warps per SM (<= 72 registers;
+// 24 warps for 256-thread CTAs) without meshes, 16 warps per SM (<= 128 registers) with meshes.
 #ifndef RS_MIN_BLOCKS
-#define RS_MIN_BLOCKS(B, SURF) ((B) <= 256 ? (((SURF) == SURF_MESHES ? 512 : 768) / (B)) : 1)
+#define RS_MIN_BLOCKS(B, SURF) ((B) <= 256 ? (((SURF) == SURF_MESHES ? 512 : 896) / (B)) : 1)
 #endif
-
-__device__ __forceinline__ uint64_t all_meshes(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
-
-// Shortest-arc SLERP with an nlerp fallback above dot 0.9995, batch.cu:106-114.
-__device__ __forceinline__ float4 slerp4(float4 a, float4 b, float t) {
-    float d = dot4(a, b);
-    if (d < 0.f) { b = scale4(b, -1.f); d = -d; }
-    if (d > 0.9995f) return normalize4(add4(scale4(a, 1.f - t), scale4(b, t)));
-    const float th = acosf(fminf(d, 1.f));
-    const float s = sinf(th);
-    return add4(scale4(a, sinf((1.f - t) * th) / s), scale4(b, sinf(t * th) / s));
-}
-__device__ __forceinline__ float4 unit_or_identity(const float* q) {
-    float4 a = make_float4(q[0], q[1], q[2], q[3]);
-    const float l = dot4(a, a);
-    return (l > 0.f) ? scale4(a, rsqrtf(l)) : make_float4(0.f, 0.f, 0.f, 1.f);
-}
-
-// Surfaces (planes, then candidate meshes in ascending index) at one probe point,
-// contact.cuh:141-163; `wr` != nullptr turns it into the readout (contact.cuh:172-204).
-template <int SURF>
-__device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
-                                         float h, f3& f, sym3& H, float* wr, f3* facc) {
-    for (int pl = 0; pl < a.num_planes; pl++) {
-        const float4 P = a.planes[pl];
-        const f3 n = mk3(P.x, P.y, P.z);
-        const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
-        if (gap >= 0.f) continue;
-        surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
-    }
-    if constexpr (SURF != SURF_MESHES) return;
-    for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
-        const int m = __ffsll((long long)mm) - 1;
-        const PoseV P = load_pose(cache + m * kPoseF4);
-        f3 n, dRel;
-        float gap;
-        if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, n, gap, dRel)) continue;
-        if (wr) {
-            f3 fm = zero3();
-            sym3 Hs = sym_zero();
-            surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, fm, Hs);
-            *facc += fm;
-            const f3 r = (pos - P.pos) + d - n * a.c_radius;
-            const f3 tq = cross(r, -fm);
-            float* w = wr + m * 6;
-            atomicAdd(w + 0, -fm.x); atomicAdd(w + 1, -fm.y); atomicAdd(w + 2, -fm.z);
-            atomicAdd(w + 3, tq.x); atomicAdd(w + 4, tq.y); atomicAdd(w + 5, tq.z);
-        } else {
-            surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, f, H);
-        }
-    }
-}
 
 template <int BLOCK, int SURF>
 __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kernel(const FrameArgs a) {
@@ -110,48 +56,39 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
     const bool act = t < bin.vcount;
     const int dv = bin.vstart + t;
 
-    // ---- load this vertex (registers for the whole frame)
-    f3 p = zero3(), v = zero3(), lv = zero3();
+    // ---- load this vertex: dynamic state in registers for the whole frame, rest rotations
+    // and the previous substep's start velocity in shared memory
+    f3 p = zero3(), v = zero3();
     float im = 0.f, lr = 1.f, ks = 0.f;
-    float4 q = make_float4(0.f, 0.f, 0.f, 1.f), qrp = q, qro = q;
+    float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
     uint32_t fl = 0;
-    int lrope = 0, uidx = 0, env = 0;
+    int lrope = 0, env = 0;
     if (act) {
         const float4 a0 = a.pos[dv], a1 = a.vel[dv], a2 = a.lvel[dv];
         const int4 tp = a.topo[dv];
         p = xyz(a0); im = a0.w;
         v = xyz(a1); lr = a1.w;
-        lv = xyz(a2); ks = a2.w;
+        ks = a2.w;
+        sm.lv[t] = a2;
         q = a.q[dv];
-        qro = a.qrest[dv];
-        fl = (uint32_t)tp.x; lrope = tp.y; uidx = tp.z; env = tp.w;
-        if (fl & F_PREV) qrp = a.qrest[dv - 1];
+        sm.qr[t] = a.qrest[dv];
+        fl = (uint32_t)tp.x; lrope = tp.y; env = tp.w;
     }
     const bool hasNext = fl & F_NEXT, hasPrev = fl & F_PREV;
     const bool isRoot = (fl & F_ROOT) != 0;
-
+    const VConst c = vertex_constants(a, im, lr, ks);
     const float h = a.h;
-    const float invl = 1.f / lr;
-    const float Hd = 1.f / (im * h * h);
-    const float fm = 1.f / (h * h * im);
     const float damp = a.damping / h;
     const float invH = 1.f / h;
     const f3 g = mk3(a.gx, a.gy, a.gz);
     const float g2 = dot(g, g);
-    const float kap = a.c_kappa / h;
-    const float kc = kap * kap / im;
     const int S = a.substeps, I = a.iters;
 
-    // ---- root driving (caller rope order). Program rows are re-read from L1 every substep
-    // instead of occupying registers of every thread for the whole frame.
+    // ---- root driving (caller rope order); rows are re-read from L1 every substep
     const float* row = (isRoot && a.root_mode != ROOT_NONE) ? a.prog + (size_t)env * 17 : nullptr;
-    if (row && a.root_mode == ROOT_SET) {  // constant-velocity frame, batch.cu:90-104
-        p = mk3(row[0], row[1], row[2]);
-        v = mk3(row[3], row[4], row[5]);
-        if (a.has_q0) q = unit_or_identity(row + 9);
-    }
+    if (row && a.root_mode == ROOT_SET) root_set(a, row, p, v, q);
 
-    // ---- mesh pose cache (per CTA: its ropes x meshes)
+    // ---- mesh pose cache (per CTA: its ropes x meshes), double buffered across substeps
     const int nsdf = (SURF == SURF_MESHES) ? a.num_sdf : 0;
     const int nPose = bin.rcount * nsdf;
     float4* cache0 = pose_smem;
@@ -173,74 +110,24 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
     if (act) sm.q[0][t] = q;
 
     for (int s = 0; s < S; s++) {
-        // ---- root program of this substep, batch.cu:122-159
         if (row && a.root_mode == ROOT_PROGRAM) {
-            const f3 P0 = mk3(__ldg(row), __ldg(row + 1), __ldg(row + 2));
-            const f3 V0 = mk3(__ldg(row + 3), __ldg(row + 4), __ldg(row + 5));
-            const f3 P1 = mk3(__ldg(row + 6), __ldg(row + 7), __ldg(row + 8));
-            const f3 A = 2.f / (a.dt * a.dt) * ((P1 - P0) - V0 * a.dt);
-            const float tau = float(s) * h;
-            p = P0 + V0 * tau + 0.5f * tau * tau * A;
-            v = V0 + (tau + 0.5f * h) * A;
-            if (a.has_q0) {
-                const float4 qa = unit_or_identity(row + 9);
-                float4 qq = a.has_q1 ? slerp4(qa, unit_or_identity(row + 13), float(s + 1) / float(S)) : qa;
-                const float l2 = dot4(qq, qq);
-                q = (l2 > 0.f) ? scale4(qq, rsqrtf(l2)) : make_float4(0.f, 0.f, 0.f, 1.f);
-                sm.q[cur][t] = q;
-            }
+            root_program(a, row, s, S, h, p, v, q);
+            if (a.has_q0) sm.q[cur][t] = q;
         }
-        // ---- kinematic mesh poses of this substep, iteration.cu:12-33
         float4* cache = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
         if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_moving) {
-            const float al = float(s + 1) / float(S);
-            const float invDt = 1.f / (float(S) * h);
             for (int e = t; e < nPose; e += BLOCK) {
                 const int r = e / nsdf, m = e % nsdf;
-                const int en = a.ropes[bin.rstart + r].user;
-                const Motion M = a.motion[(size_t)en * kMaxSdf + m];
-                const f3 p0 = mk3(M.p0x, M.p0y, M.p0z), dp = mk3(M.dpx, M.dpy, M.dpz), rot = mk3(M.rx, M.ry, M.rz);
-                const float4 q0 = make_float4(M.qx, M.qy, M.qz, M.qw);
-                f3 Pp, Pv, Pw;
-                float4 Pq;
-                const float th = len(rot);
-                if (th > 0.f || dp.x != 0.f || dp.y != 0.f || dp.z != 0.f) {
-                    Pp = p0 + al * dp;
-                    float4 dq = make_float4(0.f, 0.f, 0.f, 1.f);
-                    if (th > 0.f) {
-                        const f3 ax = rot / th;
-                        const float hr = (al * th) * 0.5f;
-                        const float sn = sinf(hr);
-                        dq = make_float4(sn * ax.x, sn * ax.y, sn * ax.z, cosf(hr));
-                    }
-                    Pq = normalize4(qmul(dq, q0));
-                    Pv = dp * invDt;
-                    Pw = rot * invDt;
-                } else {
-                    Pp = p0; Pq = q0; Pv = zero3(); Pw = zero3();
-                }
-                const GridDesc& gd = a.grids[m];
-                const f3 lo_o = mk3(gd.ox, gd.oy, gd.oz);
-                const f3 hi_o = lo_o + mk3(float(gd.nx - 1), float(gd.ny - 1), float(gd.nz - 1)) * gd.h;
-                f3 lo, hi;
-                world_box(lo_o, hi_o, Pp, Pq, lo, hi);
-                store_pose(cache + e * kPoseF4, Pp, Pq, Pv, Pw, lo, hi);
+                compute_pose(a, a.ropes[bin.rstart + r].user, m, s, S, h, cache + e * kPoseF4);
             }
         }
         const float4* mycache = cache + lrope * nsdf * kPoseF4;
 
-        // ---- inertial prediction and initial guess, iteration.cu:34-68
-        const f3 vel0 = v;
-        f3 dx = vel0 * h;
-        const f3 lv_old = lv;
-        lv = vel0;
-        const f3 y = dx + g * (h * h);
-        if (im != 0.f && g2 > 0.f) {
-            const f3 acc = (vel0 - lv_old) / a.last_h;
-            const float sg = fminf(fmaxf(dot(acc, g) / g2, 0.f), 1.f);
-            dx += g * (h * h * sg);
-        }
+        // ---- inertial prediction and initial guess
+        f3 dx, y;
+        init_vertex(v, xyz(sm.lv[t]), im, h, a.last_h, g, g2, dx, y);
         if (act) {
+            sm.lv[t] = f4(v, 0.f);
             sm.p[t] = f4(p, 0.f);
             sm.dx[t] = f4(dx, 0.f);
         }
@@ -248,24 +135,11 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
         const f3 p1 = hasNext ? xyz(sm.p[t + 1]) : zero3();
 
         for (int it = 0; it < I; it++) {
-            // ---- position step, cosserat.cu:37-193
-            f3 f = (y - dx) * fm;
-            sym3 H = sym_diag(Hd);
-            if (SURF != SURF_NONE && im != 0.f)
-                surfaces<SURF>(a, mycache, cand, p, dx, kc, h, f, H, nullptr, nullptr);
-            f3 f2 = zero3();
-            sym3 H2 = sym_zero();
-            if (hasNext) {
-                const f3 p1dx = xyz(sm.dx[t + 1]);
-                const f3 c = ((p1 - p) + (p1dx - dx)) * invl - qtangent(q);
-                const float k = ks * invl;
-                float dd = k * invl;
-                f += c * k - dx * (damp * dd);
-                f2 += c * (-k) - p1dx * (damp * dd);
-                dd *= 1.f + damp;
-                H.xx += dd; H.yy += dd; H.zz += dd;
-                H2.xx += dd; H2.yy += dd; H2.zz += dd;
-            }
+            // ---- position step: own terms, exchange the segment's share, local solve
+            f3 f, f2;
+            sym3 H, H2;
+            position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, hasNext ? xyz(sm.dx[t + 1]) : zero3(), y, q,
+                                 damp, f, H, f2, H2);
             if (act) {
                 sm.fa[t] = f4(f2, H2.xx);
                 sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
@@ -277,84 +151,42 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
                 f += xyz(fa);
                 H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
             }
-            if (im != 0.f) dx += sym_solve(H, f) * a.accel;
+            position_solve(dx, f, H, a.accel, im);
             if (act) sm.dx[t] = f4(dx, 0.f);
             __syncthreads();  // B2
 
-            // ---- frame step, cosserat.cu:242-272. The reference's sign tests
-            // dot((q_{i-1}^-1 q_i), r_{i-1}) and dot((q_i^-1 q_{i+1}), r_i) equal
-            // dot(q_i, q_{i-1} r_{i-1}) and dot(q_i, q_{i+1} r_i^*) (Re(xy) = Re(yx) for
-            // quaternions), so they reuse the products that b needs.
+            // ---- frame step over the double-buffered rotors (no barrier needed before it)
             if (!(fl & F_FIX_ORIENT) && hasNext) {
-                const f3 p1dx = xyz(sm.dx[t + 1]);
-                const f3 vv = (((p1 - p) + (p1dx - dx)) * invl) * (-2.f * ks);
-                float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (hasPrev) {
-                    const float4 pr = qmul(sm.q[cur][t - 1], qrp);
-                    b = scale4(pr, dot4(q, pr) > 0.f ? 1.f : -1.f);
-                }
-                if (fl & F_NEXT_ORIENT) {
-                    const float4 nx = qmul(sm.q[cur][t + 1], qconj(qro));
-                    b = add4(b, scale4(nx, dot4(q, nx) > 0.f ? 1.f : -1.f));
-                }
-                const float lambda = len(vv) + sqrtf(dot4(b, b));
-                const float4 m = qmul_e1(qmul_pure(vv, b));
-                q = normalize4(add4(m, scale4(b, lambda)));
+                const f3 seg = (p1 - p) + (xyz(sm.dx[t + 1]) - dx);
+                q = frame_update(q, seg, c.invl, ks, hasPrev, hasPrev ? sm.q[cur][t - 1] : q, hasPrev ? sm.qr[t - 1] : q,
+                                 (fl & F_NEXT_ORIENT) != 0, (fl & F_NEXT_ORIENT) ? sm.q[cur][t + 1] : q, sm.qr[t]);
             }
             if (act) sm.q[cur ^ 1][t] = q;
             cur ^= 1;
         }
         __syncthreads();  // B3
 
-        // ---- velocity, drag, readout, advection, broad phase; iteration.cu:85-128
+        // ---- velocity, drag, readout, advection, broad phase
         if (im != 0.f) {
-            f3 vv = dx * invH;
-            const float kn = a.drag_quad;
-            if (kn > 0.f) {
-                const f3 tg = hasNext ? qtangent(q) : qtangent(sm.q[cur][t - 1]);
-                const f3 vt = tg * dot(tg, vv);
-                f3 vn = vv - vt;
-                vn = vn / (1.f + kn * len(vn) * h);
-                const f3 vt2 = vt / (1.f + a.drag_quad_t * len(vt) * h);
-                vv = vn + vt2;
-            }
-            v = vv * (1.f - a.drag * h);
+            const f3 tg = (a.drag_quad > 0.f) ? (hasNext ? qtangent(q) : qtangent(sm.q[cur][t - 1])) : zero3();
+            v = end_velocity(a, dx, invH, tg);
             if (SURF != SURF_NONE && a.forces_on) {
-                // planes accumulate into fv; each mesh's force is added to fv and its wrench
-                // goes to the (env, mesh) row, contact.cuh:172-204
                 f3 fv = zero3();
                 sym3 Hs = sym_zero();
-                surfaces<SURF>(a, mycache, cand, p, dx, kc, h, fv, Hs, wrow, &fv);
+                surfaces<SURF>(a, mycache, cand, p, dx, c.kc, h, fv, Hs, wrow, &fv);
                 facc += fv;
             }
         }
         p += dx;
-        if (SURF == SURF_MESHES && nsdf > 0) {
-            if (im != 0.f) {
-                const float pad = 2.f * len(dx) + 0.02f;
-                uint64_t mask = 0ull;
-                int cnt = 0;
-                for (int m = 0; m < nsdf; m++) {
-                    const PoseV P = load_pose(mycache + m * kPoseF4);
-                    const float pm = pad + (a.sdf_moving ? h * (len(P.vel) + len(P.om) * 0.5f * len(P.hi - P.lo)) : 0.f);
-                    if (p.x >= P.lo.x - pm && p.x <= P.hi.x + pm && p.y >= P.lo.y - pm && p.y <= P.hi.y + pm &&
-                        p.z >= P.lo.z - pm && p.z <= P.hi.z + pm) {
-                        mask |= 1ull << m;
-                        cnt++;
-                    }
-                }
-                cand = cnt <= kMaxCand ? mask : all_meshes(nsdf);
-            } else {
-                cand = 0ull;
-            }
-        }
+        if (SURF == SURF_MESHES && nsdf > 0) cand = (im != 0.f) ? build_candidates(a, mycache, nsdf, p, dx) : 0ull;
     }
 
     // ---- write back: device-order state and caller-order views
     if (act) {
+        const int uidx = a.topo[dv].z;
         a.pos[dv] = f4(p, im);
         a.vel[dv] = f4(v, lr);
-        a.lvel[dv] = f4(lv, ks);
+        a.lvel[dv] = f4(xyz(sm.lv[t]), ks);
         a.q[dv] = q;
         float* op = a.out_pos + (size_t)uidx * 3;
         op[0] = p.x; op[1] = p.y; op[2] = p.z;

@@ -764,6 +764,11 @@ PYBIND11_MODULE(_ropesim, m) {
             return py::make_tuple(blk, nb);
         })
         .def("set_sync", [](RopeBatch& b, bool every_frame) { ok(rs_batch_set_sync(b.h, every_frame ? 1 : 0)); })
+        .def("set_autotune", [](RopeBatch& b, bool on) { ok(rs_batch_set_autotune(b.h, on ? 1 : 0)); })
+        .def("set_engine", [](RopeBatch& b, const std::string& e) {
+            if (e != "persistent" && e != "plain") throw py::value_error("engine must be 'persistent' or 'plain'");
+            ok(rs_batch_set_engine(b.h, e == "plain" ? 1 : 0));
+        }, py::arg("engine"))
         .def("set_timing", [](RopeBatch& b, bool on) { ok(rs_batch_set_timing(b.h, on ? 1 : 0)); })
         .def("last_frame_ms", [](RopeBatch& b) { double ms = 0; ok(rs_batch_last_frame_ms(b.h, &ms)); return ms; })
         .def("stream_ptr", [](RopeBatch& b) { void* s = nullptr; ok(rs_batch_stream(b.h, &s)); return (uintptr_t)s; })

@@ -1,0 +1,251 @@
+// rs_substep.cuh -- the per-vertex pieces of one substep, shared by the persistent frame kernel
+// (rs_frame.cu) and the per-substep-launch plain path (rs_plain.cu), so both engines run the
+// same arithmetic in the same order.
+//
+// Reference routines restated (deterministic ordering):
+//   root_program / root_set   csrc/batch.cu:90-159
+//   compute_pose              sim/iteration.cu:12-33, sim/contact.cuh:79-87
+//   init_vertex               sim/iteration.cu:34-68
+//   position_terms            sim/cosserat.cu:37-159 (inertia, surfaces, stretch)
+//   position_solve            sim/cosserat.cu:198-217
+//   frame_update              sim/cosserat.cu:242-272
+//   end_velocity              sim/iteration.cu:85-112
+//   build_candidates          sim/contact.cuh:121-136
+#pragma once
+
+#include "rs_device.cuh"
+#include "rs_types.h"
+
+namespace rs {
+
+using namespace rsd;
+
+// Surface-contact variants of the kernels: none, planes only, planes + SDF meshes.
+enum : int { SURF_NONE = 0, SURF_PLANES = 1, SURF_MESHES = 2 };
+constexpr int kPoseF4 = 5;  // float4 per cached pose
+
+__device__ __forceinline__ uint64_t all_meshes(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
+
+// Shortest-arc SLERP with an nlerp fallback above dot 0.9995, batch.cu:106-114.
+__device__ __forceinline__ float4 slerp4(float4 a, float4 b, float t) {
+    float d = dot4(a, b);
+    if (d < 0.f) { b = scale4(b, -1.f); d = -d; }
+    if (d > 0.9995f) return normalize4(add4(scale4(a, 1.f - t), scale4(b, t)));
+    const float th = acosf(fminf(d, 1.f));
+    const float s = sinf(th);
+    return add4(scale4(a, sinf((1.f - t) * th) / s), scale4(b, sinf(t * th) / s));
+}
+__device__ __forceinline__ float4 unit_or_identity(const float* q) {
+    float4 a = make_float4(q[0], q[1], q[2], q[3]);
+    const float l = dot4(a, a);
+    return (l > 0.f) ? scale4(a, rsqrtf(l)) : make_float4(0.f, 0.f, 0.f, 1.f);
+}
+
+// Root program of substep s of S (row = p0, v0, p1, q0, q1): quadratic position at tau = s h,
+// velocity at the substep midpoint, SLERPed frame at (s + 1) / S, batch.cu:122-159.
+__device__ __forceinline__ void root_program(const FrameArgs& a, const float* row, int s, int S, float h, f3& p, f3& v,
+                                             float4& q) {
+    const f3 P0 = mk3(__ldg(row), __ldg(row + 1), __ldg(row + 2));
+    const f3 V0 = mk3(__ldg(row + 3), __ldg(row + 4), __ldg(row + 5));
+    const f3 P1 = mk3(__ldg(row + 6), __ldg(row + 7), __ldg(row + 8));
+    const f3 A = 2.f / (a.dt * a.dt) * ((P1 - P0) - V0 * a.dt);
+    const float tau = float(s) * h;
+    p = P0 + V0 * tau + 0.5f * tau * tau * A;
+    v = V0 + (tau + 0.5f * h) * A;
+    if (a.has_q0) {
+        const float4 qa = unit_or_identity(row + 9);
+        float4 qq = a.has_q1 ? slerp4(qa, unit_or_identity(row + 13), float(s + 1) / float(S)) : qa;
+        const float l2 = dot4(qq, qq);
+        q = (l2 > 0.f) ? scale4(qq, rsqrtf(l2)) : make_float4(0.f, 0.f, 0.f, 1.f);
+    }
+}
+// Constant-velocity root of a frame (row = p, v, -, q), batch.cu:90-104.
+__device__ __forceinline__ void root_set(const FrameArgs& a, const float* row, f3& p, f3& v, float4& q) {
+    p = mk3(row[0], row[1], row[2]);
+    v = mk3(row[3], row[4], row[5]);
+    if (a.has_q0) q = unit_or_identity(row + 9);
+}
+
+// Pose of (env en, mesh m) at the end of substep s of S: constant linear and angular velocity
+// over the frame, world AABB of the lattice; 5 float4 at `out`.
+__device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, int s, int S, float h, float4* out) {
+    const Motion M = a.motion[(size_t)en * kMaxSdf + m];
+    const float al = float(s + 1) / float(S);
+    const float invDt = 1.f / (float(S) * h);
+    const f3 p0 = mk3(M.p0x, M.p0y, M.p0z), dp = mk3(M.dpx, M.dpy, M.dpz), rot = mk3(M.rx, M.ry, M.rz);
+    const float4 q0 = make_float4(M.qx, M.qy, M.qz, M.qw);
+    f3 Pp, Pv, Pw;
+    float4 Pq;
+    const float th = len(rot);
+    if (th > 0.f || dp.x != 0.f || dp.y != 0.f || dp.z != 0.f) {
+        Pp = p0 + al * dp;
+        float4 dq = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (th > 0.f) {
+            const f3 ax = rot / th;
+            const float hr = (al * th) * 0.5f;
+            const float sn = sinf(hr);
+            dq = make_float4(sn * ax.x, sn * ax.y, sn * ax.z, cosf(hr));
+        }
+        Pq = normalize4(qmul(dq, q0));
+        Pv = dp * invDt;
+        Pw = rot * invDt;
+    } else {  // a target equal to the current pose: exactly the static pose
+        Pp = p0; Pq = q0; Pv = zero3(); Pw = zero3();
+    }
+    const GridDesc& gd = a.grids[m];
+    const f3 lo_o = mk3(gd.ox, gd.oy, gd.oz);
+    const f3 hi_o = lo_o + mk3(float(gd.nx - 1), float(gd.ny - 1), float(gd.nz - 1)) * gd.h;
+    f3 lo, hi;
+    world_box(lo_o, hi_o, Pp, Pq, lo, hi);
+    store_pose(out, Pp, Pq, Pv, Pw, lo, hi);
+}
+
+// Surfaces (planes, then candidate meshes in ascending index) at one probe point,
+// contact.cuh:141-163; with `wr` != nullptr it is the readout (contact.cuh:172-204): mesh
+// forces are added to *facc and their wrenches to wr[m * 6 ...].
+template <int SURF>
+__device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
+                                         float h, f3& f, sym3& H, float* wr, f3* facc) {
+    for (int pl = 0; pl < a.num_planes; pl++) {
+        const float4 P = a.planes[pl];
+        const f3 n = mk3(P.x, P.y, P.z);
+        const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
+        if (gap >= 0.f) continue;
+        surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
+    }
+    if constexpr (SURF == SURF_MESHES) {
+    for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
+        const int m = __ffsll((long long)mm) - 1;
+        const PoseV P = load_pose(cache + m * kPoseF4);
+        f3 n, dRel;
+        float gap;
+        if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, n, gap, dRel)) continue;
+        if (wr) {
+            f3 fm = zero3();
+            sym3 Hs = sym_zero();
+            surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, fm, Hs);
+            *facc += fm;
+            const f3 r = (pos - P.pos) + d - n * a.c_radius;
+            const f3 tq = cross(r, -fm);
+            float* w = wr + m * 6;
+            atomicAdd(w + 0, -fm.x); atomicAdd(w + 1, -fm.y); atomicAdd(w + 2, -fm.z);
+            atomicAdd(w + 3, tq.x); atomicAdd(w + 4, tq.y); atomicAdd(w + 5, tq.z);
+        } else {
+            surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, f, H);
+        }
+    }
+    }
+}
+
+// Inertial target y and initial guess dx from the substep's start velocity, iteration.cu:34-68.
+__device__ __forceinline__ void init_vertex(f3 vel0, f3 lv_old, float im, float h, float last_h, f3 g, float g2, f3& dx,
+                                            f3& y) {
+    dx = vel0 * h;
+    y = dx + g * (h * h);
+    if (im != 0.f && g2 > 0.f) {
+        const f3 acc = (vel0 - lv_old) / last_h;
+        const float sg = fminf(fmaxf(dot(acc, g) / g2, 0.f), 1.f);
+        dx += g * (h * h * sg);
+    }
+}
+
+// Per-vertex constants of a frame.
+struct VConst {
+    float im, invl, ks, Hd, fm, kc;
+};
+__device__ __forceinline__ VConst vertex_constants(const FrameArgs& a, float im, float lr, float ks) {
+    VConst c;
+    c.im = im;
+    c.invl = 1.f / lr;
+    c.ks = ks;
+    c.Hd = 1.f / (im * a.h * a.h);
+    c.fm = 1.f / (a.h * a.h * im);
+    const float kap = a.c_kappa / a.h;
+    c.kc = kap * kap / im;
+    return c;
+}
+
+// Position-step terms of vertex i, cosserat.cu:37-88: own force f / Hessian H (inertia, then
+// surfaces, then the stretch of segment i) and the segment's share f2 / H2 on vertex i + 1.
+template <int SURF>
+__device__ __forceinline__ void position_terms(const FrameArgs& a, const float4* cache, uint64_t cand, const VConst& c,
+                                               bool hasNext, f3 p, f3 p1, f3 dx, f3 p1dx, f3 y, float4 q, float damp,
+                                               f3& f, sym3& H, f3& f2, sym3& H2) {
+    f = (y - dx) * c.fm;
+    H = sym_diag(c.Hd);
+    if (SURF != SURF_NONE && c.im != 0.f) surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr);
+    f2 = zero3();
+    H2 = sym_zero();
+    if (hasNext) {
+        const f3 cc = ((p1 - p) + (p1dx - dx)) * c.invl - qtangent(q);
+        const float k = c.ks * c.invl;
+        float dd = k * c.invl;
+        f += cc * k - dx * (damp * dd);
+        f2 += cc * (-k) - p1dx * (damp * dd);
+        dd *= 1.f + damp;
+        H.xx += dd; H.yy += dd; H.zz += dd;
+        H2.xx += dd; H2.yy += dd; H2.zz += dd;
+    }
+}
+
+// Local solve dx += accel * H^-1 f of a free vertex, cosserat.cu:206-209.
+__device__ __forceinline__ void position_solve(f3& dx, f3 f, const sym3& H, float accel, float im) {
+    if (im != 0.f) dx += sym_solve(H, f) * accel;
+}
+
+// Frame step of segment i, cosserat.cu:242-272: vv = -2 k ((p1 - p) + (p1dx - dx)) / l, b from
+// the neighbours' frames and rest rotations, q = normalize(vv b e1 + (|vv| + |b|) b). The
+// reference's sign tests dot((q_{i-1}^-1 q_i), r_{i-1}) and dot((q_i^-1 q_{i+1}), r_i) equal
+// dot(q_i, q_{i-1} r_{i-1}) and dot(q_i, q_{i+1} r_i^*) (Re(xy) = Re(yx) for quaternions), so
+// they reuse the products b needs.
+__device__ __forceinline__ float4 frame_update(float4 q, f3 seg, float invl, float ks, bool hasPrev, float4 qprev,
+                                               float4 qrprev, bool hasNextOrient, float4 qnext, float4 qrown) {
+    const f3 vv = (seg * invl) * (-2.f * ks);
+    float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (hasPrev) {
+        const float4 pr = qmul(qprev, qrprev);
+        b = scale4(pr, dot4(q, pr) > 0.f ? 1.f : -1.f);
+    }
+    if (hasNextOrient) {
+        const float4 nx = qmul(qnext, qconj(qrown));
+        b = add4(b, scale4(nx, dot4(q, nx) > 0.f ? 1.f : -1.f));
+    }
+    const float lambda = len(vv) + sqrtf(dot4(b, b));
+    const float4 m = qmul_e1(qmul_pure(vv, b));
+    return normalize4(add4(m, scale4(b, lambda)));
+}
+
+// New velocity of a free vertex: dx / h, quadratic drag split by the segment tangent `tg`
+// (exact frozen-direction solution), then linear drag, iteration.cu:87-112.
+__device__ __forceinline__ f3 end_velocity(const FrameArgs& a, f3 dx, float invH, f3 tg) {
+    f3 vv = dx * invH;
+    const float kn = a.drag_quad;
+    if (kn > 0.f) {
+        const f3 vt = tg * dot(tg, vv);
+        f3 vn = vv - vt;
+        vn = vn / (1.f + kn * len(vn) * a.h);
+        const f3 vt2 = vt / (1.f + a.drag_quad_t * len(vt) * a.h);
+        vv = vn + vt2;
+    }
+    return vv * (1.f - a.drag * a.h);
+}
+
+// Broad phase for the next substep: meshes of this env whose padded world AABB holds p
+// (pad = 2 |dx| + 2 cm + the mesh's own travel); more than kMaxCand = every mesh.
+__device__ __forceinline__ uint64_t build_candidates(const FrameArgs& a, const float4* cache, int nsdf, f3 p, f3 dx) {
+    const float pad = 2.f * len(dx) + 0.02f;
+    uint64_t mask = 0ull;
+    int cnt = 0;
+    for (int m = 0; m < nsdf; m++) {
+        const PoseV P = load_pose(cache + m * kPoseF4);
+        const float pm = pad + (a.sdf_moving ? a.h * (len(P.vel) + len(P.om) * 0.5f * len(P.hi - P.lo)) : 0.f);
+        if (p.x >= P.lo.x - pm && p.x <= P.hi.x + pm && p.y >= P.lo.y - pm && p.y <= P.hi.y + pm && p.z >= P.lo.z - pm &&
+            p.z <= P.hi.z + pm) {
+            mask |= 1ull << m;
+            cnt++;
+        }
+    }
+    return cnt <= kMaxCand ? mask : all_meshes(nsdf);
+}
+
+}  // namespace rs

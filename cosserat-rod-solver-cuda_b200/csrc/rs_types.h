@@ -122,4 +122,16 @@ struct FrameArgs {
     GridDesc grids[kMaxSdf];
 };
 
+// Global-memory working set of the per-substep-launch (plain) engine.
+struct PlainBufs {
+    float4* dx;       // displacement iterate
+    float4* dxn;      // next iterate (Jacobi output)
+    float4* y;        // inertial target
+    float4* qprev;    // frame snapshot of the iteration
+    float4* lpos;     // positions at the substep start (+ invMass)
+    float4* facc;     // contact-force readout accumulated over the frame
+    uint64_t* cand;   // broad-phase mesh mask per vertex
+    Pose* spose;      // [envs * 64] poses of the current substep (moving meshes)
+};
+
 }  // namespace rs

@@ -83,6 +83,14 @@ RS_API int rs_batch_get_gravity(rs_batch* b, float* g3);
 /* Bin size (CTA threads) of the packed layout; 0 = automatic. Used by the autotuner. */
 RS_API int rs_batch_set_block(rs_batch* b, int block);
 RS_API int rs_batch_layout(rs_batch* b, int* block, int* num_bins);
+/* Bin-size autotuner (default on while the bin size is automatic): the first frames each run
+ * one candidate bin size, then the fastest is kept (results are bitwise identical across bin
+ * sizes) and remembered per workload signature for the process. */
+RS_API int rs_batch_set_autotune(rs_batch* b, int on);
+/* Engine: 0 = one persistent kernel per control frame (default); 1 = the per-substep-launch
+ * plain path (the reference's launch structure: root, init, num_itr x (position, frame), end
+ * kernels per substep, the iterations replayed from a CUDA graph), the in-repo baseline. */
+RS_API int rs_batch_set_engine(rs_batch* b, int engine);
 /* 1 (default) = synchronise and read the status words after every frame (checkErrors). */
 RS_API int rs_batch_set_sync(rs_batch* b, int every_frame);
 
