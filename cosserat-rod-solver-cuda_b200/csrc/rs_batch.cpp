@@ -72,6 +72,8 @@ Batch::Batch(int num_ropes, const int* rope_verts, const float* positions, const
         if (fix_root_orientation) fl_[ustart_[r]] |= F_FIX_ORIENT;
     }
     configure(density);
+    rc_radius_ = dead_radius;
+    rc_barrier_ = dead_barrier;
     // dead collision radii gate the segment-length check of uploadMeta (YarnBall.cu:268)
     if (2.f * min_seg_ < 2.f * dead_radius + dead_barrier)
         throw std::invalid_argument("Use thinner yarn or use longer segments (2 * min segment >= 2 * radius + barrier)");
@@ -108,7 +110,8 @@ Batch::~Batch() {
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (pl_graph_) cudaGraphExecDestroy(pl_graph_);
-    void* pbufs[] = {pl_.dx, pl_.dxn, pl_.y, pl_.qprev, pl_.lpos, pl_.facc, pl_.cand, pl_.spose, d_pl_args_};
+    void* pbufs[] = {pl_.dx, pl_.dxn, pl_.y, pl_.qprev, pl_.lpos, pl_.facc, pl_.cand, pl_.spose, d_pl_args_,
+                     d_grp_, d_cols_, d_ncols_, d_maxstep_, d_pad_};
     for (void* p : pbufs)
         if (p) cudaFree(p);
     if (h_pl_args_) cudaFreeHost(h_pl_args_);
@@ -185,36 +188,58 @@ int Batch::pose_cache_entries() const { return std::max(1, max_rcount_ * (int)gr
 
 // Whole ropes into bins of `block_` threads: first-fit decreasing by length; a bin also
 // holds at most max_ropes_per_bin_ ropes (bounded by the per-CTA mesh pose cache).
+// Whole ropes into bins of `block_` threads: first-fit decreasing by size over *units* -- single
+// ropes, or whole rope-rope contact groups (group_ropes consecutive ropes, kept in caller order
+// so that detection scans candidates in the reference's order). A bin also holds at most
+// max_ropes_per_bin_ ropes (bounded by the per-CTA mesh pose cache). A contact group larger
+// than the largest CTA cannot be CTA-resident: the layout then keeps caller order and frames run
+// on the plain engine.
 void Batch::pack() {
-    int maxV = 0;
-    for (int r = 0; r < R_; r++) maxV = std::max(maxV, rope_verts(r));
+    std::vector<std::vector<int>> units;
+    const int G = rope_contact_ ? std::max(1, group_ropes_) : 1;
+    for (int r0 = 0; r0 < R_; r0 += G) {
+        std::vector<int> u;
+        for (int r = r0; r < std::min(R_, r0 + G); r++) u.push_back(r);
+        units.push_back(u);
+    }
+    auto usize = [&](const std::vector<int>& u) {
+        int v = 0;
+        for (int r : u) v += rope_verts(r);
+        return v;
+    };
+    int maxU = 0;
+    for (auto& u : units) maxU = std::max(maxU, usize(u));
+    max_unit_verts_ = maxU;
+    oversize_ = maxU > 1024;
     int blk = block_override ? block_override : tune_block_;
     if (blk == 0) {
-        blk = std::max(64, next_pow2(maxV));
+        blk = std::max(64, next_pow2(std::min(maxU, 1024)));
         if (blk < 256 && (long long)n_ > 148LL * blk) blk = 256;
     }
-    if (blk < maxV) blk = next_pow2(maxV);
-    if (blk > 1024) throw std::invalid_argument("rope longer than the largest CTA (1024)");
-    block_ = blk;
+    if (!oversize_ && blk < maxU) blk = next_pow2(maxU);
+    block_ = std::min(blk, 1024);
     const int M = (int)grids_.size();
     int cap = max_ropes_per_bin_;
     if (M > 0) cap = std::min(cap, std::max(1, (96 * 1024) / (2 * M * (int)sizeof(Pose))));
-    std::vector<int> order(R_);
+    std::vector<int> order(units.size());
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rope_verts(a) > rope_verts(b); });
+    if (!oversize_)
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return usize(units[a]) > usize(units[b]); });
     struct Open { int used, rc; std::vector<int> ropes; };
     std::vector<Open> open;
     int first_open = 0;
-    for (int r : order) {
-        const int L = rope_verts(r);
+    for (int ui : order) {
+        const int L = usize(units[ui]);
+        const int nr = (int)units[ui].size();
         int b = -1;
-        for (int k = first_open; k < (int)open.size(); k++)
-            if (open[k].used + L <= blk && open[k].rc < cap) { b = k; break; }
+        if (!oversize_)
+            for (int k = first_open; k < (int)open.size(); k++)
+                if (open[k].used + L <= block_ && open[k].rc + nr <= std::max(cap, nr)) { b = k; break; }
         if (b < 0) { open.push_back(Open{0, 0, {}}); b = (int)open.size() - 1; }
         open[b].used += L;
-        open[b].rc++;
-        open[b].ropes.push_back(r);
-        while (first_open < (int)open.size() && (open[first_open].used + 3 > blk || open[first_open].rc >= cap)) first_open++;
+        open[b].rc += nr;
+        for (int r : units[ui]) open[b].ropes.push_back(r);
+        while (first_open < (int)open.size() && (open[first_open].used + 3 > block_ || open[first_open].rc >= cap)) first_open++;
     }
     bins_.clear();
     dropes_.clear();
@@ -232,6 +257,16 @@ void Batch::pack() {
         b.vcount = dv - b.vstart;
         bins_.push_back(b);
         max_rcount_ = std::max(max_rcount_, b.rcount);
+    }
+    // contact-group and rope ranges per device vertex (device order)
+    grp_.assign(n_, int4{0, 0, 0, 0});
+    for (auto& u : units) {
+        const int gs = u2d_[ustart_[u.front()]];
+        const int ge = u2d_[ustart_[u.back()]] + rope_verts(u.back());
+        for (int r : u) {
+            const int rs0 = u2d_[ustart_[r]];
+            for (int i = 0; i < rope_verts(r); i++) grp_[rs0 + i] = int4{gs, ge, rs0, rs0 + rope_verts(r)};
+        }
     }
 }
 
@@ -304,6 +339,8 @@ void Batch::ensure_device() {
         check(cudaMemcpy(d_topo_, topo.data(), sizeof(int4) * n_, cudaMemcpyHostToDevice), "upload(topo)");
         check(cudaMemcpy(d_init_pos_, ip.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(init pos)");
         check(cudaMemcpy(d_init_q_, iq.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(init q)");
+        if (!d_grp_) check(cudaMalloc(&d_grp_, sizeof(int4) * n_), "cudaMalloc(groups)");
+        check(cudaMemcpy(d_grp_, grp_.data(), sizeof(int4) * n_, cudaMemcpyHostToDevice), "upload(groups)");
         layout_valid_ = true;
         device_valid_ = false;
     }
@@ -487,9 +524,15 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     a.pose_cache = pose_cache_entries();
     a.poses = d_poses_; a.motion = d_motion_;
     for (int m = 0; m < (int)grids_.size(); m++) a.grids[m] = grids_[m];
+    a.n = n_;
+    a.rope_contact = rope_contact_ ? 1 : 0;
+    a.rc_radius = rc_radius_; a.rc_barrier = rc_barrier_; a.rc_kcol = rc_kcol_; a.rc_mu = rc_mu_; a.rc_kfric = rc_kfric_;
+    a.det_radius = rc_radius_ + 0.5f * rc_barrier_;          // uploadMeta, YarnBall.cu:262-263
+    a.sdet_radius = a.det_radius * rc_scaler_;
+    a.grp = d_grp_; a.cols = d_cols_; a.ncols = d_ncols_; a.maxstep = d_maxstep_; a.pad = d_pad_;
     const bool timed = timing_ || tuning();
     if (timed) check(cudaEventRecord(ev0_, stream_), "event");
-    if (engine_ == 1) run_frame_plain(a);
+    if (engine_ == 1 || (rope_contact_ && oversize_)) run_frame_plain(a);
     else check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
     if (timed) check(cudaEventRecord(ev1_, stream_), "event");
     host_dyn_valid_ = false;
@@ -526,12 +569,12 @@ void Batch::run_frame_plain(const FrameArgs& a) {
     *h_pl_args_ = a;
     check(cudaMemcpyAsync(d_pl_args_, h_pl_args_, sizeof(FrameArgs), cudaMemcpyHostToDevice, stream_), "upload(args)");
     const int surf = a.num_sdf > 0 ? 2 : (a.num_planes > 0 ? 1 : 0);
-    const std::string key = std::to_string(a.iters) + ":" + std::to_string(surf);
+    const std::string key = std::to_string(a.iters) + ":" + std::to_string(surf) + ":" + std::to_string(a.rope_contact);
     if (!pl_graph_ || key != pl_graph_key_) {
         if (pl_graph_) { cudaGraphExecDestroy(pl_graph_); pl_graph_ = nullptr; }
         cudaGraph_t graph;
         check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-        const cudaError_t rec = plain_record_inner(d_pl_args_, pl_, n_, a.iters, surf, stream_);
+        const cudaError_t rec = plain_record_inner(d_pl_args_, pl_, n_, a.iters, surf, a.rope_contact != 0, stream_);
         check(cudaStreamEndCapture(stream_, &graph), "end capture");
         check(rec, "record plain iterations");
         check(cudaGraphInstantiate(&pl_graph_, graph, 0), "instantiate plain graph");
@@ -539,7 +582,8 @@ void Batch::run_frame_plain(const FrameArgs& a) {
         pl_graph_key_ = key;
     }
     for (int s = 0; s < a.substeps; s++) {
-        check(plain_launch_pre(d_pl_args_, pl_, n_, R_, R_, a.num_sdf, a.sdf_moving != 0, a.root_mode, s, stream_),
+        check(plain_launch_pre(d_pl_args_, pl_, n_, R_, R_, a.num_sdf, a.sdf_moving != 0, a.root_mode, a.rope_contact != 0, s,
+                               stream_),
               "plain substep prologue");
         check(cudaGraphLaunch(pl_graph_, stream_), "plain graph launch");
     }
@@ -684,7 +728,12 @@ void Batch::step_legacy(const float* p, const float* v, const float* q, float dt
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");
-        if (h_status_[2]) { nonfinite_ = 1; check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status"); }
+        if (h_status_[0] || h_status_[2]) {
+            if (h_status_[2]) nonfinite_ = 1;
+            const int err = h_status_[0];
+            check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
+            if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
+        }
     }
     if (timing_) {
         float ms = 0.f;
@@ -704,7 +753,12 @@ void Batch::step_free(float dt, int substeps) {
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");
-        if (h_status_[2]) { nonfinite_ = 1; check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status"); }
+        if (h_status_[0] || h_status_[2]) {
+            if (h_status_[2]) nonfinite_ = 1;
+            const int err = h_status_[0];
+            check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
+            if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
+        }
     }
 }
 
@@ -724,7 +778,48 @@ void Batch::advance(float dt, int substeps) {
     if (sync_every_frame) {
         check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
         check(cudaStreamSynchronize(stream_), "frame");
-        if (h_status_[2]) { nonfinite_ = 1; check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status"); }
+        if (h_status_[0] || h_status_[2]) {
+            if (h_status_[2]) nonfinite_ = 1;
+            const int err = h_status_[0];
+            check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
+            if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
+        }
+    }
+}
+
+void Batch::set_rope_contact(bool on, float radius, float barrier, float k_collision, float mu, float k_friction,
+                             float detection_scaler, int group_ropes) {
+    if (on) {
+        // uploadMeta enforces this every step (YarnBall.cu:268): check it here so a bad call
+        // leaves the old state (batch.cu:509-512)
+        if (2.f * min_seg_ < 2.f * radius + barrier)
+            throw std::invalid_argument("rope contact needs 2 * radius + barrier <= 2 * shortest segment");
+        if (!(detection_scaler > 1.f)) throw std::invalid_argument("Detection scaler must be greater than 1.");
+    }
+    ensure_host();
+    const bool relayout = on != rope_contact_ || (on && group_ropes != group_ropes_);
+    if (on) {
+        rc_radius_ = radius; rc_barrier_ = barrier; rc_kcol_ = k_collision; rc_mu_ = mu; rc_kfric_ = k_friction;
+        rc_scaler_ = detection_scaler;
+        group_ropes_ = group_ropes > 0 ? group_ropes : 1;
+        if (!d_cols_) {
+            check(cudaMalloc(&d_cols_, sizeof(int) * (size_t)kMaxCols * n_), "cudaMalloc(rope candidates)");
+            check(cudaMalloc(&d_ncols_, sizeof(int) * n_), "cudaMalloc(rope candidate counts)");
+            check(cudaMalloc(&d_maxstep_, sizeof(float) * n_), "cudaMalloc(step limits)");
+            check(cudaMalloc(&d_pad_, sizeof(float) * n_), "cudaMalloc(paddings)");
+            check(cudaMemset(d_ncols_, 0, sizeof(int) * n_), "memset(rope candidate counts)");
+        }
+    }
+    rope_contact_ = on;
+    if (relayout) {
+        layout_valid_ = false;
+        device_valid_ = false;
+        tuned_ = false;
+        tune_cands_.clear();
+        tune_log_.clear();
+        tune_block_ = 0;
+        ensure_device();
+        gather();
     }
 }
 

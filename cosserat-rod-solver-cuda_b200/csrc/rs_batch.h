@@ -116,6 +116,12 @@ public:
     void contact_forces_host(float* out);   // [n, 3]
     void wrenches_host(float* out);         // [R, M, 6]
 
+    // ---- rope-rope contact (RopeBatch::set_rope_contact, batch.cu:504-522): group_ropes
+    // consecutive ropes form one contact group; groups never interact
+    void set_rope_contact(bool on, float radius, float barrier, float k_collision, float mu, float k_friction,
+                          float detection_scaler, int group_ropes);
+    bool rope_contact() const { return rope_contact_; }
+
     // ---- layout introspection (tests, autotuner)
     int block() const { return block_; }
     void set_block(int block);   // 0 = automatic; repacks the device layout
@@ -189,6 +195,18 @@ private:
     double last_frame_ms_ = 0.0;
     bool autotune_ = true, tuned_ = false;
     int engine_ = 0;
+    // rope-rope contact
+    bool rope_contact_ = false;
+    float rc_radius_ = 1e-4f, rc_barrier_ = 8e-4f, rc_kcol_ = 1e-5f, rc_mu_ = 0.1f, rc_kfric_ = 5.f, rc_scaler_ = 1.2f;
+    int group_ropes_ = 1;
+    int max_unit_verts_ = 0;
+    bool oversize_ = false;          // a contact group is larger than one CTA: plain engine
+    std::vector<int4> grp_;          // host copy of d_grp_
+    int4* d_grp_ = nullptr;          // [n] (group start, group end, rope start, rope end), device order
+    int* d_cols_ = nullptr;          // [kMaxCols * n] candidate lists (scratch)
+    int* d_ncols_ = nullptr;         // [n]
+    float* d_maxstep_ = nullptr;     // [n]
+    float* d_pad_ = nullptr;         // [n]
     PlainBufs pl_{};
     FrameArgs* d_pl_args_ = nullptr;
     FrameArgs* h_pl_args_ = nullptr;   // pinned staging of the frame parameters

@@ -465,6 +465,20 @@ int rs_batch_set_planes(rs_batch* b, int count, const float* rows) {
         s.set_planes(count, unit.data());
     });
 }
+int rs_batch_set_rope_contact(rs_batch* b, int enabled, float radius, float barrier, float k_collision, float mu,
+                              float k_friction, float detection_scaler, int group_ropes) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        if (enabled)
+            need(radius > 0 && barrier > 0 && k_collision > 0 && mu >= 0 && k_friction >= 0 && detection_scaler > 1 &&
+                     group_ropes >= 1,
+                 "rope contact needs radius, barrier, k_collision > 0, mu, k_friction >= 0, detection_scaler > 1, "
+                 "group_ropes >= 1");
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_rope_contact(enabled != 0, radius, barrier, k_collision, mu, k_friction, detection_scaler, group_ropes);
+    });
+}
+
 int rs_batch_add_mesh(rs_batch* b, const float* values, int nx, int ny, int nz, const float* origin3, float spacing,
                       float mu_s, float mu_k, const float* pos, const float* quat, int rows, int* index) {
     return guarded([&] {

@@ -37,16 +37,19 @@ struct FrameSmem {
     float4 qr[BLOCK];     // rest rotation of segment i (vertex i reads slots i-1 and i)
     float4 lv[BLOCK];     // velocity at the previous substep's start (initial-guess extrapolation)
     float fc[BLOCK];      // H2.yz
+    float pad[BLOCK];     // rope-rope detection padding of the substep
+    float lim[BLOCK];     // rope-rope step limit of segment i
+    int flg[BLOCK];       // vertex flags (rope-rope detection reads the group's)
 };
 
 // Resident CTAs per SM the register allocation targets: 28 warps per SM (<= 72 registers;
 // 24 warps for 256-thread CTAs) without meshes, 16 warps per SM (<= 128 registers) with meshes.
 #ifndef RS_MIN_BLOCKS
-#define RS_MIN_BLOCKS(B, SURF) ((B) <= 256 ? (((SURF) == SURF_MESHES ? 512 : 896) / (B)) : 1)
+#define RS_MIN_BLOCKS(B, SURF, ROPE) ((B) <= 256 ? (((SURF) == SURF_MESHES || (ROPE) ? 512 : 896) / (B)) : 1)
 #endif
 
-template <int BLOCK, int SURF>
-__global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kernel(const FrameArgs a) {
+template <int BLOCK, int SURF, bool ROPE>
+__global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame_kernel(const FrameArgs a) {
     extern __shared__ float4 dyn_smem[];  // FrameSmem<BLOCK>, then the pose cache [2][pose_cache][kPoseF4]
     FrameSmem<BLOCK>& sm = *reinterpret_cast<FrameSmem<BLOCK>*>(dyn_smem);
     float4* pose_smem = dyn_smem + sizeof(FrameSmem<BLOCK>) / sizeof(float4);
@@ -77,6 +80,17 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
     const bool hasNext = fl & F_NEXT, hasPrev = fl & F_PREV;
     const bool isRoot = (fl & F_ROOT) != 0;
     const VConst c = vertex_constants(a, im, lr, ks);
+    // rope-rope contact group and rope of this vertex (CTA-local indices)
+    int g0 = 0, g1 = 0, r0 = 0, r1 = 0;
+    if constexpr (ROPE) {
+        sm.flg[t] = (int)fl;
+        if (act) {
+            const int4 gr = a.grp[dv];
+            g0 = gr.x - bin.vstart; g1 = gr.y - bin.vstart; r0 = gr.z - bin.vstart; r1 = gr.w - bin.vstart;
+        }
+    }
+    int ncol = 0;
+    float lim = INFINITY;
     const float h = a.h;
     const float damp = a.damping / h;
     const float invH = 1.f / h;
@@ -130,16 +144,61 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
             sm.lv[t] = f4(v, 0.f);
             sm.p[t] = f4(p, 0.f);
             sm.dx[t] = f4(dx, 0.f);
+            if constexpr (ROPE) sm.pad[t] = a.sdet_radius + len(y);
         }
         __syncthreads();  // B0
         const f3 p1 = hasNext ? xyz(sm.p[t + 1]) : zero3();
+
+        // ---- rope-rope detection over the CTA-resident group (ascending j, cap kMaxCols) and
+        // the step limit of segment i, batch.cu:19-49 and collision.cu:103-136
+        if constexpr (ROPE) {
+            ncol = 0;
+            lim = INFINITY;
+            if (hasNext) {
+                const f3 a1 = p1 - p;
+                const float ri = fmaxf(sm.pad[t], sm.pad[t + 1]);
+                lim = sm.pad[t] - a.det_radius;
+                int cnt = 0;
+                for (int j = g0; j < g1; j++) {
+                    if (!(sm.flg[j] & F_NEXT)) continue;
+                    if (j >= r0 && j < r1 && abs(j - t) <= 2) continue;
+                    const f3 pj0 = xyz(sm.p[j]), pj1 = xyz(sm.p[j + 1]);
+                    if (rope_pair_candidate(p, a1, ri, pj0, pj1, fmaxf(sm.pad[j], sm.pad[j + 1]))) {
+                        if (cnt < kMaxCols) {
+                            a.cols[(size_t)cnt * a.n + dv] = j;
+                            lim = fminf(lim, step_limit_of(p, a1, pj0, pj1));
+                        }
+                        cnt++;
+                    }
+                }
+                if (cnt > kMaxCols) atomicMax(a.status, ERR_MAX_COLLISIONS);
+                ncol = cnt < kMaxCols ? cnt : kMaxCols;
+            }
+            sm.lim[t] = lim;
+        }
 
         for (int it = 0; it < I; it++) {
             // ---- position step: own terms, exchange the segment's share, local solve
             f3 f, f2;
             sym3 H, H2;
-            position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, hasNext ? xyz(sm.dx[t + 1]) : zero3(), y, q,
-                                 damp, f, H, f2, H2);
+            const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
+            position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            if constexpr (ROPE) {
+                if (ncol > 0) {
+                    // even candidates join the own terms, odd ones a second partial added after
+                    // them (the reference's two sectors, cosserat.cu:99-182)
+                    f3 fo = zero3(), f2o = zero3();
+                    sym3 Ho = sym_zero(), H2o = sym_zero();
+                    for (int cc = 0; cc < ncol; cc++) {
+                        const int j = a.cols[(size_t)cc * a.n + dv];
+                        const f3 b0 = xyz(sm.p[j]), b1 = xyz(sm.p[j + 1]);
+                        const f3 db0 = xyz(sm.dx[j]), db1 = xyz(sm.dx[j + 1]);
+                        if (cc & 1) collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, fo, f2o, Ho, H2o);
+                        else collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, f, f2, H, H2);
+                    }
+                    if (ncol > 1) { f += fo; f2 += f2o; sym_add(H, Ho); sym_add(H2, H2o); }
+                }
+            }
             if (act) {
                 sm.fa[t] = f4(f2, H2.xx);
                 sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
@@ -151,7 +210,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
                 f += xyz(fa);
                 H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
             }
-            position_solve(dx, f, H, a.accel, im);
+            if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
+            else position_solve(dx, f, H, a.accel, im);
             if (act) sm.dx[t] = f4(dx, 0.f);
             __syncthreads();  // B2
 
@@ -203,9 +263,9 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF)) frame_kerne
 }
 
 // ------------------------------------------------------------------ launch
-template <int BLOCK, int SURF>
+template <int BLOCK, int SURF, bool ROPE>
 static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_bytes, cudaStream_t s) {
-    auto k = frame_kernel<BLOCK, SURF>;
+    auto k = frame_kernel<BLOCK, SURF, ROPE>;
     const size_t dyn_smem = sizeof(FrameSmem<BLOCK>) + pose_bytes;
     if (dyn_smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
@@ -215,12 +275,17 @@ static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_
     return cudaGetLastError();
 }
 
+template <int BLOCK, bool ROPE>
+static cudaError_t launch_frame_r(const FrameArgs& a, int num_bins, cudaStream_t s) {
+    if (a.num_sdf > 0)
+        return launch_frame_t<BLOCK, SURF_MESHES, ROPE>(a, num_bins, (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4), s);
+    if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES, ROPE>(a, num_bins, 0, s);
+    return launch_frame_t<BLOCK, SURF_NONE, ROPE>(a, num_bins, 0, s);
+}
+
 template <int BLOCK>
 static cudaError_t launch_frame_b(const FrameArgs& a, int num_bins, cudaStream_t s) {
-    if (a.num_sdf > 0)
-        return launch_frame_t<BLOCK, SURF_MESHES>(a, num_bins, (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4), s);
-    if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES>(a, num_bins, 0, s);
-    return launch_frame_t<BLOCK, SURF_NONE>(a, num_bins, 0, s);
+    return a.rope_contact ? launch_frame_r<BLOCK, true>(a, num_bins, s) : launch_frame_r<BLOCK, false>(a, num_bins, s);
 }
 
 cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s) {

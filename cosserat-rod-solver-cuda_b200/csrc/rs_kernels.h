@@ -22,9 +22,10 @@ cudaError_t launch_commit(Pose7* cur, const Pose7* tgt, uint8_t* tele, Pose* pos
                           int only, int N, cudaStream_t s);
 cudaError_t launch_scale(float* x, int n, float k, cudaStream_t s);
 // Plain (per-substep-launch) engine: `pa` is the frame's FrameArgs in device memory.
-cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, int surf, cudaStream_t s);
+cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, int surf, bool rope,
+                               cudaStream_t s);
 cudaError_t plain_launch_pre(const FrameArgs* pa, const PlainBufs& b, int n, int nropes, int envs, int num_sdf, bool moving,
-                             int root_mode, int s, cudaStream_t st);
+                             int root_mode, bool rope, int s, cudaStream_t st);
 cudaError_t plain_launch_finish(const FrameArgs* pa, const PlainBufs& b, int n, cudaStream_t st);
 // FP32 FMA throughput probe (16 * 8 FMAs per thread per iteration).
 cudaError_t launch_fp32_probe(float* out, int blocks, int threads, int iters, cudaStream_t s);

@@ -68,11 +68,46 @@ __global__ void plain_init_kernel(const FrameArgs* __restrict__ pa, PlainBufs b,
     b.y[d] = f4(y, 0.f);
     b.lpos[d] = P;
     if (first) b.cand[d] = all_meshes(a.num_sdf);
+    if (a.rope_contact) a.pad[d] = a.sdet_radius + len(y);
+}
+
+// Rope-rope detection of segment d over its contact group (ascending j, cap kMaxCols) and its
+// step limit, batch.cu:19-49 and collision.cu:103-136.
+__global__ void plain_detect_kernel(const FrameArgs* __restrict__ pa, PlainBufs b, int n) {
+    const FrameArgs& a = *pa;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const uint32_t fl = (uint32_t)a.topo[d].x;
+    if (!(fl & F_NEXT)) {
+        a.ncols[d] = 0;
+        a.maxstep[d] = INFINITY;
+        return;
+    }
+    const int4 gr = a.grp[d];
+    const f3 p = xyz(b.lpos[d]), a1 = xyz(b.lpos[d + 1]) - p;
+    const float ri = fmaxf(a.pad[d], a.pad[d + 1]);
+    float lim = a.pad[d] - a.det_radius;
+    int cnt = 0;
+    for (int j = gr.x; j < gr.y; j++) {
+        if (!(a.topo[j].x & F_NEXT)) continue;
+        if (j >= gr.z && j < gr.w && abs(j - d) <= 2) continue;
+        const f3 pj0 = xyz(b.lpos[j]), pj1 = xyz(b.lpos[j + 1]);
+        if (rope_pair_candidate(p, a1, ri, pj0, pj1, fmaxf(a.pad[j], a.pad[j + 1]))) {
+            if (cnt < kMaxCols) {
+                a.cols[(size_t)cnt * n + d] = j;
+                lim = fminf(lim, step_limit_of(p, a1, pj0, pj1));
+            }
+            cnt++;
+        }
+    }
+    if (cnt > kMaxCols) atomicMax(a.status, ERR_MAX_COLLISIONS);
+    a.ncols[d] = cnt < kMaxCols ? cnt : kMaxCols;
+    a.maxstep[d] = lim;
 }
 
 // Position step (SNAPSHOT): reads the previous iterate, writes dxNext and the frame snapshot,
 // cosserat.cu:23-225.
-template <int SURF>
+template <int SURF, bool ROPE>
 __global__ void __launch_bounds__(kPosBlock) plain_position_kernel(const FrameArgs* __restrict__ pa, PlainBufs b, int n) {
     const FrameArgs& a = *pa;
     __shared__ float4 sfa[kPosBlock], sfb[kPosBlock];
@@ -98,8 +133,22 @@ __global__ void __launch_bounds__(kPosBlock) plain_position_kernel(const FrameAr
         const f3 p1dx = hasNext ? xyz(b.dx[d + 1]) : zero3();
         const float4* cache = (SURF == SURF_MESHES) ? env_poses(a, b, tp.w) : nullptr;
         const uint64_t cand = (SURF == SURF_MESHES) ? b.cand[d] : 0ull;
-        position_terms<SURF>(a, cache, cand, c, hasNext, xyz(P), p1, dx, p1dx, xyz(b.y[d]), q, a.damping / a.h, f, H,
-                             f2, H2);
+        const float damp = a.damping / a.h;
+        position_terms<SURF>(a, cache, cand, c, hasNext, xyz(P), p1, dx, p1dx, xyz(b.y[d]), q, damp, f, H, f2, H2);
+        if constexpr (ROPE) {
+            const int nc = hasNext ? a.ncols[d] : 0;
+            if (nc > 0) {
+                f3 fo = zero3(), f2o = zero3();
+                sym3 Ho = sym_zero(), H2o = sym_zero();
+                for (int cc = 0; cc < nc; cc++) {
+                    const int j = a.cols[(size_t)cc * n + d];
+                    const f3 b0 = xyz(b.lpos[j]), b1 = xyz(b.lpos[j + 1]), db0 = xyz(b.dx[j]), db1 = xyz(b.dx[j + 1]);
+                    if (cc & 1) collision_term(a, damp, xyz(P), p1, dx, p1dx, b0, b1, db0, db1, fo, f2o, Ho, H2o);
+                    else collision_term(a, damp, xyz(P), p1, dx, p1dx, b0, b1, db0, db1, f, f2, H, H2);
+                }
+                if (nc > 1) { f += fo; f2 += f2o; sym_add(H, Ho); sym_add(H2, H2o); }
+            }
+        }
     }
     sfa[lt] = f4(f2, H2.xx);
     sfb[lt] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
@@ -111,7 +160,12 @@ __global__ void __launch_bounds__(kPosBlock) plain_position_kernel(const FrameAr
         f += xyz(fa);
         H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sfc[lt - 1];
     }
-    position_solve(dx, f, H, a.accel, im);
+    if constexpr (ROPE) {
+        const float lim = (fl & F_PREV) ? fminf(a.maxstep[d], a.maxstep[d - 1]) : a.maxstep[d];
+        position_solve_limited(dx, f, H, a.accel, im, lim);
+    } else {
+        position_solve(dx, f, H, a.accel, im);
+    }
     b.dxn[d] = f4(dx, 0.f);
     b.qprev[d] = q;
 }
@@ -184,10 +238,10 @@ __global__ void plain_finish_kernel(const FrameArgs* __restrict__ pa, PlainBufs 
 
 inline int blocks_of(int n, int t) { return (n + t - 1) / t; }
 
-template <int SURF>
+template <int SURF, bool ROPE>
 void capture_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, cudaStream_t s) {
     for (int it = 0; it < iters; it++) {
-        plain_position_kernel<SURF><<<blocks_of(n, kOwned), kPosBlock, 0, s>>>(pa, b, n);
+        plain_position_kernel<SURF, ROPE><<<blocks_of(n, kOwned), kPosBlock, 0, s>>>(pa, b, n);
         plain_frame_kernel<<<blocks_of(n, 128), 128, 0, s>>>(pa, b, n);
     }
     plain_end_kernel<SURF><<<blocks_of(n, 256), 256, 0, s>>>(pa, b, n);
@@ -195,19 +249,27 @@ void capture_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, cu
 
 }  // namespace
 
-cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, int surf, cudaStream_t s) {
-    if (surf == SURF_MESHES) capture_inner<SURF_MESHES>(pa, b, n, iters, s);
-    else if (surf == SURF_PLANES) capture_inner<SURF_PLANES>(pa, b, n, iters, s);
-    else capture_inner<SURF_NONE>(pa, b, n, iters, s);
+template <bool ROPE>
+void record_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, int surf, cudaStream_t s) {
+    if (surf == SURF_MESHES) capture_inner<SURF_MESHES, ROPE>(pa, b, n, iters, s);
+    else if (surf == SURF_PLANES) capture_inner<SURF_PLANES, ROPE>(pa, b, n, iters, s);
+    else capture_inner<SURF_NONE, ROPE>(pa, b, n, iters, s);
+}
+
+cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, int surf, bool rope,
+                               cudaStream_t s) {
+    if (rope) record_inner<true>(pa, b, n, iters, surf, s);
+    else record_inner<false>(pa, b, n, iters, surf, s);
     return cudaGetLastError();
 }
 
 cudaError_t plain_launch_pre(const FrameArgs* pa, const PlainBufs& b, int n, int nropes, int envs, int num_sdf, bool moving,
-                             int root_mode, int s, cudaStream_t st) {
+                             int root_mode, bool rope, int s, cudaStream_t st) {
     if (root_mode != ROOT_NONE && (root_mode == ROOT_PROGRAM || s == 0))
         plain_root_kernel<<<blocks_of(nropes, 128), 128, 0, st>>>(pa, nropes, s);
     if (num_sdf > 0 && moving) plain_pose_kernel<<<blocks_of(envs * num_sdf, 128), 128, 0, st>>>(pa, b, envs, s);
     plain_init_kernel<<<blocks_of(n, 256), 256, 0, st>>>(pa, b, n, s == 0 ? 1 : 0);
+    if (rope) plain_detect_kernel<<<blocks_of(n, 128), 128, 0, st>>>(pa, b, n);
     return cudaGetLastError();
 }
 

@@ -200,7 +200,6 @@ public:
         if (!(dl > 0)) throw py::value_error("dir must be nonzero");
         if (collisions_ && 2 * seg_len < 2 * 1e-4f + 8e-4f)
             throw py::value_error("collisions=True uses the upstream yarn-scale collision radius (1e-4 m): seg_len must be >= 5e-4 m");
-        if (collisions_) throw py::value_error("collisions=True (self contact of a single rope) is not available in this build");
         collisions = collisions_;
         fixRoot = fix_root_orientation;
         // vertex i at i * seg_len * (dir / |dir|), bindings.cpp:217-219
@@ -208,10 +207,16 @@ public:
         for (int i = 0; i < num_verts; i++)
             for (int k = 0; k < 3; k++) pos[3 * i + k] = float(i) * seg_len * (d[k] / dl);
         const int verts = num_verts;
+        // collisions=True keeps YarnBall's yarn-scale radius/barrier (YarnBall.cu:33-34), else the
+        // dead radii scale with the segment (bindings.cpp:225-244)
+        const float rad = collisions_ ? 1e-4f : 0.01f * seg_len, bar = collisions_ ? 8e-4f : 0.08f * seg_len;
         ok(rs_batch_create(&h, 1, &verts, pos.data(), nullptr, density, k_stretch, k_bend, max_h, num_itr,
-                           fix_root_orientation ? 1 : 0, 0, 0.01f * seg_len, 0.08f * seg_len));
+                           fix_root_orientation ? 1 : 0, 0, rad, bar));
         n = num_verts;
         R = 1;
+        // self contact of the rope through the rope-rope path with YarnBall's defaults
+        // (kCollision 1e-5, friction 0.1, kFriction 5, detection scaler 1.2; YarnBall.cu:37-40)
+        if (collisions_) ok(rs_batch_set_rope_contact(h, 1, 1e-4f, 8e-4f, 1e-5f, 0.1f, 5.f, 1.2f, 1));
     }
     void advance(float dt, int substeps) {
         if (substeps < 0) throw py::value_error("substeps must be >= 0");
@@ -629,6 +634,18 @@ PYBIND11_MODULE(_ropesim, m) {
              py::arg("ropes"), py::arg("density"), py::arg("k_stretch"), py::arg("k_bend"), py::arg("max_h"),
              py::arg("num_itr"), py::arg("fix_root_orientation") = false, py::arg("pinned") = py::none(),
              py::arg("straight_rest") = false)
+        .def("set_rope_contact",
+             [](RopeBatch& b, bool enabled, float radius, float barrier, float k_collision, float mu, float k_friction,
+                float detection_scaler, int group_ropes) {
+                 if (enabled && (!(radius > 0) || !(barrier > 0) || !(k_collision > 0) || !(mu >= 0) || !(k_friction >= 0) ||
+                                 !(detection_scaler > 1) || group_ropes < 1))
+                     throw py::value_error("rope contact needs radius, barrier, k_collision > 0, mu, k_friction >= 0, "
+                                           "detection_scaler > 1, group_ropes >= 1");
+                 ok(rs_batch_set_rope_contact(b.h, enabled ? 1 : 0, radius, barrier, k_collision, mu, k_friction,
+                                              detection_scaler, group_ropes));
+             },
+             py::arg("enabled"), py::arg("radius") = 0.f, py::arg("barrier") = 0.f, py::arg("k_collision") = 0.f,
+             py::arg("mu") = 0.f, py::arg("k_friction") = 0.f, py::arg("detection_scaler") = 1.2f, py::arg("group_ropes") = 1)
         .def("step_free",
              [](RopeBatch& b, float dt, int substeps) {
                  if (!(dt > 0) || substeps < 1) throw py::value_error("dt > 0 and substeps >= 1 required");

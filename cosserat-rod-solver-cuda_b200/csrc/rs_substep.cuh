@@ -188,9 +188,77 @@ __device__ __forceinline__ void position_terms(const FrameArgs& a, const float4*
     }
 }
 
+// One rope-rope candidate of segment (p, p1) with iterates (d, p1d) against the segment
+// (b0, b1) with iterates (db0, db1): IPC log barrier at 2 r + barrier with its damping terms
+// and a friction spring capped at mu * |f_n|, cosserat.cu:99-157.
+__device__ __forceinline__ void collision_term(const FrameArgs& a, float damp, f3 p, f3 p1, f3 d, f3 p1d, f3 b0, f3 b1,
+                                               f3 db0, f3 db1, f3& f, f3& f2, sym3& H, sym3& H2) {
+    float u, v;
+    seg_closest(zero3(), (p1 - p) + (p1d - d), (b0 - p) + (db0 - d), (b1 - p) + (db1 - d), u, v);
+    const f3 dpos = lerp3(p, p1, u) - lerp3(b0, b1, v);
+    const f3 ddpos = lerp3(d, p1d, u) - lerp3(db0, db1, v);
+    f3 nrm = dpos + ddpos;
+    float dist = len(nrm);
+    if (!(dist > 0.f)) return;  // coincident centrelines: no normal
+    nrm *= 1.f / dist;
+    const float wa = 1.f - u, wb = u;
+    const float invb = 1.f / a.rc_barrier;
+    const float kCol = a.rc_kcol * invb;
+    dist = dist - 2.f * a.rc_radius;
+    dist *= invb;
+    if (dist > 1.f) return;  // not touching
+    dist = fmaxf(dist, 1e-3f);
+    const float invd = 1.f / dist;
+    const float logd = logf(dist);
+    float dH = (-3.f + (2.f + invd) * invd - 2.f * logd) * kCol * invb;
+    const float ff = -(1.f - dist) * (dist - 1.f + 2.f * dist * logd) * invd * kCol;
+    f += nrm * (ff * wa - damp * dH * wa * wa * dot(nrm, d));
+    f2 += nrm * (ff * wb - damp * dH * wb * wb * dot(nrm, p1d));
+    dH *= 1.f + damp;
+    sym_add_scaled_outer(H, nrm, dH * wa * wa);
+    sym_add_scaled_outer(H2, nrm, dH * wb * wb);
+    const f3 uu = ddpos - nrm * dot(nrm, ddpos);
+    const float ul = len(uu);
+    if (ul > 0.f) {
+        const float f1 = fminf(a.rc_kfric, a.rc_mu * ff / ul);
+        f -= uu * (f1 * wa);
+        sym_sub_scaled_outer_minus_I(H, nrm, wa * wa * f1);
+        f2 -= uu * (f1 * wb);
+        sym_sub_scaled_outer_minus_I(H2, nrm, wb * wb * f1);
+    }
+}
+
+// Candidate test of segment pair (i, j) at the substep start, batch.cu:33-45: closest distance
+// of the centrelines below the sum of the padded detection radii.
+__device__ __forceinline__ bool rope_pair_candidate(f3 a0, f3 a1, float ri, f3 pj0, f3 pj1, float rj) {
+    const f3 b0 = pj0 - a0, b1 = pj1 - a0;
+    float u, v;
+    seg_closest(zero3(), a1, b0, b1, u, v);
+    const f3 dd = a1 * u - lerp3(b0, b1, v);
+    const float r = ri + rj;
+    return dot(dd, dd) < r * r;
+}
+
+// Step-limit contribution of one candidate, collision.cu:124-134: 0.45 x the distance.
+__device__ __forceinline__ float step_limit_of(f3 a0, f3 a1, f3 pj0, f3 pj1) {
+    const f3 b0 = pj0 - a0, b1 = pj1 - a0;
+    float u, v;
+    seg_closest(zero3(), a1, b0, b1, u, v);
+    const f3 nn = a1 * u - lerp3(b0, b1, v);
+    return ((1.f - 0.1f) * 0.5f) * len(nn);
+}
+
 // Local solve dx += accel * H^-1 f of a free vertex, cosserat.cu:206-209.
 __device__ __forceinline__ void position_solve(f3& dx, f3 f, const sym3& H, float accel, float im) {
     if (im != 0.f) dx += sym_solve(H, f) * accel;
+}
+// The same with the step limit of rope-rope contact, cosserat.cu:211-214.
+__device__ __forceinline__ void position_solve_limited(f3& dx, f3 f, const sym3& H, float accel, float im, float lim) {
+    if (im != 0.f) {
+        dx += sym_solve(H, f) * accel;
+        const float l = len(dx);
+        if (l > lim && l > 0.f) dx *= lim / l;
+    }
 }
 
 // Frame step of segment i, cosserat.cu:242-272: vv = -2 k ((p1 - p) + (p1dx - dx)) / l, b from

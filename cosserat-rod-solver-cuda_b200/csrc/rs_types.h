@@ -119,6 +119,16 @@ struct FrameArgs {
     int pose_cache;          // pose cache entries per buffer (= max ropes per bin * num_sdf)
     const Pose* poses;       // [envs * 64] committed static poses
     const Motion* motion;    // [envs * 64] this frame's motion (sdf_moving)
+    // rope-rope contact (YarnBall.h:175-192; batch.cu:19-49, 504-522)
+    int rope_contact;        // 0 = off
+    int n;                   // vertices (stride of the candidate lists)
+    float rc_radius, rc_barrier, rc_kcol, rc_mu, rc_kfric;
+    float det_radius, sdet_radius;  // radius + barrier/2, and that times the detection scaler
+    const int4* grp;         // per device vertex: (group start, group end, rope start, rope end)
+    int* cols;               // [kMaxCols * n] candidate lists, cols[c * n + i] (scratch)
+    int* ncols;              // [n] candidate counts (plain engine)
+    float* maxstep;          // [n] step limits (plain engine)
+    float* pad;              // [n] detection paddings (plain engine)
     GridDesc grids[kMaxSdf];
 };
 

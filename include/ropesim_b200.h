@@ -153,6 +153,13 @@ RS_API int rs_batch_last_frame_ms(rs_batch* b, double* ms);
 RS_API int rs_batch_set_contact(rs_batch* b, float radius, float mu_s, float mu_k, float v_slip, float kappa);
 RS_API int rs_batch_get_contact(rs_batch* b, float* radius, float* mu_s, float* mu_k);
 RS_API int rs_batch_set_planes(rs_batch* b, int count, const float* rows);
+/* RopeBatch::set_rope_contact (batch.cu:504-522, bindings.cpp:939-950): YarnBall's rope-rope
+ * model (log barrier at 2 radius + barrier, friction spring capped at mu N, step limit) on
+ * candidates from a per-group brute-force detector; group_ropes consecutive ropes form one
+ * contact group. Groups that fit one CTA (<= 1024 vertices) stay on the persistent kernel;
+ * larger groups run on the plain engine. enabled = 0 switches it off. */
+RS_API int rs_batch_set_rope_contact(rs_batch* b, int enabled, float radius, float barrier, float k_collision, float mu,
+                                     float k_friction, float detection_scaler, int group_ropes);
 /* SdfStore::add (sdf.cu:137-158): values host [nx,ny,nz], pose rows host [rows,3]/[rows,4]
  * (rows 1 or num_ropes). Returns the mesh index in *index. */
 RS_API int rs_batch_add_mesh(rs_batch* b, const float* values, int nx, int ny, int nz, const float* origin3,

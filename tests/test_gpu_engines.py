@@ -47,7 +47,7 @@ def test_plain_engine_matches_persistent_program():
     print(f"\n  persistent vs plain after 10 frames: positions {dp:.2e} m, frames {np.abs(a[2] - p[2]).max():.2e}")
     assert dp <= 5e-6
     np.testing.assert_allclose(a[2], p[2], atol=1e-4)
-    np.testing.assert_allclose(a[1], p[1], atol=1e-3)
+    np.testing.assert_allclose(a[1], p[1], atol=2e-2)  # velocity = dx / h amplifies position rounding by 6000
 
 
 def test_plain_engine_matches_persistent_meshes():
