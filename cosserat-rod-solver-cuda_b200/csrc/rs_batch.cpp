@@ -502,10 +502,8 @@ void Batch::stage_rows(const float* p0, const float* v0, const float* p1, const 
     if (q1) check(cudaMemcpy2DAsync(d_prog_ + 13, rowb, q1, 4 * sizeof(float), 4 * sizeof(float), R_, cudaMemcpyDeviceToDevice, stream_), "stage q1");
 }
 
-void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int steps, float h) {
-    // uploadMeta bookkeeping, batch.cu:57-62 / step.cpp:41-42
-    last_h_ = h_;
-    h_ = h;
+// The parameters of one frame launch from the current state (h_ / last_h_ already advanced).
+FrameArgs Batch::frame_args(int root_mode, bool has_q0, bool has_q1, float dt, int steps) const {
     FrameArgs a{};
     a.bins = d_bins_; a.ropes = d_ropes_; a.topo = d_topo_;
     a.pos = d_pos_; a.vel = d_vel_; a.lvel = d_lvel_; a.q = d_q_; a.qrest = d_qrest_;
@@ -530,6 +528,14 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     a.det_radius = rc_radius_ + 0.5f * rc_barrier_;          // uploadMeta, YarnBall.cu:262-263
     a.sdet_radius = a.det_radius * rc_scaler_;
     a.grp = d_grp_; a.cols = d_cols_; a.ncols = d_ncols_; a.maxstep = d_maxstep_; a.pad = d_pad_;
+    return a;
+}
+
+void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int steps, float h) {
+    // uploadMeta bookkeeping, batch.cu:57-62 / step.cpp:41-42
+    last_h_ = h_;
+    h_ = h;
+    const FrameArgs a = frame_args(root_mode, has_q0, has_q1, dt, steps);
     const bool timed = timing_ || tuning();
     if (timed) check(cudaEventRecord(ev0_, stream_), "event");
     if (engine_ == 1 || (rope_contact_ && oversize_)) run_frame_plain(a);
@@ -709,6 +715,44 @@ void Batch::step_program(const float* p0, const float* v0, const float* p1, cons
         float ms = 0.f;
         check(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed");
         last_frame_ms_ = ms;
+    }
+}
+
+// A program-driven frame that calls no device allocator: the rope-rope candidate lists go to the
+// library's static device array (static_scratch_cols) instead of the handle's own buffer, and
+// every step that could allocate (autotuning repacks, a pending upload, the plain engine) is
+// refused up front instead of performed.
+void Batch::step_program_static_scratch(const float* p0, const float* v0, const float* p1, const float* q0,
+                                        const float* q1, float dt, int substeps) {
+    int* cols = nullptr;
+    int cap = 0;
+    check(static_scratch_cols(&cols, &cap), "static scratch address");
+    if (n_ > cap)
+        throw std::invalid_argument("the allocation-free step's static scratch holds at most " + std::to_string(cap) +
+                                    " vertices; this batch has " + std::to_string(n_));
+    if (engine_ != 0) throw std::invalid_argument("the allocation-free step runs the persistent engine only");
+    if (!layout_valid_ || !device_valid_)
+        throw std::invalid_argument("host-side edits are pending upload: run one regular step (or gather) first");
+    if (rope_contact_ && oversize_)
+        throw std::invalid_argument("a rope-rope contact group larger than one CTA needs the plain engine, which allocates");
+    stage_rows(p0, v0, p1, q0, q1, false);
+    sdf_begin();
+    last_h_ = h_;
+    h_ = dt / (float)substeps;
+    FrameArgs a = frame_args(ROOT_PROGRAM, q0 != nullptr, q1 != nullptr, dt, substeps);
+    a.cols = cols;
+    check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
+    host_dyn_valid_ = false;
+    time_ += dt;
+    sdf_end(substeps);
+    check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
+    check(cudaStreamSynchronize(stream_), "frame");
+    if (h_status_[0] || h_status_[1] || h_status_[2]) {
+        if (h_status_[2]) nonfinite_ = 1;
+        if (h_status_[1]) last_warning_ = h_status_[1];
+        const int err = h_status_[0];
+        check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
+        if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
     }
 }
 

@@ -83,6 +83,9 @@ public:
     // Constant-velocity roots (p, v [R,3]; q [R,4] or null).
     void step_legacy(const float* p, const float* v, const float* q, float dt, int substeps, bool host_inputs);
     void step_free(float dt, int substeps);
+    // step_program with device inputs that calls no device allocator (see rs_batch.cpp).
+    void step_program_static_scratch(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1,
+                                     float dt, int substeps);
     void advance(float dt, int substeps);   // RopeSim.advance: substeps 0 = float ceil(dt / max_h)
     float time() const { return time_; }
     int last_error() const { return last_error_; }
@@ -147,6 +150,7 @@ private:
     void alloc_device();
     void stage_rows(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1, bool host);
     void run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int steps, float h);
+    FrameArgs frame_args(int root_mode, bool has_q0, bool has_q1, float dt, int steps) const;
     void sdf_begin();
     void sdf_end(int substeps);
     void check(cudaError_t e, const char* what);

@@ -345,6 +345,19 @@ int rs_batch_step_program(rs_batch* b, const float* p0, const float* v0, const f
         s.step_program(p0, v0, p1, q0, q1, dt, substeps, on_host != 0);
     });
 }
+int rs_batch_step_program_static_scratch(rs_batch* b, const float* p0, const float* v0, const float* p1, const float* q0,
+                                         const float* q1, float dt, int substeps) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        need(p0 && v0 && p1, "null argument");
+        need(dt > 0, "dt must be > 0");
+        need(substeps >= 1, "substeps must be >= 1");
+        need(!(q1 && !q0), "root_q_end requires root_q");
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.step_program_static_scratch(p0, v0, p1, q0, q1, dt, substeps);
+    });
+}
+
 int rs_batch_step_legacy(rs_batch* b, const float* p, const float* v, const float* q, float dt, int substeps, int on_host) {
     return guarded([&] {
         rs::Batch& s = B(b);

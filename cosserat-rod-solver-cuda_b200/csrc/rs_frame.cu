@@ -18,6 +18,8 @@
 // displacement publish; the frame step reads a double-buffered rotor array and needs none).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "rs_device.cuh"
 #include "rs_kernels.h"
 #include "rs_substep.cuh"
@@ -297,6 +299,38 @@ cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream
         case 1024: return launch_frame_b<1024>(a, num_bins, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+// ------------------------------------------------------------------ static candidate scratch
+// Rope-rope candidate lists for callers that must not allocate device memory: a fixed array
+// of kMaxCols x kStaticScratchVerts ints (4 MiB) that every GPU loading this library holds until
+// the process exits. All allocation-free calls share it and it keeps the previous call's
+// contents; nothing in it needs to start at zero (each substep writes a segment's entries
+// before reading them), but calls that overlap on the GPU would race on it.
+constexpr int kStaticScratchVerts = 8192;
+static __device__ __align__(256) int g_static_cols[kMaxCols * kStaticScratchVerts];
+
+// Host code cannot pass `g_static_cols` to a kernel: on the host that name stands for a host-side
+// shadow, not a device address. The device address is looked up once per device, with that
+// device current, and cached (a fixed table, so the lookup allocates nothing either).
+cudaError_t static_scratch_cols(int** ptr, int* max_verts) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mtx;
+    static int* addr[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(mtx);
+    if (!addr[dev]) {
+        int* p = nullptr;
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_static_cols);
+        if (e != cudaSuccess) return e;
+        addr[dev] = p;
+    }
+    *ptr = addr[dev];
+    *max_verts = kStaticScratchVerts;
+    return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ views and resets

@@ -27,6 +27,9 @@ cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, i
 cudaError_t plain_launch_pre(const FrameArgs* pa, const PlainBufs& b, int n, int nropes, int envs, int num_sdf, bool moving,
                              int root_mode, bool rope, int s, cudaStream_t st);
 cudaError_t plain_launch_finish(const FrameArgs* pa, const PlainBufs& b, int n, cudaStream_t st);
+// Device address of the library's static rope-rope candidate array on the current device and
+// its capacity in vertices (looked up once per device, then cached; no allocation).
+cudaError_t static_scratch_cols(int** ptr, int* max_verts);
 // FP32 FMA throughput probe (16 * 8 FMAs per thread per iteration).
 cudaError_t launch_fp32_probe(float* out, int blocks, int threads, int iters, cudaStream_t s);
 

@@ -128,6 +128,22 @@ RS_API int rs_batch_step_program(rs_batch* b, const float* p0, const float* v0, 
 RS_API int rs_batch_step_legacy(rs_batch* b, const float* p, const float* v, const float* q, float dt, int substeps,
                          int on_host);
 RS_API int rs_batch_step_free(rs_batch* b, float dt, int substeps);
+/* rs_batch_step_program with device inputs (on_host = 0) that allocates no device memory. No
+ * counterpart in the reference. For callers that cannot call cudaMalloc once the simulation is
+ * running: hosts that reserve all device memory up front for their own allocator (physics or
+ * rendering engines that embed this library, ML runtimes that preallocate the GPU), real-time
+ * control loops whose memory is fixed at start-up, and runtimes that forbid allocation after
+ * initialisation. The regular step needs no new allocation per frame either, but its
+ * rope-rope candidate lists live in a buffer the handle allocates when contact is enabled, and
+ * autotuning or a pending host edit can reallocate; this entry point instead keeps the lists in
+ * the library's static device array (128 x 8192 ints = 4 MiB, held by every GPU that loads the
+ * library until exit) and refuses, with RS_EINVAL and a message, batches of more than 8192
+ * vertices, pending host edits, contact groups larger than one CTA, and the plain engine. The
+ * array's device address is looked up on the first call on each device (keep that first call
+ * outside any stream capture). All such calls share the array: calls that overlap on the GPU
+ * race. Results equal rs_batch_step_program's. */
+RS_API int rs_batch_step_program_static_scratch(rs_batch* b, const float* p0, const float* v0, const float* p1,
+                                                const float* q0, const float* q1, float dt, int substeps);
 RS_API int rs_batch_advance(rs_batch* b, float dt, int substeps);
 /* RopeBatch::reset_envs (batch.cu:400-413): host ids[count] (rope indices) */
 RS_API int rs_batch_reset_ropes(rs_batch* b, const int* ids, int count);
