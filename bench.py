@@ -234,6 +234,131 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def config3_scene(n_ropes, seed=3):
+    """Config 3: n_ropes uneven ropes, V ~ U{16..256} at 2 cm, EA log-U[1e2, 1e4] and
+    EI log-U[1e-5, 1e-2] per rope, per-vertex masses x U[0.8, 1.2], two planes, eight meshes
+    (sphere, box, capsule closed forms baked to 64^3 float32 lattices) with per-env poses."""
+    from ropesim import sdf
+
+    rng = np.random.default_rng(seed)
+    verts = rng.integers(16, 257, n_ropes)
+    g = int(np.ceil(np.sqrt(n_ropes)))
+    ropes = []
+    for r in range(n_ropes):
+        L = 0.02 * (verts[r] - 1)
+        root = np.array([(r % g) * 0.7, (r // g) * 0.7, 0.06 + 0.97 * L])
+        tilt = np.deg2rad(rng.uniform(5, 20))
+        az = rng.uniform(0, 2 * np.pi)
+        d = np.array([np.sin(tilt) * np.cos(az), np.sin(tilt) * np.sin(az), -np.cos(tilt)])
+        pts = root + np.outer(np.arange(verts[r]) * 0.02, d)
+        pts[1:] += rng.normal(0, 1e-3, (verts[r] - 1, 3))
+        ropes.append(pts.astype(np.float32))
+    ea = np.exp(rng.uniform(np.log(1e2), np.log(1e4), n_ropes))
+    ei = np.exp(rng.uniform(np.log(1e-5), np.log(1e-2), n_ropes))
+    ea_v = np.concatenate([np.full(v, ea[i]) for i, v in enumerate(verts)]).astype(np.float32)
+    ei_v = np.concatenate([np.full(v, ei[i]) for i, v in enumerate(verts)]).astype(np.float32)
+    m_v = []
+    for i, rope in enumerate(ropes):
+        seg = np.linalg.norm(np.diff(rope.astype(np.float64), axis=0), axis=1)
+        m = np.zeros(len(rope))
+        m[:-1] += 0.5 * 0.117 * seg
+        m[1:] += 0.5 * 0.117 * seg
+        m_v.append(m * rng.uniform(0.8, 1.2, len(rope)))
+    m_v = np.concatenate(m_v).astype(np.float32)
+    n64 = lambda lo, hi: (hi - lo) / 63.0
+    grids = [sdf.from_function(sdf.sdf_sphere(0.12), [-0.2] * 3, [0.2] * 3, n64(-0.2, 0.2)),
+             sdf.from_function(sdf.sdf_box([0.12, 0.08, 0.06], round=0.01), [-0.2] * 3, [0.2] * 3, n64(-0.2, 0.2)),
+             sdf.from_function(sdf.sdf_capsule(0.06, 0.12, axis=0), [-0.2] * 3, [0.2] * 3, n64(-0.2, 0.2))]
+    grids = [grids[i % 3] for i in range(8)]
+    return ropes, verts, ea_v, ei_v, m_v, grids
+
+
+def build_config3(ropesim, scene, engine):
+    ropes, verts, ea_v, ei_v, m_v, grids = scene
+    b = ropesim.RopeBatch.from_ropes(ropes, 0.117, 1000.0, 1e-3, H, ITERS)
+    b.set_stretch_stiffnesses(ea_v)
+    b.set_bend_stiffnesses(ei_v)
+    b.set_masses(m_v)
+    b.set_engine(engine)
+    b.set_gravity(np.array([0, 0, -9.81], np.float32))
+    b.damping = 0.0
+    b.drag = 0.2
+    b.set_planes(np.array([[0, 0, 1, 0], [0.05, 0.0, 1.0, -0.02]], np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
+    for gd in grids:
+        b.add_mesh(*gd.as_args())
+    return b
+
+
+def run_config3(args):
+    """Config 3 forward: persistent (autotuned bins) vs the plain per-substep path, same inputs."""
+    import torch
+
+    import ropesim
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import scenarios as Sc
+
+    torch.cuda.set_device(0)
+    R = args.ropes if args.ropes != 4096 else 8192
+    scene = config3_scene(R)
+    ropes, verts = scene[0], scene[1]
+    nv = int(np.sum(verts))
+    rng = np.random.default_rng(17)
+    M = 8
+    frames = args.warmup + args.steps
+    # per-env mesh poses: next to each rope along its length, then a random rigid walk
+    pos0 = np.zeros((R, M, 3), np.float32)
+    for r, rope in enumerate(ropes):
+        L = 0.02 * (len(rope) - 1)
+        for m in range(M):
+            pos0[r, m] = rope[0] + np.array([0.25 * np.cos(0.8 * m), 0.25 * np.sin(0.8 * m), -(0.15 + 0.1 * m) * L])
+    q0 = np.zeros((R, M, 4), np.float32)
+    q0[..., 3] = 1.0
+    poses = []
+    p, q = pos0, q0
+    for f in range(frames):
+        poses.append((torch.as_tensor(p, device="cuda"), torch.as_tensor(q, device="cuda")))
+        p, q = Sc.walk_poses(rng, p, q, step=0.003, ang=0.02)
+    roots = np.stack([r[0] for r in ropes]).astype(np.float32)
+    prog = []
+    cur = roots.copy()
+    for f in range(frames):
+        v0 = rng.normal(0, 0.1, (R, 3)).astype(np.float32)
+        p1 = (cur + rng.normal(0, 0.01, (R, 3))).astype(np.float32)
+        prog.append(tuple(torch.as_tensor(x, device="cuda") for x in (cur, v0, p1)))
+        cur = p1
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {}
+    for engine in ("persistent", "plain"):
+        b = build_config3(ropesim, scene, engine)
+        st = torch.cuda.ExternalStream(b.stream_ptr())
+        ms = []
+        for f in range(frames):
+            b.set_mesh_poses_all(poses[f][0], poses[f][1], teleport=(f == 0))
+            if f >= args.warmup:
+                flush.fill_(float(f))
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+            b.step(prog[f][0], prog[f][1], DT, S, root_pos_end=prog[f][2])
+            if f >= args.warmup:
+                e1.record(st)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        pos = torch.as_tensor(b.positions()).cpu().numpy()
+        out[engine] = {"ms_per_step": float(np.mean(ms)), "value": nv * S * len(ms) / (sum(ms) * 1e-3),
+                       "finite": bool(np.isfinite(pos).all()), "layout": list(b.layout())}
+        del b
+    line = {"metric": METRIC, "value": out["persistent"]["value"], "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["persistent"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-3 scene)",
+            "config": {"workload": f"config3-uneven-{R}", "ropes": R, "verts": nv, "verts_per_rope": "U{16..256}",
+                       "substeps": S, "num_itr": ITERS, "planes": 2, "meshes": M, "lattice": "64^3",
+                       "l2": "flushed between frames (256 MB write)"},
+            "persistent": out["persistent"], "plain_path": out["plain"],
+            "speedup_vs_plain": out["persistent"]["value"] / out["plain"]["value"]}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -406,12 +531,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     ap.add_argument("--block", type=int, default=0, help="bin size (CTA threads); 0 = the library's choice")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3"],
+                    help="config2 (the headline line) or config3 (uneven ropes, planes and meshes vs the plain path)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     N_ROPES = args.ropes
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "config3":
+        run_config3(args)
     else:
         run_ours(args)
 
