@@ -1,0 +1,522 @@
+// rs_adjoint.cu -- reverse-mode adjoint of one control frame (the differentiable path) and the
+// state / parameter transfer kernels it needs.
+//
+// The reference has no gradients. What is differentiated is the deterministic (Jacobi) substep
+// the frame kernel runs: root program (batch.cu:122-159), inertial prediction with the
+// acceleration-projected gravity (iteration.cu:34-68), num_itr x (position step with inertia,
+// plane contact + friction, stretch and damping, cosserat.cu:37-88,198-209; frame step,
+// cosserat.cu:242-272), velocity with linear and quadratic drag (iteration.cu:85-112). Every
+// iteration is reversed (not only the converged state); branches that switch terms (contact
+// active, friction regime, frame-step signs, clamps) are held where the forward pass took them.
+//
+// Data flow of one frame's backward (Batch::backward_program):
+//   1. the frame is replayed by frame_kernel from the frame-start checkpoint, writing the state
+//      after each substep's root program to a tape [S][4][n] (x, v, lv, q) in HBM;
+//   2. adjoint_kernel (one CTA per bin, one thread per vertex, like the forward) walks the
+//      substeps backwards: it recomputes the substep's iterates d^k, q^k into shared memory
+//      from the tape, then reverses end -> frame/position steps -> init -> root program.
+// Per reverse iteration two CTA barriers: the frame step's neighbour rotor/segment adjoints,
+// then the position step's force adjoints. Cross-vertex contributions are gathered by the
+// receiving vertex, so no atomics are used and the result is deterministic.
+//
+// Reverse of the local solve d' = d + a H^-1 F (H symmetric): F̄ = a H^-1 ḡ, H̄ = -(H^-1 ḡ) δᵀ,
+// δ = d' - d. Quaternion products c = a b reverse as ā = c̄ b*, b̄ = a* c̄.
+#include <cuda_runtime.h>
+
+#include "rs_device.cuh"
+#include "rs_kernels.h"
+#include "rs_substep.cuh"
+#include "rs_types.h"
+
+using namespace rsd;
+
+namespace rs {
+
+namespace {
+
+__device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+__device__ __forceinline__ f3 ld3(const float* a, int u) { return mk3(a[3 * u], a[3 * u + 1], a[3 * u + 2]); }
+__device__ __forceinline__ void st3(float* a, int u, f3 v) { a[3 * u] = v.x; a[3 * u + 1] = v.y; a[3 * u + 2] = v.z; }
+
+// Transposed Jacobian of the tangent t(q) = q e_x q*.
+__device__ __forceinline__ float4 tangent_vjp(float4 q, f3 tb) {
+    return make_float4(2.f * (q.x * tb.x + q.y * tb.y + q.z * tb.z), 2.f * (-q.y * tb.x + q.x * tb.y - q.w * tb.z),
+                       2.f * (-q.z * tb.x + q.w * tb.y + q.x * tb.z), 2.f * (q.w * tb.x + q.z * tb.y - q.y * tb.z));
+}
+
+// Plane contact (contact.cuh:27-46) reversed, given F̄ and the contractions n·H̄n and tr H̄:
+// adds to d̄, returns the adjoints of the gap and of the penalty stiffness k.
+__device__ __forceinline__ void surface_contact_bwd(f3 n, float gap, f3 d, float k, float h, float muS, float muK,
+                                                    float eps, f3 Fb, float nHn, float trHb, f3& db, float& gapb,
+                                                    float& kb) {
+    const float N = -k * gap;
+    const f3 ut = d - n * dot(n, d);
+    const float ul = len(ut);
+    const float vt = ul / h;
+    float Nb = dot(n, Fb);
+    kb = nHn;
+    float kt, mu = 0.f, xr = 0.f;
+    if (vt <= eps) kt = muS * N / (eps * h);
+    else {
+        xr = vt / eps - 1.f;
+        const float sw = 1.f - fminf(1.f, xr);
+        mu = sw * muS + (1.f - sw) * muK;
+        kt = mu * N / ul;
+    }
+    f3 utb = Fb * (-kt);
+    const float ktb = -dot(ut, Fb) - (nHn - trHb);
+    if (vt <= eps) Nb += ktb * muS / (eps * h);
+    else {
+        Nb += ktb * mu / ul;
+        float ulb = -ktb * mu * N / (ul * ul);
+        if (xr < 1.f) ulb -= ktb * (muS - muK) * N / ul / (eps * h);
+        utb += ut * (ulb / ul);
+    }
+    db += utb - n * dot(n, utb);
+    kb += -gap * Nb;
+    gapb = -k * Nb;
+}
+
+// Shared memory of the adjoint kernel, in float4 units (BLOCK = bin size, I = iterations):
+//   X, QR, KC, EA, EB, EC, EF, ES   one slot per vertex each
+//   LD [I+1][BLOCK]   displacement iterates d^k
+//   LE [I][BLOCK]     increments δ^k = d^{k+1} - d^k as the solve produced them
+//   LQ [I+1][BLOCK]   frame iterates q^k
+template <int BLOCK, int SURF>
+__global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const AdjArgs g) {
+    extern __shared__ float4 smem[];
+    const int I = a.iters;
+    float4* X = smem;
+    float4* QR = X + BLOCK;
+    float4* KC = QR + BLOCK;   // (kStretch, 1 / lRest, invMass, -)
+    float4* EA = KC + BLOCK;
+    float4* EB = EA + BLOCK;
+    float4* EC = EB + BLOCK;
+    float4* EF = EC + BLOCK;
+    float4* ES = EF + BLOCK;
+    float4* LD = ES + BLOCK;
+    float4* LE = LD + (size_t)(I + 1) * BLOCK;
+    float4* LQ = LE + (size_t)I * BLOCK;
+
+    const Bin bin = a.bins[blockIdx.x];
+    const int t = threadIdx.x;
+    const bool act = t < bin.vcount;
+    const int dv = bin.vstart + t;
+    uint32_t fl = 0;
+    int uidx = 0, env = 0;
+    float im = 0.f, lr = 1.f, ks = 0.f;
+    QR[t] = make_float4(0.f, 0.f, 0.f, 1.f);
+    if (act) {
+        const int4 tp = a.topo[dv];
+        fl = (uint32_t)tp.x; uidx = tp.z; env = tp.w;
+        im = a.pos[dv].w; lr = a.vel[dv].w; ks = a.lvel[dv].w;
+        QR[t] = a.qrest[dv];
+    }
+    const bool hasNext = fl & F_NEXT, hasPrev = fl & F_PREV, nextOrient = fl & F_NEXT_ORIENT;
+    const bool upd = hasNext && !(fl & F_FIX_ORIENT);
+    const bool driven = (fl & F_ROOT) && a.root_mode == ROOT_PROGRAM;
+    const VConst c = vertex_constants(a, im, lr, ks);
+    KC[t] = make_float4(ks, c.invl, im, 0.f);
+    const float h = a.h, invH = 1.f / h;
+    const float damp = a.damping / h;
+    const f3 gv = mk3(a.gx, a.gy, a.gz);
+    const float g2 = dot(gv, gv);
+    const int S = a.substeps;
+    const size_t n = (size_t)a.n;
+
+    // adjoints of the frame-end state
+    f3 xb = zero3(), vb = zero3(), lvb = zero3();
+    float4 qb = zero4();
+    if (act) {
+        if (g.g_pos) xb = ld3(g.g_pos, uidx);
+        if (g.g_vel) vb = ld3(g.g_vel, uidx);
+        if (g.g_lvel) lvb = ld3(g.g_lvel, uidx);
+        if (g.g_q) qb = reinterpret_cast<const float4*>(g.g_q)[uidx];
+    }
+    f3 P0b = zero3(), V0b = zero3(), P1b = zero3();
+    float ksb = 0.f, rhob = 0.f, rhobp = 0.f, wb = 0.f;
+
+    for (int s = S - 1; s >= 0; s--) {
+        // ---- the substep's start state (after its root program) from the tape
+        f3 p = zero3(), v = zero3(), lvin = zero3();
+        float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (act) {
+            const float4* tp = g.tape + (size_t)s * 4 * n + dv;
+            p = xyz(tp[0]); v = xyz(tp[n]); lvin = xyz(tp[2 * n]); q = tp[3 * n];
+        }
+        f3 dx, y;
+        init_vertex(v, lvin, im, h, a.last_h, gv, g2, dx, y);
+        X[t] = f4(p, 0.f);
+        LD[t] = f4(dx, 0.f);
+        LQ[t] = q;
+        __syncthreads();
+        const f3 p1 = hasNext ? xyz(X[t + 1]) : zero3();
+
+        // ---- recompute the iterates (the frame kernel's arithmetic)
+        for (int k = 0; k < I; k++) {
+            f3 f, f2;
+            sym3 H, H2;
+            const f3 p1dx = hasNext ? xyz(LD[(size_t)k * BLOCK + t + 1]) : zero3();
+            position_terms<SURF>(a, nullptr, 0ull, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            EA[t] = f4(f2, H2.xx);
+            EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
+            EC[t].x = H2.yz;
+            __syncthreads();
+            if (hasPrev) {
+                const float4 fa = EA[t - 1], fb = EB[t - 1];
+                f += xyz(fa);
+                H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
+            }
+            f3 del = zero3();
+            if (im != 0.f) del = sym_solve(H, f) * a.accel;
+            dx += del;
+            LE[(size_t)k * BLOCK + t] = f4(del, 0.f);
+            LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, 0.f);
+            __syncthreads();
+            if (upd) {
+                const f3 seg = (p1 - p) + (xyz(LD[(size_t)(k + 1) * BLOCK + t + 1]) - dx);
+                const float4* Lk = LQ + (size_t)k * BLOCK;
+                q = frame_update(q, seg, c.invl, ks, hasPrev, hasPrev ? Lk[t - 1] : q, hasPrev ? QR[t - 1] : q, nextOrient,
+                                 nextOrient ? Lk[t + 1] : q, QR[t]);
+            }
+            LQ[(size_t)(k + 1) * BLOCK + t] = q;
+        }
+        __syncthreads();
+
+        // ---- end of substep reversed: x' = x + d, v' = drag(d / h), lv' = v
+        f3 db = xb;
+        f3 vbn = lvb, lvbn = zero3(), yb = zero3();
+        float4 qpart = zero4();   // quadratic-drag share on the previous vertex's frame (rope ends)
+        if (im != 0.f) {
+            const f3 ob = vb * (1.f - a.drag * h);
+            f3 vbar = ob;
+            if (a.drag_quad > 0.f) {
+                const float4 tq = hasNext ? q : LQ[(size_t)I * BLOCK + t - 1];
+                const f3 tg = qtangent(tq);
+                const f3 vv = dx * invH;
+                const float tv = dot(tg, vv);
+                const f3 vt = tg * tv, vn = vv - vt;
+                const float ln = len(vn), Dn = 1.f + a.drag_quad * ln * h;
+                const float lt = len(vt), Dt = 1.f + a.drag_quad_t * lt * h;
+                f3 vnb = ob / Dn;
+                if (ln > 0.f) vnb -= vn * (a.drag_quad * h * dot(vn, ob) / (ln * Dn * Dn));
+                f3 vtb = ob / Dt;
+                if (lt > 0.f) vtb -= vt * (a.drag_quad_t * h * dot(vt, ob) / (lt * Dt * Dt));
+                vbar = vnb;
+                vtb -= vnb;
+                const float tvb = dot(vtb, tg);
+                vbar += tg * tvb;
+                const float4 qg = tangent_vjp(tq, vtb * tv + vv * tvb);
+                if (hasNext) qb = add4(qb, qg);
+                else qpart = qg;
+            }
+            db += vbar * invH;
+        } else {
+            vbn += vb;  // a pinned vertex keeps its driven velocity
+        }
+        if (a.drag_quad > 0.f) {
+            EF[t] = qpart;
+            __syncthreads();
+            if (hasNext) qb = add4(qb, EF[t + 1]);
+        }
+
+        // ---- iterations reversed
+        for (int k = I - 1; k >= 0; k--) {
+            const float4* Lq = LQ + (size_t)k * BLOCK;
+            // frame step k: q^{k+1}_t = normalize(vv b e1 + (|vv| + |b|) b)
+            float4 own = qb, toL = zero4(), toR = zero4();
+            f3 su = zero3();
+            if (upd) {
+                own = zero4();
+                const float4* Ld = LD + (size_t)(k + 1) * BLOCK;
+                const f3 u = ((p1 - p) + (xyz(Ld[t + 1]) - xyz(Ld[t]))) * c.invl;
+                const f3 vv = u * (-2.f * ks);
+                const float4 q0 = Lq[t];
+                float4 b = zero4(), qp = zero4(), qn = zero4(), rp = zero4(), rn = zero4();
+                float sp = 0.f, sn = 0.f;
+                if (hasPrev) {
+                    qp = Lq[t - 1]; rp = QR[t - 1];
+                    const float4 pr = qmul(qp, rp);
+                    sp = dot4(q0, pr) > 0.f ? 1.f : -1.f;
+                    b = scale4(pr, sp);
+                }
+                if (nextOrient) {
+                    qn = Lq[t + 1]; rn = QR[t];
+                    const float4 nx = qmul(qn, qconj(rn));
+                    sn = dot4(q0, nx) > 0.f ? 1.f : -1.f;
+                    b = add4(b, scale4(nx, sn));
+                }
+                const float lvv = len(vv), lb = sqrtf(dot4(b, b)), lambda = lvv + lb;
+                const float4 z = add4(qmul_e1(qmul_pure(vv, b)), scale4(b, lambda));
+                const float izl = 1.f / sqrtf(dot4(z, z));
+                const float4 qo = scale4(z, izl);
+                const float4 zb = scale4(add4(qb, scale4(qo, -dot4(qo, qb))), izl);
+                float4 bb = scale4(zb, lambda);
+                const float lamb = dot4(zb, b);
+                f3 vvb = (lvv > 0.f) ? vv * (lamb / lvv) : zero3();
+                if (lb > 0.f) bb = add4(bb, scale4(b, lamb / lb));
+                const float4 Ab = scale4(qmul_e1(zb), -1.f);   // z = A e1  ->  Ā = z̄ e1* = -(z̄ e1)
+                vvb += xyz(qmul(Ab, qconj(b)));
+                bb = add4(bb, scale4(qmul_pure(vv, Ab), -1.f)); // (vv, 0)* Ā = -(vv, 0) Ā
+                ksb += -2.f * dot(u, vvb);
+                su = vvb * (-2.f * ks * c.invl);
+                if (hasPrev) {
+                    const float4 bq = scale4(bb, sp);
+                    toL = qmul(bq, qconj(rp));
+                    rhobp += dot4(qmul(qconj(qp), bq), rp) / sqrtf(dot4(rp, rp));
+                }
+                if (nextOrient) {
+                    const float4 bq = scale4(bb, sn);
+                    toR = qmul(bq, rn);
+                    rhob += dot4(qconj(qmul(qconj(qn), bq)), rn) / sqrtf(dot4(rn, rn));
+                }
+            }
+            EA[t] = toL;
+            EB[t] = toR;
+            EC[t] = f4(su, 0.f);
+            __syncthreads();
+            qb = own;
+            if (hasPrev) qb = add4(qb, EB[t - 1]);
+            if (hasNext) qb = add4(qb, EA[t + 1]);
+            {
+                f3 dd = -su;
+                if (hasPrev) dd += xyz(EC[t - 1]);
+                db += dd;
+                xb += dd;
+            }
+
+            // position step k: d^{k+1}_t = d^k_t + a H_t^-1 F_t
+            const f3 dk = xyz(LD[(size_t)k * BLOCK + t]);
+            f3 dn = db;
+            f3 Fb = zero3();
+            float trH = 0.f;
+            if (im != 0.f) {
+                sym3 H = sym_diag(c.Hd);
+                if constexpr (SURF != SURF_NONE) {
+                    f3 fdummy = zero3();
+                    for (int pl = 0; pl < a.num_planes; pl++) {
+                        const float4 P = a.planes[pl];
+                        const f3 nrm = mk3(P.x, P.y, P.z);
+                        const float gap = (dot(nrm, p) - P.w) + dot(nrm, dk) - a.c_radius;
+                        if (gap >= 0.f) continue;
+                        surface_contact(nrm, gap, dk, c.kc, h, a.c_mu_s, a.c_mu_k, a.c_vslip, fdummy, H);
+                    }
+                }
+                if (hasNext) {
+                    const float dd = ks * c.invl * c.invl * (1.f + damp);
+                    H.xx += dd; H.yy += dd; H.zz += dd;
+                }
+                if (hasPrev) {
+                    const float4 kp = KC[t - 1];
+                    const float dd = kp.x * kp.y * kp.y * (1.f + damp);
+                    H.xx += dd; H.yy += dd; H.zz += dd;
+                }
+                const f3 e = sym_solve(H, db);
+                const f3 del = xyz(LE[(size_t)k * BLOCK + t]);
+                Fb = e * a.accel;
+                trH = -dot(e, del);
+                yb += Fb * c.fm;
+                dn -= Fb * c.fm;
+                float wsum = (dot(y - dk, Fb) + trH) * (-c.fm / im);
+                if constexpr (SURF != SURF_NONE) {
+                    for (int pl = 0; pl < a.num_planes; pl++) {
+                        const float4 P = a.planes[pl];
+                        const f3 nrm = mk3(P.x, P.y, P.z);
+                        const float gap = (dot(nrm, p) - P.w) + dot(nrm, dk) - a.c_radius;
+                        if (gap >= 0.f) continue;
+                        float gapb, kb;
+                        surface_contact_bwd(nrm, gap, dk, c.kc, h, a.c_mu_s, a.c_mu_k, a.c_vslip, Fb,
+                                            -dot(nrm, e) * dot(nrm, del), trH, dn, gapb, kb);
+                        dn += nrm * gapb;
+                        xb += nrm * gapb;
+                        wsum += kb * (-c.kc / im);
+                    }
+                }
+                wb += wsum;
+            }
+            // segment t's residual c = ((x1 - x) + (d1 - d)) / l - t(q), read before the barrier:
+            // after it a neighbour may already be writing the next substep's iterates
+            const float4 qk = Lq[t];
+            const f3 cc = hasNext ? ((p1 - p) + (xyz(LD[(size_t)k * BLOCK + t + 1]) - dk)) * c.invl - qtangent(qk) : zero3();
+            EF[t] = f4(Fb, trH);
+            ES[t].x = dot(dk, Fb);
+            __syncthreads();
+            if (hasNext) {
+                const float4 Fn4 = EF[t + 1];
+                const f3 Fn = xyz(Fn4);
+                const float kk = ks * c.invl, dd = kk * c.invl;
+                const f3 dF = Fb - Fn;
+                const f3 cb = dF * kk;
+                ksb += dot(cc, dF) * c.invl +
+                       (-damp * (dot(dk, Fb) + ES[t + 1].x) + (1.f + damp) * (trH + Fn4.w)) * c.invl * c.invl;
+                qb = add4(qb, scale4(tangent_vjp(qk, cb), -1.f));
+                dn -= cb * c.invl;
+                xb -= cb * c.invl;
+                dn -= Fb * (damp * dd);
+            }
+            if (hasPrev) {
+                const float4 kp = KC[t - 1];
+                const float kkp = kp.x * kp.y, ddp = kkp * kp.y;
+                const f3 cbp = (xyz(EF[t - 1]) - Fb) * kkp;
+                dn += cbp * kp.y;
+                xb += cbp * kp.y;
+                dn -= Fb * (damp * ddp);
+            }
+            db = dn;
+        }
+
+        // ---- inertial prediction reversed: d^0 = v h + g h² s(v, lv), y = v h + g h²
+        if (im != 0.f) {
+            vbn += (db + yb) * h;
+            if (g2 > 0.f) {
+                const f3 acc = (v - lvin) / a.last_h;
+                const float raw = dot(acc, gv) / g2;
+                if (raw >= 0.f && raw <= 1.f) {  // inclusive at the clamp's ends (as torch.clamp)
+                    const float sb = dot(gv * (h * h), db);
+                    const f3 gs = gv * (sb / (a.last_h * g2));
+                    vbn += gs;
+                    lvbn -= gs;
+                }
+            }
+        } else {
+            vbn += db * h;
+        }
+        // ---- root program reversed: x = P0 + V0 tau + A tau²/2, v = V0 + A (tau + h/2)
+        if (driven) {
+            const float dt = a.dt, tau = float(s) * h, th = tau + 0.5f * h, idt2 = 2.f / (dt * dt);
+            const float xa = 0.5f * tau * tau * idt2;
+            P0b += xb * (1.f - xa) + vbn * (-th * idt2);
+            V0b += xb * (tau - xa * dt) + vbn * (1.f - th * idt2 * dt);
+            P1b += xb * xa + vbn * (th * idt2);
+            xb = zero3();
+            vbn = zero3();
+            if (a.has_q0) qb = zero4();
+        }
+        vb = vbn;
+        lvb = lvbn;
+    }
+
+    // ---- outputs (caller order); segment t's bending adjoint also has vertex t+1's share
+    EA[t] = make_float4(rhobp, 0.f, 0.f, 0.f);
+    __syncthreads();
+    if (act) {
+        st3(g.o_pos, uidx, xb);
+        st3(g.o_vel, uidx, vb);
+        st3(g.o_lvel, uidx, lvb);
+        reinterpret_cast<float4*>(g.o_q)[uidx] = qb;
+        const float rho = rhob + (hasNext ? EA[t + 1].x : 0.f);
+        if (g.o_ea) g.o_ea[uidx] = hasNext ? ksb * lr : 0.f;        // kStretch = EA lRest
+        if (g.o_ei) g.o_ei[uidx] = hasNext ? rho * 4.f / lr : 0.f;  // |qRest| = 4 EI / lRest
+        if (g.o_mass) g.o_mass[uidx] = (im != 0.f) ? -im * im * wb : 0.f;
+        if (driven) {
+            if (g.o_p0) st3(g.o_p0, env, P0b);
+            if (g.o_v0) st3(g.o_v0, env, V0b);
+            if (g.o_p1) st3(g.o_p1, env, P1b);
+        }
+    }
+}
+
+template <int BLOCK, int SURF>
+cudaError_t launch_adjoint_t(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
+    auto k = adjoint_kernel<BLOCK, SURF>;
+    const size_t bytes = adjoint_smem_bytes(BLOCK, a.iters);
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+    }
+    k<<<num_bins, BLOCK, bytes, s>>>(a, g);
+    return cudaGetLastError();
+}
+template <int BLOCK>
+cudaError_t launch_adjoint_b(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
+    if (a.num_planes > 0) return launch_adjoint_t<BLOCK, SURF_PLANES>(a, g, num_bins, s);
+    return launch_adjoint_t<BLOCK, SURF_NONE>(a, g, num_bins, s);
+}
+
+// Caller-order state (pos / vel / lvel [n,3], q [n,4]) into device order, keeping the
+// per-vertex constants stored in the .w lanes (invMass, lRest, kStretch) of `cst_*`.
+__global__ void state_in_kernel(const int4* topo, const float* pos, const float* vel, const float* lvel, const float* q,
+                                const float4* cst_pos, const float4* cst_vel, const float4* cst_lvel, float4* o_pos,
+                                float4* o_vel, float4* o_lvel, float4* o_q, int n) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const int u = topo[d].z;
+    if (pos) o_pos[d] = f4(ld3(pos, u), cst_pos[d].w);
+    if (vel) o_vel[d] = f4(ld3(vel, u), cst_vel[d].w);
+    if (lvel) o_lvel[d] = f4(ld3(lvel, u), cst_lvel[d].w);
+    if (q) o_q[d] = reinterpret_cast<const float4*>(q)[u];
+}
+__global__ void state_out_kernel(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,
+                                 const float4* q, float* o_pos, float* o_vel, float* o_lvel, float* o_q, int n) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const int u = topo[d].z;
+    if (o_pos) st3(o_pos, u, xyz(pos[d]));
+    if (o_vel) st3(o_vel, u, xyz(vel[d]));
+    if (o_lvel) st3(o_lvel, u, xyz(lvel[d]));
+    if (o_q) reinterpret_cast<float4*>(o_q)[u] = q[d];
+}
+// Per-vertex parameters in caller order: EA (kStretch = EA lRest), EI (|qRest| = 4 EI / lRest)
+// on vertices that own a segment, mass (invMass = 1 / mass) on free vertices.
+__global__ void params_in_kernel(const int4* topo, const float* ea, const float* ei, const float* mass, float4* pos,
+                                 const float4* vel, float4* lvel, float4* qrest, int n) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const int4 tp = topo[d];
+    const int u = tp.z;
+    const bool seg = (tp.x & F_NEXT) != 0;
+    const float lr = vel[d].w;
+    if (ea && seg) lvel[d].w = ea[u] * lr;
+    if (ei && seg) qrest[d] = scale4(normalize4(qrest[d]), 4.f * ei[u] / lr);
+    if (mass && pos[d].w != 0.f) pos[d].w = 1.f / mass[u];
+}
+__global__ void params_out_kernel(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,
+                                  const float4* qrest, float* ea, float* ei, float* mass, int n) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const int4 tp = topo[d];
+    const int u = tp.z;
+    const bool seg = (tp.x & F_NEXT) != 0;
+    const float lr = vel[d].w;
+    if (ea) ea[u] = seg ? lvel[d].w / lr : 0.f;
+    if (ei) ei[u] = seg ? sqrtf(dot4(qrest[d], qrest[d])) * lr * 0.25f : 0.f;
+    if (mass) mass[u] = pos[d].w != 0.f ? 1.f / pos[d].w : 0.f;
+}
+
+}  // namespace
+
+size_t adjoint_smem_bytes(int block, int iters) { return sizeof(float4) * (size_t)block * (size_t)(3 * iters + 10); }
+
+cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int num_bins, cudaStream_t s) {
+    switch (block) {
+        case 64: return launch_adjoint_b<64>(a, g, num_bins, s);
+        case 128: return launch_adjoint_b<128>(a, g, num_bins, s);
+        case 256: return launch_adjoint_b<256>(a, g, num_bins, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_state_in(const int4* topo, const float* pos, const float* vel, const float* lvel, const float* q,
+                            const float4* cst_pos, const float4* cst_vel, const float4* cst_lvel, float4* o_pos,
+                            float4* o_vel, float4* o_lvel, float4* o_q, int n, cudaStream_t s) {
+    state_in_kernel<<<(n + 255) / 256, 256, 0, s>>>(topo, pos, vel, lvel, q, cst_pos, cst_vel, cst_lvel, o_pos, o_vel,
+                                                     o_lvel, o_q, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_state_out(const int4* topo, const float4* pos, const float4* vel, const float4* lvel, const float4* q,
+                             float* o_pos, float* o_vel, float* o_lvel, float* o_q, int n, cudaStream_t s) {
+    state_out_kernel<<<(n + 255) / 256, 256, 0, s>>>(topo, pos, vel, lvel, q, o_pos, o_vel, o_lvel, o_q, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_params_in(const int4* topo, const float* ea, const float* ei, const float* mass, float4* pos,
+                             const float4* vel, float4* lvel, float4* qrest, int n, cudaStream_t s) {
+    params_in_kernel<<<(n + 255) / 256, 256, 0, s>>>(topo, ea, ei, mass, pos, vel, lvel, qrest, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_params_out(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,
+                              const float4* qrest, float* ea, float* ei, float* mass, int n, cudaStream_t s) {
+    params_out_kernel<<<(n + 255) / 256, 256, 0, s>>>(topo, pos, vel, lvel, qrest, ea, ei, mass, n);
+    return cudaGetLastError();
+}
+
+}  // namespace rs

@@ -111,7 +111,7 @@ Batch::~Batch() {
         if (p) cudaFree(p);
     if (pl_graph_) cudaGraphExecDestroy(pl_graph_);
     void* pbufs[] = {pl_.dx, pl_.dxn, pl_.y, pl_.qprev, pl_.lpos, pl_.facc, pl_.cand, pl_.spose, d_pl_args_,
-                     d_grp_, d_cols_, d_ncols_, d_maxstep_, d_pad_};
+                     d_grp_, d_cols_, d_ncols_, d_maxstep_, d_pad_, gs_pos_, gs_vel_, gs_lvel_, gs_q_, gs_buf_, d_tape_};
     for (void* p : pbufs)
         if (p) cudaFree(p);
     if (h_pl_args_) cudaFreeHost(h_pl_args_);
@@ -371,7 +371,7 @@ void Batch::ensure_device() {
 }
 
 void Batch::ensure_host() {
-    if (host_dyn_valid_) return;
+    if (host_dyn_valid_ && !host_const_stale_) return;
     std::vector<float4> P(n_), Vv(n_), L(n_), Q(n_);
     check(cudaStreamSynchronize(stream_), "sync");
     check(cudaMemcpy(P.data(), d_pos_, sizeof(float4) * n_, cudaMemcpyDeviceToHost), "download(pos)");
@@ -384,6 +384,17 @@ void Batch::ensure_host() {
         vel_[u] = V4{Vv[d].x, Vv[d].y, Vv[d].z, 0.f};
         lvel_[u] = V4{L[d].x, L[d].y, L[d].z, 0.f};
         q_[u] = V4{Q[d].x, Q[d].y, Q[d].z, Q[d].w};
+    }
+    if (host_const_stale_) {  // constants changed by set_parameters live in the .w lanes and qrest
+        std::vector<float4> QR(n_);
+        check(cudaMemcpy(QR.data(), d_qrest_, sizeof(float4) * n_, cudaMemcpyDeviceToHost), "download(qrest)");
+        for (int u = 0; u < n_; u++) {
+            const int d = u2d_[u];
+            im_[u] = P[d].w;
+            ks_[u] = L[d].w;
+            qrest_[u] = V4{QR[d].x, QR[d].y, QR[d].z, QR[d].w};
+        }
+        host_const_stale_ = false;
     }
     host_dyn_valid_ = true;
 }
@@ -993,6 +1004,148 @@ void Batch::wrenches_host(float* out) {
     for (int e = 0; e < R_; e++)
         for (int m = 0; m < M; m++)
             for (int k = 0; k < 6; k++) out[((size_t)e * M + m) * 6 + k] = w[((size_t)e * kMaxSdf + m) * 6 + k];
+}
+
+// ------------------------------------------------------------------ differentiable frames
+void Batch::grad_alloc(int substeps) {
+    const size_t n4 = sizeof(float4) * n_;
+    if (!gs_pos_) {
+        check(cudaMalloc(&gs_pos_, n4), "cudaMalloc(replay pos)");
+        check(cudaMalloc(&gs_vel_, n4), "cudaMalloc(replay vel)");
+        check(cudaMalloc(&gs_lvel_, n4), "cudaMalloc(replay lvel)");
+        check(cudaMalloc(&gs_q_, n4), "cudaMalloc(replay q)");
+        check(cudaMalloc(&gs_buf_, sizeof(float) * 13 * n_), "cudaMalloc(replay views)");
+    }
+    if (substeps > tape_steps_) {
+        if (d_tape_) {
+            check(cudaStreamSynchronize(stream_), "tape reuse");
+            cudaFree(d_tape_);
+            d_tape_ = nullptr;
+        }
+        check(cudaMalloc(&d_tape_, n4 * 4 * (size_t)substeps), "cudaMalloc(substep tape)");
+        tape_steps_ = substeps;
+    }
+}
+
+void Batch::set_state(const float* pos, const float* vel, const float* lvel, const float* q, bool on_device) {
+    ensure_device();
+    grad_alloc(0);
+    const float *p = pos, *v = vel, *l = lvel, *qq = q;
+    if (!on_device) {  // stage host rows through the replay buffer
+        check(cudaStreamSynchronize(stream_), "staging reuse");
+        float* b = gs_buf_;
+        if (pos) check(cudaMemcpy(b, pos, sizeof(float) * 3 * n_, cudaMemcpyHostToDevice), "upload(state pos)"), p = b;
+        if (vel) check(cudaMemcpy(b + 3 * n_, vel, sizeof(float) * 3 * n_, cudaMemcpyHostToDevice), "upload(state vel)"), v = b + 3 * n_;
+        if (lvel) check(cudaMemcpy(b + 6 * n_, lvel, sizeof(float) * 3 * n_, cudaMemcpyHostToDevice), "upload(state lvel)"), l = b + 6 * n_;
+        if (q) check(cudaMemcpy(b + 9 * n_, q, sizeof(float) * 4 * n_, cudaMemcpyHostToDevice), "upload(state q)"), qq = b + 9 * n_;
+    }
+    check(launch_state_in(d_topo_, p, v, l, qq, d_pos_, d_vel_, d_lvel_, d_pos_, d_vel_, d_lvel_, d_q_, n_, stream_), "set state");
+    host_dyn_valid_ = false;
+    gather();
+    check(cudaStreamSynchronize(stream_), "set state");
+}
+
+void Batch::get_state(float* pos, float* vel, float* lvel, float* q, bool on_device) {
+    ensure_device();
+    if (on_device) {
+        check(launch_state_out(d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, pos, vel, lvel, q, n_, stream_), "get state");
+        check(cudaStreamSynchronize(stream_), "get state");
+        return;
+    }
+    ensure_host();
+    for (int u = 0; u < n_; u++) {
+        if (pos) { pos[3 * u] = pos_[u].x; pos[3 * u + 1] = pos_[u].y; pos[3 * u + 2] = pos_[u].z; }
+        if (vel) { vel[3 * u] = vel_[u].x; vel[3 * u + 1] = vel_[u].y; vel[3 * u + 2] = vel_[u].z; }
+        if (lvel) { lvel[3 * u] = lvel_[u].x; lvel[3 * u + 1] = lvel_[u].y; lvel[3 * u + 2] = lvel_[u].z; }
+        if (q) { q[4 * u] = q_[u].x; q[4 * u + 1] = q_[u].y; q[4 * u + 2] = q_[u].z; q[4 * u + 3] = q_[u].w; }
+    }
+}
+
+void Batch::set_parameters(const float* ea, const float* ei, const float* mass, bool on_device) {
+    if (!on_device) {  // host values are validated and applied through the host mirror
+        ensure_host();
+        for (int u = 0; u < n_; u++) {
+            const bool seg = (fl_[u] & F_NEXT) != 0;
+            if (ea && seg && !(ea[u] > 0.f && std::isfinite(ea[u]))) throw std::invalid_argument("ea must be finite and > 0");
+            if (ei && seg && !(ei[u] > 0.f && std::isfinite(ei[u]))) throw std::invalid_argument("ei must be finite and > 0");
+            if (mass && im_[u] != 0.f && !(mass[u] > 0.f && std::isfinite(mass[u])))
+                throw std::invalid_argument("mass must be finite and > 0");
+        }
+        for (int u = 0; u < n_; u++) {
+            const bool seg = (fl_[u] & F_NEXT) != 0;
+            if (ea && seg) ks_[u] = ea[u] * lr_[u];
+            if (ei && seg) qrest_[u] = scale4(normalize4(qrest_[u]), 4.f * ei[u] / lr_[u]);
+            if (mass && im_[u] != 0.f) im_[u] = 1.f / mass[u];
+        }
+        device_valid_ = false;
+        ensure_device();
+        return;
+    }
+    ensure_device();
+    check(launch_params_in(d_topo_, ea, ei, mass, d_pos_, d_vel_, d_lvel_, d_qrest_, n_, stream_), "set parameters");
+    check(cudaStreamSynchronize(stream_), "set parameters");
+    host_const_stale_ = true;
+}
+
+void Batch::get_parameters(float* ea, float* ei, float* mass, bool on_device) {
+    ensure_device();
+    if (on_device) {
+        check(launch_params_out(d_topo_, d_pos_, d_vel_, d_lvel_, d_qrest_, ea, ei, mass, n_, stream_), "get parameters");
+        check(cudaStreamSynchronize(stream_), "get parameters");
+        return;
+    }
+    ensure_host();
+    for (int u = 0; u < n_; u++) {
+        const bool seg = (fl_[u] & F_NEXT) != 0;
+        if (ea) ea[u] = seg ? ks_[u] / lr_[u] : 0.f;
+        if (ei) {
+            const V4 r = qrest_[u];
+            ei[u] = seg ? std::sqrt(r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w) * lr_[u] * 0.25f : 0.f;
+        }
+        if (mass) mass[u] = im_[u] != 0.f ? 1.f / im_[u] : 0.f;
+    }
+}
+
+void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h) {
+    if (!(dt > 0.f)) throw std::invalid_argument("dt must be > 0");
+    if (substeps < 1) throw std::invalid_argument("substeps must be >= 1");
+    if (!(last_h > 0.f)) throw std::invalid_argument("last_h must be > 0");
+    if (!io.pos || !io.vel || !io.lvel || !io.q) throw std::invalid_argument("the frame-start state (pos, vel, lvel, q) is required");
+    if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the state adjoint outputs are required");
+    if (io.p0 && (!io.v0 || !io.p1)) throw std::invalid_argument("a program frame needs p0, v0 and p1");
+    if (io.q1 && !io.q0) throw std::invalid_argument("root_q_end requires root_q");
+    if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
+    if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
+    ensure_device();
+    if (block_ > 256)
+        throw std::invalid_argument("the adjoint runs bins of at most 256 vertices (set_block(256) or smaller)");
+    if (adjoint_smem_bytes(block_, num_itr) > 227 * 1024)
+        throw std::invalid_argument("num_itr too large for the adjoint's shared memory at this bin size");
+    grad_alloc(substeps);
+    if (io.p0) stage_rows(io.p0, io.v0, io.p1, io.q0, io.q1, false);
+    check(launch_state_in(d_topo_, io.pos, io.vel, io.lvel, io.q, d_pos_, d_vel_, d_lvel_, gs_pos_, gs_vel_, gs_lvel_, gs_q_,
+                          n_, stream_), "replay state");
+    FrameArgs a = frame_args(io.p0 ? ROOT_PROGRAM : ROOT_NONE, io.q0 != nullptr, io.q1 != nullptr, dt, substeps);
+    a.h = dt / (float)substeps;
+    a.last_h = last_h;
+    a.pos = gs_pos_; a.vel = gs_vel_; a.lvel = gs_lvel_; a.q = gs_q_;
+    a.out_pos = gs_buf_; a.out_vel = gs_buf_ + 3 * (size_t)n_; a.out_q = gs_buf_ + 6 * (size_t)n_;
+    a.forces_on = 0; a.out_force = nullptr; a.wrench = nullptr;
+    a.tape = d_tape_;
+    check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame replay");
+    AdjArgs g{};
+    g.tape = d_tape_;
+    g.g_pos = io.g_pos; g.g_vel = io.g_vel; g.g_lvel = io.g_lvel; g.g_q = io.g_q;
+    g.o_pos = io.o_pos; g.o_vel = io.o_vel; g.o_lvel = io.o_lvel; g.o_q = io.o_q;
+    g.o_ea = io.o_ea; g.o_ei = io.o_ei; g.o_mass = io.o_mass;
+    g.o_p0 = io.o_p0; g.o_v0 = io.o_v0; g.o_p1 = io.o_p1;
+    if (io.p0) {  // ropes whose root the program does not reach keep zero program adjoints
+        if (io.o_p0) check(cudaMemsetAsync(io.o_p0, 0, sizeof(float) * 3 * R_, stream_), "zero");
+        if (io.o_v0) check(cudaMemsetAsync(io.o_v0, 0, sizeof(float) * 3 * R_, stream_), "zero");
+        if (io.o_p1) check(cudaMemsetAsync(io.o_p1, 0, sizeof(float) * 3 * R_, stream_), "zero");
+    }
+    check(launch_adjoint(a, g, block_, (int)bins_.size(), stream_), "adjoint");
+    check(cudaStreamSynchronize(stream_), "backward");
 }
 
 }  // namespace rs

@@ -92,6 +92,29 @@ public:
     int last_warning() const { return last_warning_; }
     int nonfinite() const { return nonfinite_; }
 
+    // ---- differentiable frames (no counterpart in the reference, which has no gradients).
+    // Arrays are caller order (device pointers when on_device, else host): pos / vel / lvel
+    // [n,3] (lvel = the velocity at the last substep's start, which the next substep's initial
+    // guess extrapolates from), q [n,4]; ea / ei [n] per segment i -> i+1 (a rope's last vertex
+    // is ignored), mass [n] (pinned vertices are ignored). A null pointer leaves that part alone.
+    // Unlike the reference's per-vertex setters, set_parameters works between any two frames.
+    void set_state(const float* pos, const float* vel, const float* lvel, const float* q, bool on_device);
+    void get_state(float* pos, float* vel, float* lvel, float* q, bool on_device);
+    void set_parameters(const float* ea, const float* ei, const float* mass, bool on_device);
+    void get_parameters(float* ea, float* ei, float* mass, bool on_device);
+    float current_h() const { return h_; }   // the last frame's substep: the next frame's lastH
+    // One frame reversed: replays it from the frame-start state (io.pos ...) with the program
+    // rows io.p0 / v0 / p1 (null p0 = a free frame), recording a tape, then runs the adjoint
+    // kernel. All pointers are device, caller order. The batch's own state is not touched.
+    struct BackwardIO {
+        const float *pos, *vel, *lvel, *q;
+        const float *p0, *v0, *p1, *q0, *q1;
+        const float *g_pos, *g_vel, *g_lvel, *g_q;
+        float *o_pos, *o_vel, *o_lvel, *o_q;
+        float *o_ea, *o_ei, *o_mass, *o_p0, *o_v0, *o_p1;
+    };
+    void backward(const BackwardIO& io, float dt, int substeps, float last_h);
+
     // ---- views (device, caller order, stable for the object's life)
     float* out_pos() const { return d_out_pos_; }
     float* out_vel() const { return d_out_vel_; }
@@ -172,6 +195,7 @@ private:
     bool host_dyn_valid_ = true;   // mirror holds the latest dynamic state
     bool device_valid_ = false;    // device holds the latest state and constants
     bool layout_valid_ = false;
+    bool host_const_stale_ = false; // set_parameters changed constants on the device only
 
     // packed layout
     int block_ = 256;
@@ -248,6 +272,13 @@ private:
     float* d_force_ = nullptr;      // [n, 3]
     float* d_wrench_ = nullptr;     // [R, 64, 6]
     int last_substeps_ = 1;
+
+    // differentiable frames: replay state, staging and the substep tape
+    float4 *gs_pos_ = nullptr, *gs_vel_ = nullptr, *gs_lvel_ = nullptr, *gs_q_ = nullptr;
+    float* gs_buf_ = nullptr;       // [13 n] host-call staging / replay views
+    float4* d_tape_ = nullptr;      // [tape_steps_][4][n]
+    int tape_steps_ = 0;
+    void grad_alloc(int substeps);
 };
 
 }  // namespace rs

@@ -144,6 +144,7 @@ int rs_batch_get_param(rs_batch* b, int which, float* value) {
             case RS_P_ACCEL: *value = s.accel; break;
             case RS_P_MAX_H: *value = s.max_h; break;
             case RS_P_TIME: *value = s.time(); break;
+            case RS_P_H: *value = s.current_h(); break;
             default: throw std::invalid_argument("unknown parameter");
         }
     });
@@ -568,6 +569,47 @@ int rs_batch_contact_views(rs_batch* b, float** forces, float** wrenches) {
         need(s.forces_enabled(), "enable_contact_forces(True) first");
         if (forces) *forces = s.contact_force_view();
         if (wrenches) *wrenches = s.wrench_view();
+    });
+}
+
+// ------------------------------------------------------------------ differentiable frames
+int rs_batch_set_state(rs_batch* b, const float* pos, const float* vel, const float* lvel, const float* q, int on_device) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_state(pos, vel, lvel, q, on_device != 0);
+    });
+}
+int rs_batch_get_state(rs_batch* b, float* pos, float* vel, float* lvel, float* q, int on_device) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.get_state(pos, vel, lvel, q, on_device != 0);
+    });
+}
+int rs_batch_set_parameters(rs_batch* b, const float* ea, const float* ei, const float* mass, int on_device) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_parameters(ea, ei, mass, on_device != 0);
+    });
+}
+int rs_batch_get_parameters(rs_batch* b, float* ea, float* ei, float* mass, int on_device) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.get_parameters(ea, ei, mass, on_device != 0);
+    });
+}
+int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        need(io != nullptr, "null argument");
+        rs::Batch::BackwardIO x{io->pos, io->vel, io->lvel, io->q, io->p0, io->v0, io->p1, io->q0, io->q1,
+                                io->g_pos, io->g_vel, io->g_lvel, io->g_q, io->o_pos, io->o_vel, io->o_lvel, io->o_q,
+                                io->o_ea, io->o_ei, io->o_mass, io->o_p0, io->o_v0, io->o_p1};
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.backward(x, dt, substeps, last_h);
     });
 }
 

@@ -130,6 +130,13 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             root_program(a, row, s, S, h, p, v, q);
             if (a.has_q0) sm.q[cur][t] = q;
         }
+        if (a.tape && act) {  // differentiable replay: this substep's start state
+            float4* tp = a.tape + (size_t)s * 4 * a.n + dv;
+            tp[0] = f4(p, 0.f);
+            tp[a.n] = f4(v, 0.f);
+            tp[2 * (size_t)a.n] = sm.lv[t];
+            tp[3 * (size_t)a.n] = q;
+        }
         float4* cache = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
         if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_moving) {
             for (int e = t; e < nPose; e += BLOCK) {

@@ -1,4 +1,4 @@
-// rs_kernels.h -- host-side launchers of the kernels in rs_frame.cu.
+// rs_kernels.h -- host-side launchers of the kernels in rs_frame.cu, rs_plain.cu and rs_adjoint.cu.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -30,6 +30,21 @@ cudaError_t plain_launch_finish(const FrameArgs* pa, const PlainBufs& b, int n, 
 // Device address of the library's static rope-rope candidate array on the current device and
 // its capacity in vertices (looked up once per device, then cached; no allocation).
 cudaError_t static_scratch_cols(int** ptr, int* max_verts);
+// Differentiable frames (rs_adjoint.cu): one frame's reverse sweep from the tape that a frame
+// launch with a.tape set wrote; shared memory it needs per CTA.
+cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int num_bins, cudaStream_t s);
+size_t adjoint_smem_bytes(int block, int iters);
+// Caller-order state <-> device order (the .w constants of cst_* are kept).
+cudaError_t launch_state_in(const int4* topo, const float* pos, const float* vel, const float* lvel, const float* q,
+                            const float4* cst_pos, const float4* cst_vel, const float4* cst_lvel, float4* o_pos,
+                            float4* o_vel, float4* o_lvel, float4* o_q, int n, cudaStream_t s);
+cudaError_t launch_state_out(const int4* topo, const float4* pos, const float4* vel, const float4* lvel, const float4* q,
+                             float* o_pos, float* o_vel, float* o_lvel, float* o_q, int n, cudaStream_t s);
+// Per-vertex EA / EI / mass in caller order -> device constants, and back.
+cudaError_t launch_params_in(const int4* topo, const float* ea, const float* ei, const float* mass, float4* pos,
+                             const float4* vel, float4* lvel, float4* qrest, int n, cudaStream_t s);
+cudaError_t launch_params_out(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,
+                              const float4* qrest, float* ea, float* ei, float* mass, int n, cudaStream_t s);
 // FP32 FMA throughput probe (16 * 8 FMAs per thread per iteration).
 cudaError_t launch_fp32_probe(float* out, int blocks, int threads, int iters, cudaStream_t s);
 

@@ -15,6 +15,7 @@
 #include "../../include/ropesim_b200.h"
 
 namespace py = pybind11;
+static_assert(sizeof(rs_backward_io) == 23 * sizeof(const float*), "rs_backward_io is 23 pointers");
 using farray = py::array_t<float, py::array::c_style | py::array::forcecast>;
 
 namespace {
@@ -55,6 +56,18 @@ uintptr_t parse_cai(const py::object& obj, const std::vector<py::ssize_t>& want,
         }
     }
     return d["data"].cast<py::tuple>()[0].cast<uintptr_t>();
+}
+
+// A per-vertex CUDA array of k components (k = 0: scalar per vertex) in caller order, as
+// [total_verts(, k)] or, for equal-length ropes, [num_envs, V(, k)]. None -> 0.
+uintptr_t parse_vertex_array(const py::object& obj, int n, int R, int V, int k, const char* name) {
+    if (obj.is_none()) return 0;
+    if (!py::hasattr(obj, "__cuda_array_interface__"))
+        throw py::value_error(std::string(name) + " must be a CUDA array (e.g. a contiguous float32 torch tensor on cuda)");
+    auto shape = obj.attr("__cuda_array_interface__").cast<py::dict>()["shape"].cast<std::vector<py::ssize_t>>();
+    std::vector<py::ssize_t> flat{n}, grid{R, V};
+    if (k > 0) { flat.push_back(k); grid.push_back(k); }
+    return parse_cai(obj, (V > 0 && shape.size() == grid.size()) ? grid : flat, name);
 }
 
 // Device buffer handed back to Python; torch.as_tensor(view) shares it (bindings.cpp:622-625).
@@ -654,6 +667,63 @@ PYBIND11_MODULE(_ropesim, m) {
                  ok(rs_batch_step_free(b.h, dt, substeps));
              },
              py::arg("dt"), py::arg("substeps"))
+        // ---- differentiable frames (no counterpart in the reference; see ropesim.grad)
+        .def("set_state",
+             [](RopeBatch& b, py::object pos, py::object vel, py::object lvel, py::object q) {
+                 const uintptr_t p = parse_vertex_array(pos, b.n, b.R, b.V, 3, "pos");
+                 const uintptr_t v = parse_vertex_array(vel, b.n, b.R, b.V, 3, "vel");
+                 const uintptr_t l = parse_vertex_array(lvel, b.n, b.R, b.V, 3, "lvel");
+                 const uintptr_t qq = parse_vertex_array(q, b.n, b.R, b.V, 4, "q");
+                 py::gil_scoped_release rel;
+                 ok(rs_batch_set_state(b.h, (const float*)p, (const float*)v, (const float*)l, (const float*)qq, 1));
+             },
+             py::arg("pos"), py::arg("vel"), py::arg("lvel"), py::arg("q"))
+        .def("get_state",
+             [](RopeBatch& b, py::object pos, py::object vel, py::object lvel, py::object q) {
+                 const uintptr_t p = parse_vertex_array(pos, b.n, b.R, b.V, 3, "pos");
+                 const uintptr_t v = parse_vertex_array(vel, b.n, b.R, b.V, 3, "vel");
+                 const uintptr_t l = parse_vertex_array(lvel, b.n, b.R, b.V, 3, "lvel");
+                 const uintptr_t qq = parse_vertex_array(q, b.n, b.R, b.V, 4, "q");
+                 py::gil_scoped_release rel;
+                 ok(rs_batch_get_state(b.h, (float*)p, (float*)v, (float*)l, (float*)qq, 1));
+             },
+             py::arg("pos"), py::arg("vel"), py::arg("lvel"), py::arg("q"))
+        .def("set_parameters",
+             [](RopeBatch& b, py::object ea, py::object ei, py::object mass) {
+                 const uintptr_t a = parse_vertex_array(ea, b.n, b.R, b.V, 0, "ea");
+                 const uintptr_t e = parse_vertex_array(ei, b.n, b.R, b.V, 0, "ei");
+                 const uintptr_t m = parse_vertex_array(mass, b.n, b.R, b.V, 0, "mass");
+                 py::gil_scoped_release rel;
+                 ok(rs_batch_set_parameters(b.h, (const float*)a, (const float*)e, (const float*)m, 1));
+             },
+             py::arg("ea"), py::arg("ei"), py::arg("mass"))
+        .def("get_parameters",
+             [](RopeBatch& b, py::object ea, py::object ei, py::object mass) {
+                 const uintptr_t a = parse_vertex_array(ea, b.n, b.R, b.V, 0, "ea");
+                 const uintptr_t e = parse_vertex_array(ei, b.n, b.R, b.V, 0, "ei");
+                 const uintptr_t m = parse_vertex_array(mass, b.n, b.R, b.V, 0, "mass");
+                 py::gil_scoped_release rel;
+                 ok(rs_batch_get_parameters(b.h, (float*)a, (float*)e, (float*)m, 1));
+             },
+             py::arg("ea"), py::arg("ei"), py::arg("mass"))
+        .def_property_readonly("current_h",
+                               [](RopeBatch& b) {
+                                   float v = 0.f;
+                                   ok(rs_batch_get_param(b.h, RS_P_H, &v));
+                                   return v;
+                               })
+        // Low-level reverse of one frame: 23 device pointers in rs_backward_io order (0 = NULL);
+        // ropesim.grad validates the tensors behind them.
+        .def("_backward",
+             [](RopeBatch& b, std::vector<uintptr_t> ptrs, float dt, int substeps, float last_h) {
+                 if (ptrs.size() != 23) throw py::value_error("_backward expects 23 pointers");
+                 rs_backward_io io;
+                 const float** c = reinterpret_cast<const float**>(&io);
+                 for (int i = 0; i < 23; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
+                 py::gil_scoped_release rel;
+                 ok(rs_batch_backward(b.h, &io, dt, substeps, last_h));
+             },
+             py::arg("ptrs"), py::arg("dt"), py::arg("substeps"), py::arg("last_h"))
         .def("set_velocities",
              [](RopeBatch& b, farray v) {
                  if (b.V > 0) {
@@ -796,5 +866,6 @@ PYBIND11_MODULE(_ropesim, m) {
         .def_property_readonly("num_envs", [](RopeBatch& b) { return b.R; })
         .def_property_readonly("verts_per_rope", [](RopeBatch& b) { return b.V; })
         .def_property_readonly("rope_verts", [](RopeBatch& b) { return b.verts; })
+        .def_property_readonly("num_verts", [](RopeBatch& b) { return b.n; })
         .def_property_readonly("fixed_root_orientation", [](RopeBatch& b) { return b.fixRoot; });
 }

@@ -72,7 +72,8 @@ enum rs_param {
     RS_P_DAMPING = 3,     /* YarnBall damping (enters as damping/h) (meta.damping) */
     RS_P_ACCEL = 4,       /* local-solve relaxation                 (meta.accelerationRatio) */
     RS_P_MAX_H = 5,       /* largest substep of advance()           (Sim::maxH) */
-    RS_P_TIME = 6         /* read-only accumulated time             (meta.time) */
+    RS_P_TIME = 6,        /* read-only accumulated time             (meta.time) */
+    RS_P_H = 7            /* read-only substep of the last frame    (meta.h; the next frame's lastH) */
 };
 RS_API int rs_batch_set_param(rs_batch* b, int which, float value);
 RS_API int rs_batch_get_param(rs_batch* b, int which, float* value);
@@ -196,6 +197,41 @@ RS_API int rs_batch_contact_forces(rs_batch* b, float* out);
 RS_API int rs_batch_mesh_wrenches(rs_batch* b, float* out);
 /* device views [n,3] and [num_ropes, 64, 6] (contact_forces_view / mesh_wrenches_view) */
 RS_API int rs_batch_contact_views(rs_batch* b, float** forces, float** wrenches);
+
+/* ---------------------------------------------------------------- differentiable frames
+ * No counterpart in the reference, which has no gradients. What is differentiated is the
+ * deterministic substep (root program, inertial prediction, num_itr x (position step with
+ * inertia, plane contact and friction, stretch, damping; frame step), velocity with linear and
+ * quadratic drag); branches (contact active, friction regime, frame-step signs) are held where
+ * the forward pass took them. Rope-rope and mesh contact are refused (RS_EINVAL).
+ *
+ * State: pos / vel / lvel [n,3], q [n,4], caller order; lvel is the velocity at the last
+ * substep's start (the next substep's initial guess extrapolates from it). Parameters: ea / ei
+ * [n] per segment i -> i+1 (a rope's last vertex is ignored), mass [n] (pinned vertices are
+ * ignored). on_device = 1 for device pointers; a NULL pointer leaves that part unchanged.
+ * rs_batch_set_parameters works between any two frames (the reference's per-vertex setters
+ * only before the first step). */
+RS_API int rs_batch_set_state(rs_batch* b, const float* pos, const float* vel, const float* lvel, const float* q,
+                              int on_device);
+RS_API int rs_batch_get_state(rs_batch* b, float* pos, float* vel, float* lvel, float* q, int on_device);
+RS_API int rs_batch_set_parameters(rs_batch* b, const float* ea, const float* ei, const float* mass, int on_device);
+RS_API int rs_batch_get_parameters(rs_batch* b, float* ea, float* ei, float* mass, int on_device);
+/* One frame reversed (all pointers device, caller order). Inputs: the frame-start state, the
+ * frame's program rows (p0 = NULL: a step_free frame; q0 / q1 optional, not differentiated),
+ * the adjoints of the frame-end state (NULL = zero). Outputs: the adjoints of the frame-start
+ * state (required) and, where non-NULL, of ea / ei / mass [n] and of p0 / v0 / p1 [R,3].
+ * dt / substeps are the frame's; last_h is RS_P_H read before the frame was stepped. The frame
+ * is replayed from the given state (the handle's own state is left untouched), recording each
+ * substep's start state in a device tape of 64 B per vertex-substep, then reversed. */
+typedef struct rs_backward_io {
+    const float *pos, *vel, *lvel, *q;
+    const float *p0, *v0, *p1, *q0, *q1;
+    const float *g_pos, *g_vel, *g_lvel, *g_q;
+    float *o_pos, *o_vel, *o_lvel, *o_q;
+    float *o_ea, *o_ei, *o_mass;
+    float *o_p0, *o_v0, *o_p1;
+} rs_backward_io;
+RS_API int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
 
 /* ---------------------------------------------------------------- measurement
  * Measured FP32 FMA throughput of the current device in TFLOP/s (2 FLOP per FMA), from a

@@ -8,6 +8,7 @@
 #include <chrono>
 #include <thread>
 
+#include "rs_adjoint.hpp"
 #include "rs_opcount.hpp"
 #include "rs_oracle.hpp"
 
@@ -15,6 +16,18 @@ namespace py = pybind11;
 using f32a = py::array_t<float, py::array::c_style | py::array::forcecast>;
 using i32a = py::array_t<int, py::array::c_style | py::array::forcecast>;
 using u8a = py::array_t<uint8_t, py::array::c_style | py::array::forcecast>;
+using f64a = py::array_t<double, py::array::c_style | py::array::forcecast>;
+
+template <class T>
+static void v3_in(std::vector<rso::V3<T>>& v, const f64a& a) {
+    const double* p = a.data();
+    for (size_t i = 0; i < v.size(); i++) v[i] = rso::V3<T>(T(p[3 * i]), T(p[3 * i + 1]), T(p[3 * i + 2]));
+}
+template <class T>
+static void q4_in(std::vector<rso::Q4<T>>& v, const f64a& a) {
+    const double* p = a.data();
+    for (size_t i = 0; i < v.size(); i++) v[i] = rso::Q4<T>(T(p[4 * i]), T(p[4 * i + 1]), T(p[4 * i + 2]), T(p[4 * i + 3]));
+}
 
 template <class T>
 static py::array_t<double> v3_out(const std::vector<rso::V3<T>>& v) {
@@ -131,6 +144,52 @@ static void bind_sim(py::module_& m, const char* name) {
         .def("rest_lengths", [](S& s) { return s_out(s.lRest); })
         .def("k_stretch", [](S& s) { return s_out(s.kStretch); })
         .def("flags", [](S& s) { return std::vector<uint32_t>(s.flags.begin(), s.flags.end()); })
+        .def("last_velocities", [](S& s) { return v3_out(s.lastVel); })
+        .def_property_readonly("last_h", [](S& s) { return (double)s.lastH; })
+        // Full dynamic state (pos, vel, lastVel, q, h, lastH) in double, for the adjoint checks.
+        .def("get_state", [](S& s) {
+            return py::make_tuple(v3_out(s.pos), v3_out(s.vel), v3_out(s.lastVel), q4_out(s.q), (double)s.h, (double)s.lastH);
+        })
+        .def("set_state", [](S& s, f64a pos, f64a vel, f64a lv, f64a q, double h, double lastH) {
+            v3_in(s.pos, pos); v3_in(s.vel, vel); v3_in(s.lastVel, lv); q4_in(s.q, q);
+            s.h = T(h); s.lastH = T(lastH);
+        })
+        // Differentiated parameters: kStretch (EA l), |qRest| (4 EI / l), invMass.
+        .def("get_params", [](S& s) {
+            std::vector<T> rho(s.n);
+            for (int i = 0; i < s.n; i++) rho[i] = rso::len4(s.qRest[i]);
+            return py::make_tuple(s_out(s.kStretch), s_out(rho), s_out(s.invMass));
+        })
+        .def("set_params", [](S& s, f64a ks, f64a rho, f64a w) {
+            for (int i = 0; i < s.n; i++) {
+                s.kStretch[i] = T(ks.data()[i]);
+                const T l = rso::len4(s.qRest[i]);
+                if (l > 0) s.qRest[i] = s.qRest[i] * (T(rho.data()[i]) / l);
+                s.invMass[i] = T(w.data()[i]);
+            }
+        })
+        .def("step_program_rows", [](S& s, f64a prog, float dt, int S_) {
+            std::vector<T> p(prog.data(), prog.data() + prog.size());
+            py::gil_scoped_release rel;
+            s.step_program_rows(p.data(), dt, S_);
+        })
+        // Reverse one frame from the current (frame-start) state; leaves the Sim at the frame end.
+        .def("frame_backward", [](S& s, py::object prog, float dt, int S_, f64a gx, f64a gv, f64a glv, f64a gq) {
+            std::vector<T> p;
+            if (!prog.is_none()) { f64a pa = f64a::ensure(prog); p.assign(pa.data(), pa.data() + pa.size()); }
+            rso::FrameGrad<T> g;
+            g.init(s.n, s.R);
+            v3_in(g.x, gx); v3_in(g.v, gv); v3_in(g.lv, glv); q4_in(g.q, gq);
+            {
+                py::gil_scoped_release rel;
+                rso::FrameAdjoint<T>(s).frame_backward(p.empty() ? nullptr : p.data(), false, nullptr, nullptr, dt, S_, g);
+            }
+            py::dict d;
+            d["x"] = v3_out(g.x); d["v"] = v3_out(g.v); d["lv"] = v3_out(g.lv); d["q"] = q4_out(g.q);
+            d["P0"] = v3_out(g.P0); d["V0"] = v3_out(g.V0); d["P1"] = v3_out(g.P1);
+            d["ks"] = s_out(g.ks); d["rho"] = s_out(g.rho); d["w"] = s_out(g.w);
+            return d;
+        })
         .def("contact_forces", [](S& s) { return v3_out(s.contactForce); })
         .def("wrenches", [](S& s) { return v3_out(s.wrench); });
 }

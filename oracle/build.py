@@ -24,7 +24,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     import pybind11
 
     out = ext_path()
-    srcs = [os.path.join(HERE, "_oracle.cpp"), os.path.join(HERE, "rs_oracle.hpp"), os.path.join(HERE, "rs_opcount.hpp")]
+    srcs = [os.path.join(HERE, "_oracle.cpp"), os.path.join(HERE, "rs_oracle.hpp"), os.path.join(HERE, "rs_opcount.hpp"),
+            os.path.join(HERE, "rs_adjoint.hpp")]
     if not force and os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(s) for s in srcs):
         return out
     cmd = [

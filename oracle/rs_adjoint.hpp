@@ -1,0 +1,378 @@
+// rs_adjoint.hpp -- TEST INFRASTRUCTURE ONLY. Hand-written reverse-mode adjoint of one control
+// frame of rso::Sim<T> (rs_oracle.hpp), the FP64 checker of the CUDA adjoint kernel. It is
+// itself pinned on the CPU by FP64 central finite differences of Sim<double> and by an FP64
+// torch-autograd restatement of the same update (oracle/torch_rods.py).
+//
+// The reference has no gradients; the update differentiated here is the deterministic
+// (SNAPSHOT) substep it runs (iteration.cu:34-129, cosserat.cu:23-273, contact.cuh:27-46,
+// batch.cu:122-159). The adjoint is exact for the discrete update: every iteration of the
+// local solve and every frame step is reversed, not only the converged state. Branches that
+// switch terms on and off (contact active, friction regime, sign choices of the frame step,
+// clamps) are held at the branch the forward pass took ("differentiated through the active set").
+//
+// Per substep, given the adjoints of the end state (x', v', lv', q'):
+//   end     x' = x + d^I, v' = drag(d^I / h), lv' = v            -> x̄, d̄^I, v̄, q̄^I
+//   k = I-1 .. 0:
+//     frame    q^{k+1}_i = normalize(vv b e1 + (|vv| + |b|) b)    -> q̄^k (neighbours), d̄^{k+1}, x̄, k̄s, ρ̄
+//     position d^{k+1}_i = d^k_i + a H_i^-1 F_i                   -> d̄^k, x̄, ȳ, q̄^k (tangents), k̄s, w̄
+//       with F̄ = a H^-1 ḡ and H̄ = -(H^-1 ḡ) δᵀ, δ = d^{k+1} - d^k (H is symmetric)
+//   init    d^0 = v h + g h² s(v, lv), y = v h + g h²            -> v̄, l̄v
+//   program x_root, v_root = P(P0, V0, P1; s)                     -> P̄0, V̄0, P̄1
+// Quaternion products c = a b reverse as ā = c̄ b*, b̄ = a* c̄ (left and right multiplication
+// are transposed by conjugation). Contributions that cross vertices are gathered per vertex,
+// the same decomposition the CUDA kernel uses.
+#pragma once
+
+#include "rs_oracle.hpp"
+
+namespace rso {
+
+template <class T> inline Q4<T> qc(const Q4<T>& a) { return Q4<T>(-a.x, -a.y, -a.z, a.w); }
+
+// Transposed Jacobian of the tangent t(q) = q e_x q*:  q̄ = J_t(q)ᵀ t̄.
+template <class T> inline Q4<T> tangent_vjp(const Q4<T>& q, const V3<T>& tb) {
+    return Q4<T>(T(2) * (q.x * tb.x + q.y * tb.y + q.z * tb.z), T(2) * (-q.y * tb.x + q.x * tb.y - q.w * tb.z),
+                 T(2) * (-q.z * tb.x + q.w * tb.y + q.x * tb.z), T(2) * (q.w * tb.x + q.z * tb.y - q.y * tb.z));
+}
+
+// Adjoints of a frame's start state, of its root program and of the per-vertex parameters.
+// Parameters: ks = kStretch (EA l), rho = |qRest| (4 EI / l), w = invMass.
+template <class T> struct FrameGrad {
+    std::vector<V3<T>> x, v, lv;
+    std::vector<Q4<T>> q;
+    std::vector<V3<T>> P0, V0, P1;
+    std::vector<T> ks, rho, w;
+    void init(int n, int R) {
+        x.assign(n, V3<T>()); v.assign(n, V3<T>()); lv.assign(n, V3<T>()); q.assign(n, Q4<T>(0, 0, 0, 0));
+        P0.assign(R, V3<T>()); V0.assign(R, V3<T>()); P1.assign(R, V3<T>());
+        ks.assign(n, T(0)); rho.assign(n, T(0)); w.assign(n, T(0));
+    }
+};
+
+template <class T> class FrameAdjoint {
+public:
+    explicit FrameAdjoint(Sim<T>& sim) : s(sim) {}
+
+    // Reverse one frame. On entry the Sim holds the frame's START state (pos, vel, lastVel, q,
+    // h and lastH as left by the previous frame) and g.x/v/lv/q hold the adjoints of its END
+    // state; on return g.x/v/lv/q hold the adjoints of the start state, g.P0/V0/P1 those of the
+    // program rows (zero when prog == nullptr: a free frame) and g.ks/rho/w have been ADDED to.
+    // The Sim is left at the frame's end state. prog is [p0 (3R), v0 (3R), p1 (3R)].
+    void frame_backward(const T* prog, bool has_q0, const float* q0, const float* q1, float dt, int S, FrameGrad<T>& g) {
+        if (s.ropeContact || !s.grids.empty())
+            throw std::invalid_argument("oracle adjoint: rope-rope and mesh contact are not differentiated");
+        const int n = s.n;
+        s.sdf_begin_step();
+        s.prepare(T(dt / (float)S));
+        // forward replay: substep-start states
+        std::vector<State> st(S);
+        for (int k = 0; k < S; k++) {
+            st[k].save(s);
+            if (prog) s.apply_root_program(prog, q0, q1, k, S, dt);
+            s.substep(k, S);
+        }
+        State end;
+        end.save(s);
+        // reverse
+        for (int k = S - 1; k >= 0; k--) {
+            st[k].load(s);
+            substep_backward(k, S, dt, prog, has_q0 && prog != nullptr, q0, q1, g);
+        }
+        end.load(s);
+        s.finish(dt);
+        s.sdf_end_step(S);
+        (void)n;
+    }
+
+private:
+    Sim<T>& s;
+    struct State {
+        std::vector<V3<T>> pos, vel, lastVel;
+        std::vector<Q4<T>> q;
+        void save(const Sim<T>& m) { pos = m.pos; vel = m.vel; lastVel = m.lastVel; q = m.q; }
+        void load(Sim<T>& m) const { m.pos = pos; m.vel = vel; m.lastVel = lastVel; m.q = q; }
+    };
+
+    bool has(int i, uint32_t f) const { return (s.flags[i] & f) != 0; }
+
+    // Plane contact reverse (contact.cuh:27-46) given F̄ and the two contractions of H̄ the
+    // contact Hessian k nnᵀ - kt (nnᵀ - I) needs: nᵀH̄n and tr H̄.
+    void surface_contact_bwd(const V3<T>& nrm, T gap, const V3<T>& d, T k, T muS, T muK, const V3<T>& Fb, T nHn, T trHb,
+                             V3<T>& db, T& gapb, T& kb) const {
+        const T eps = s.cVSlip, h = s.h;
+        const T N = -k * gap;
+        const V3<T> ut = d - nrm * dot(nrm, d);
+        const T ul = len(ut);
+        const T vt = ul / h;
+        T Nb = dot(nrm, Fb);
+        kb = nHn;
+        T kt;
+        T mu = 0, xr = 0;
+        if (vt <= eps) kt = muS * N / (eps * h);
+        else {
+            xr = vt / eps - T(1);
+            const T sw = T(1) - std::min(T(1), xr);
+            mu = sw * muS + (T(1) - sw) * muK;
+            kt = mu * N / ul;
+        }
+        V3<T> utb = Fb * (-kt);
+        const T ktb = -dot(ut, Fb) - (nHn - trHb);
+        if (vt <= eps) Nb += ktb * muS / (eps * h);
+        else {
+            Nb += ktb * mu / ul;
+            T ulb = -ktb * mu * N / (ul * ul);
+            if (xr < T(1)) ulb += ktb * (muS - muK) * N / ul * (T(-1) / (eps * h));
+            utb += ut * (ulb / ul);
+        }
+        db += utb - nrm * dot(nrm, utb);
+        kb += -gap * Nb;
+        gapb = -k * Nb;
+    }
+
+    void substep_backward(int sub, int S, float dtf, const T* prog, bool q0set, const float* q0, const float* q1,
+                          FrameGrad<T>& g) {
+        const int n = s.n, I = s.numItr;
+        // -- recompute the substep, keeping the iterates
+        if (prog) s.apply_root_program(prog, q0, q1, sub, S, dtf);
+        s.stage_poses(sub, S);
+        const std::vector<V3<T>> x = s.pos, vin = s.vel, lvin = s.lastVel;
+        s.init_itr();
+        const std::vector<V3<T>> y = s.vel;  // the inertial target of free vertices
+        std::vector<std::vector<V3<T>>> d(I + 1);
+        std::vector<std::vector<Q4<T>>> qk(I + 1);
+        d[0] = s.dx;
+        qk[0] = s.q;
+        for (int it = 0; it < I; it++) {
+            s.position_sweep();
+            s.frame_sweep();
+            d[it + 1] = s.dx;
+            qk[it + 1] = s.q;
+        }
+        const T h = s.h, damp = s.damping / h, accel = s.accel;
+        std::vector<V3<T>> db(n), xb(n), yb(n), vb(n), lvb(n);
+        std::vector<Q4<T>> qb(n);
+        // -- end: x' = x + d, v' = drag(d / h) for free vertices, lv' = v_in
+        for (int i = 0; i < n; i++) {
+            xb[i] = g.x[i];
+            db[i] = g.x[i];
+            qb[i] = g.q[i];
+            vb[i] = g.lv[i];
+            lvb[i] = V3<T>();
+        }
+        for (int i = 0; i < n; i++) {
+            if (s.invMass[i] != 0) {
+                const V3<T> ob = g.v[i] * (T(1) - s.drag * h);
+                V3<T> vbar = ob;
+                if (s.dragQuad > 0) {
+                    const int ti = has(i, F_NEXT) ? i : i - 1;
+                    const Q4<T>& tq = qk[I][ti];
+                    const V3<T> t = qtangent(tq);
+                    const V3<T> v = d[I][i] / h;
+                    const T tv = dot(t, v);
+                    const V3<T> vt = t * tv, vn = v - vt;
+                    const T ln = len(vn), Dn = T(1) + s.dragQuad * ln * h;
+                    const T lt = len(vt), Dt = T(1) + s.dragQuadT * lt * h;
+                    V3<T> vnb = ob / Dn;
+                    if (ln > 0) vnb -= vn * (s.dragQuad * h * dot(vn, ob) / (ln * Dn * Dn));
+                    V3<T> vtb = ob / Dt;
+                    if (lt > 0) vtb -= vt * (s.dragQuadT * h * dot(vt, ob) / (lt * Dt * Dt));
+                    vbar = vnb;
+                    vtb -= vnb;
+                    const T tvb = dot(vtb, t);
+                    vbar += t * tvb;
+                    const V3<T> tb = vtb * tv + v * tvb;
+                    qb[ti] += tangent_vjp(tq, tb);
+                }
+                db[i] += vbar / h;
+            } else {
+                vb[i] += g.v[i];  // a pinned vertex keeps its (driven) velocity
+            }
+        }
+        // -- iterations in reverse
+        for (int it = I - 1; it >= 0; it--) {
+            frame_reverse(x, d[it + 1], qk[it], qb, db, xb, g);
+            position_reverse(x, y, d[it], d[it + 1], qk[it], damp, accel, db, qb, xb, yb, g);
+        }
+        // -- init: d^0 = v h + g h² s, y = v h + g h²
+        const V3<T> grav = s.gravity;
+        const T g2 = len2(grav);
+        for (int i = 0; i < n; i++) {
+            if (s.invMass[i] != 0) {
+                vb[i] += (db[i] + yb[i]) * h;
+                if (g2 > 0) {
+                    const V3<T> acc = (vin[i] - lvin[i]) / s.lastH;
+                    const T raw = dot(acc, grav) / g2;
+                    if (raw >= 0 && raw <= 1) {  // inclusive at the clamp's ends (as torch.clamp)
+                        const T sb = dot(grav * (h * h), db[i]);
+                        const V3<T> gs = grav * (sb / (s.lastH * g2));
+                        vb[i] += gs;
+                        lvb[i] -= gs;
+                    }
+                }
+            } else {
+                vb[i] += db[i] * h;
+            }
+        }
+        // -- root program: x = P0 + V0 tau + A tau²/2, v = V0 + A (tau + h/2),
+        //    A = ((P1 - P0) - V0 dt) 2 / dt²; the program overwrites the root's incoming state
+        if (prog) {
+            const T dt = T(dtf), tau = T(sub) * h, th = tau + T(0.5) * h, idt2 = T(2) / (dt * dt);
+            const T xa = T(0.5) * tau * tau * idt2;  // d x / d P1
+            for (int r = 0; r < s.R; r++) {
+                const int root = s.start[r];
+                const V3<T> X = xb[root], Vv = vb[root];
+                g.P0[r] += X * (T(1) - xa) + Vv * (-th * idt2);
+                g.V0[r] += X * (tau - xa * dt) + Vv * (T(1) - th * idt2 * dt);
+                g.P1[r] += X * xa + Vv * (th * idt2);
+                xb[root] = V3<T>();
+                vb[root] = V3<T>();
+                if (q0set) qb[root] = Q4<T>(0, 0, 0, 0);
+            }
+        }
+        g.x = xb; g.v = vb; g.lv = lvb; g.q = qb;
+    }
+
+    // Frame step k reversed: qb holds q̄^{k+1} on entry and q̄^k on return; db gains the
+    // d^{k+1} contributions, xb the position ones.
+    void frame_reverse(const std::vector<V3<T>>& x, const std::vector<V3<T>>& dn, const std::vector<Q4<T>>& qo,
+                       std::vector<Q4<T>>& qb, std::vector<V3<T>>& db, std::vector<V3<T>>& xb, FrameGrad<T>& g) {
+        const int n = s.n;
+        const Q4<T> e1(1, 0, 0, 0);
+        std::vector<Q4<T>> own(n), toL(n, Q4<T>(0, 0, 0, 0)), toR(n, Q4<T>(0, 0, 0, 0));
+        std::vector<V3<T>> su(n);
+        for (int i = 0; i < n; i++) {
+            if (has(i, F_FIX_ORIENT) || !has(i, F_NEXT)) { own[i] = qb[i]; continue; }
+            own[i] = Q4<T>(0, 0, 0, 0);
+            const T l = s.lRest[i], ks = s.kStretch[i];
+            const V3<T> u = ((x[i + 1] - x[i]) + (dn[i + 1] - dn[i])) / l;
+            const V3<T> vv = u * (T(-2) * ks);
+            const Q4<T> q0 = qo[i];
+            Q4<T> b(0, 0, 0, 0);
+            T sp = 0, sn = 0;
+            if (has(i, F_PREV)) {
+                const Q4<T> qr = s.qRest[i - 1], qq = qo[i - 1];
+                sp = dot4(qmul(qq.inv(), q0), qr) > 0 ? T(1) : T(-1);
+                b += qmul(qq, qr) * sp;
+            }
+            if (has(i, F_NEXT_ORIENT)) {
+                const Q4<T> qr = s.qRest[i], qq = qo[i + 1];
+                sn = dot4(qmul(q0.inv(), qq), qr) > 0 ? T(1) : T(-1);
+                b += qmul(qq, qr.inv()) * sn;
+            }
+            const T lvv = len(vv), lb = len4(b), lambda = lvv + lb;
+            const Q4<T> V(vv, T(0));
+            const Q4<T> A = qmul(V, b);
+            const Q4<T> z = qmul(A, e1) + b * lambda;
+            const T zl = len4(z);
+            const Q4<T> qn = z * (T(1) / zl);
+            const Q4<T> qbn = qb[i];
+            const Q4<T> zb = (qbn - qn * dot4(qn, qbn)) * (T(1) / zl);
+            Q4<T> bb = zb * lambda;
+            const T lamb = dot4(zb, b);
+            V3<T> vvb = lvv > 0 ? vv * (lamb / lvv) : V3<T>();
+            if (lb > 0) bb += b * (lamb / lb);
+            const Q4<T> Ab = qmul(zb, qc(e1));
+            vvb += qmul(Ab, qc(b)).vec();
+            bb += qmul(qc(V), Ab);
+            const V3<T> ub = vvb * (T(-2) * ks);
+            g.ks[i] += T(-2) * dot(u, vvb);
+            if (has(i, F_PREV)) {
+                const Q4<T> bq = bb * sp, qr = s.qRest[i - 1];
+                toL[i] = qmul(bq, qc(qr));
+                g.rho[i - 1] += dot4(qmul(qc(qo[i - 1]), bq), qr) / len4(qr);
+            }
+            if (has(i, F_NEXT_ORIENT)) {
+                const Q4<T> bq = bb * sn, qr = s.qRest[i];
+                toR[i] = qmul(bq, qr);
+                g.rho[i] += dot4(qc(qmul(qc(qo[i + 1]), bq)), qr) / len4(qr);
+            }
+            su[i] = ub / l;
+        }
+        for (int i = 0; i < n; i++) {
+            Q4<T> a = own[i];
+            if (i > 0) a += toR[i - 1];
+            if (i + 1 < n) a += toL[i + 1];
+            qb[i] = a;
+            V3<T> dv = V3<T>() - su[i];
+            if (i > 0) dv += su[i - 1];
+            db[i] += dv;
+            xb[i] += dv;
+        }
+    }
+
+    // Position step k reversed: db holds d̄^{k+1} on entry and d̄^k on return.
+    void position_reverse(const std::vector<V3<T>>& x, const std::vector<V3<T>>& y, const std::vector<V3<T>>& dk,
+                          const std::vector<V3<T>>& dn, const std::vector<Q4<T>>& qo, T damp, T accel,
+                          std::vector<V3<T>>& db, std::vector<Q4<T>>& qb, std::vector<V3<T>>& xb, std::vector<V3<T>>& yb,
+                          FrameGrad<T>& g) {
+        const int n = s.n;
+        const T h = s.h;
+        std::vector<V3<T>> Fb(n), dnew(n), sc(n);
+        std::vector<T> trH(n, T(0));
+        for (int i = 0; i < n; i++) {
+            dnew[i] = db[i];
+            const T w = s.invMass[i];
+            if (w == 0) continue;
+            const T a = T(1) / (w * h * h);
+            S3<T> H(a);
+            const bool surf = s.numPlanes > 0;
+            const T kap = s.cKappa / h, kc = kap * kap / w;
+            if (surf) {
+                V3<T> fdummy;
+                for (int pl = 0; pl < s.numPlanes; pl++) {
+                    const V3<T> nrm(s.planes[pl][0], s.planes[pl][1], s.planes[pl][2]);
+                    const T gap = (dot(nrm, x[i]) - s.planes[pl][3]) + dot(nrm, dk[i]) - s.cR;
+                    if (gap >= 0) continue;
+                    s.surface_contact(nrm, gap, dk[i], kc, s.cMuS, s.cMuK, fdummy, H);
+                }
+            }
+            if (has(i, F_NEXT)) H.add_diag(s.kStretch[i] / s.lRest[i] / s.lRest[i] * (T(1) + damp));
+            if (has(i, F_PREV)) H.add_diag(s.kStretch[i - 1] / s.lRest[i - 1] / s.lRest[i - 1] * (T(1) + damp));
+            const V3<T> e = sym_solve(H, db[i]);
+            const V3<T> delta = dn[i] - dk[i];
+            Fb[i] = e * accel;
+            trH[i] = -dot(e, delta);
+            yb[i] += Fb[i] * a;
+            dnew[i] -= Fb[i] * a;
+            T wb = (dot(y[i] - dk[i], Fb[i]) + trH[i]) * (-a / w);
+            if (surf) {
+                for (int pl = 0; pl < s.numPlanes; pl++) {
+                    const V3<T> nrm(s.planes[pl][0], s.planes[pl][1], s.planes[pl][2]);
+                    const T gap = (dot(nrm, x[i]) - s.planes[pl][3]) + dot(nrm, dk[i]) - s.cR;
+                    if (gap >= 0) continue;
+                    const T nHn = -dot(nrm, e) * dot(nrm, delta);
+                    T gapb, kb;
+                    surface_contact_bwd(nrm, gap, dk[i], kc, s.cMuS, s.cMuK, Fb[i], nHn, trH[i], dnew[i], gapb, kb);
+                    dnew[i] += nrm * gapb;
+                    xb[i] += nrm * gapb;
+                    wb += kb * (-kc / w);
+                }
+            }
+            g.w[i] += wb;
+        }
+        for (int j = 0; j < n; j++) {
+            if (!has(j, F_NEXT)) continue;
+            const T l = s.lRest[j], invl = T(1) / l;
+            const V3<T> c = ((x[j + 1] - x[j]) + (dk[j + 1] - dk[j])) * invl - qtangent(qo[j]);
+            const T kk = s.kStretch[j] * invl, dd = kk * invl;
+            const V3<T> dF = Fb[j] - Fb[j + 1];
+            const V3<T> cb = dF * kk;
+            const T kb = dot(c, dF);
+            const T ddb = -damp * (dot(dk[j], Fb[j]) + dot(dk[j + 1], Fb[j + 1])) + (T(1) + damp) * (trH[j] + trH[j + 1]);
+            g.ks[j] += kb * invl + ddb * invl * invl;
+            qb[j] += tangent_vjp(qo[j], cb) * T(-1);
+            sc[j] = cb * invl;
+            dnew[j] -= Fb[j] * (damp * dd);
+            dnew[j + 1] -= Fb[j + 1] * (damp * dd);
+        }
+        for (int i = 0; i < n; i++) {
+            V3<T> dv = V3<T>() - sc[i];
+            if (i > 0) dv += sc[i - 1];
+            dnew[i] += dv;
+            xb[i] += dv;
+        }
+        db = dnew;
+    }
+};
+
+}  // namespace rso

@@ -872,7 +872,8 @@ public:
         int s = (int)std::ceil(dt / mh);
         return s < 1 ? 1 : s;
     }
-    void run_substeps(int steps, float dt, const float* prog, const float* q0, const float* q1) {
+    template <class P>
+    void run_substeps(int steps, float dt, const P* prog, const float* q0, const float* q1) {
         for (int s = 0; s < steps; s++) {
             if (prog) apply_root_program(prog, q0, q1, s, steps, dt);
             substep(s, steps);
@@ -885,7 +886,7 @@ public:
         const float mh = substeps > 0 ? (dt / (float)substeps) * 1.000001f : maxH;
         const int steps = ceil_steps(dt, mh);
         prepare(T(dt / (float)steps));
-        run_substeps(steps, dt, nullptr, nullptr, nullptr);
+        run_substeps<float>(steps, dt, nullptr, nullptr, nullptr);
         finish(dt);
         sdf_end_step(substeps > 0 ? substeps : steps);
     }
@@ -904,13 +905,13 @@ public:
         sdf_begin_step();
         if (ropeContact) {
             prepare(T(dt / (float)substeps));
-            run_substeps(substeps, dt, nullptr, nullptr, nullptr);
+            run_substeps<float>(substeps, dt, nullptr, nullptr, nullptr);
             finish(dt);
         } else {
             const float mh = (dt / (float)substeps) * 1.000001f;
             const int steps = ceil_steps(dt, mh);
             prepare(T(dt / (float)steps));
-            run_substeps(steps, dt, nullptr, nullptr, nullptr);
+            run_substeps<float>(steps, dt, nullptr, nullptr, nullptr);
             finish(dt);
         }
         sdf_end_step(substeps);
@@ -929,8 +930,10 @@ public:
         const T l = dot4(a, a);
         return l > 0 ? a * (T(1) / m_sqrt(l)) : Q4<T>(0, 0, 0, 1);
     }
-    // applyRootProgramK, batch.cu:122-159. prog = [p0 (3R), v0 (3R), p1 (3R)].
-    void apply_root_program(const float* prog, const float* q0, const float* q1, int s, int S, float dtf) {
+    // applyRootProgramK, batch.cu:122-159. prog = [p0 (3R), v0 (3R), p1 (3R)] (float rows as the
+    // API passes them, or rows in T for finite differences of the program).
+    template <class P>
+    void apply_root_program(const P* prog, const float* q0, const float* q1, int s, int S, float dtf) {
         const T dt = T(dtf);
         for (int r = 0; r < R; r++) {
             const int root = start[r];
@@ -962,11 +965,19 @@ public:
         finish(dt);
         sdf_end_step(substeps);
     }
+    // The same frame with program rows in T (finite differences with respect to the program).
+    void step_program_rows(const T* prog, float dt, int substeps) {
+        sdf_begin_step();
+        prepare(T(dt / (float)substeps));
+        run_substeps(substeps, dt, prog, nullptr, nullptr);
+        finish(dt);
+        sdf_end_step(substeps);
+    }
     // RopeBatch::step_free, batch.cu:388-398.
     void step_free(float dt, int substeps) {
         sdf_begin_step();
         prepare(T(dt / (float)substeps));
-        run_substeps(substeps, dt, nullptr, nullptr, nullptr);
+        run_substeps<float>(substeps, dt, nullptr, nullptr, nullptr);
         finish(dt);
         sdf_end_step(substeps);
     }

@@ -1,0 +1,177 @@
+"""The CUDA adjoint (rs_batch_backward behind ropesim.grad) against the FP64 oracle adjoint.
+
+Workload: the differentiable configuration's check size, 8 ropes x 16 vertices of the
+config-1 rope (3 cm segments, density 0.1, EA 500, EI 1e-4, 8 iterations), program roots,
+5 control frames x 100 substeps of 1/6000 s, loss = mean squared distance of the rope tips to
+a seeded target curve summed over frames. Gradients with respect to the root programs
+(p0, v0, p1 of every frame), EA, EI, per-vertex mass and the initial state.
+
+The oracle adjoint is pinned on the CPU by FP64 finite differences and by FP64 torch autograd
+(test_adjoint_oracle.py); here the GPU's FP32 gradients are compared with it. Tolerance, per
+gradient group (norm-wise relative): 1e-4, or 4x the deviation of the oracle's own FP32
+adjoint from FP64 when that FP32 noise floor is larger (an FP32 gradient linearises the FP32
+trajectory, which itself deviates from the FP64 one). A direct check against FP64 central
+finite differences of the oracle's forward along seeded directions uses the same rule.
+
+Scenes whose FP64 loss is itself ill-conditioned are not usable here: with the stiff config-2
+rope (EA 11473 N on 2 cm segments) and no damping, 8 Jacobi sweeps leave the stiffest stretch
+mode unconverged, and FP64 finite differences of the tip loss with respect to the initial
+positions disagree with each other by 10% across step sizes.
+"""
+import numpy as np
+import pytest
+
+import adjoint_cases as ac
+
+pytestmark = pytest.mark.gpu
+
+R, V, F, S, DT = 8, 16, 5, 100, 1.0 / 60.0
+GROUPS = ["g_p0", "g_v0", "g_p1", "g_ea", "g_ei", "g_mass", "g_pos", "g_vel", "g_lvel", "g_q"]
+SCENES = {
+    "free": (dict(plane=False), dict(v_std=0.3, p_std=0.02)),
+    "resting_on_plane": (dict(plane=True, clearance=-0.002), dict(v_std=0.05, p_std=0.01)),
+    "damped_quadratic_drag": (dict(plane=False, damping=0.01, drag_quad=2.0), dict(v_std=0.3, p_std=0.02)),
+}
+
+
+def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clearance=None):
+    import ropesim
+
+    _, density, ea, ei = ac.MATERIALS[material]
+    b = ropesim.RopeBatch.from_positions(pos, density, ea, ei, 1 / 6000, 8)
+    b.set_gravity(np.array([0.0, 0.0, -9.81], np.float32))
+    b.damping = damping
+    b.drag = 0.2
+    b.drag_quad = drag_quad
+    b.drag_quad_t = 0.5 * drag_quad
+    if plane:
+        b.set_planes(np.array([[0.0, 0.0, 1.0, 0.0]], np.float32), radius=0.00635, mu_s=0.5, mu_k=0.3)
+    return b
+
+
+def _gpu_loss_and_grad(pos, progs, tgt, **kw):
+    import torch
+
+    import ropesim.grad as rg
+
+    b = _gpu_batch(pos, **kw)
+    st = [t.clone().requires_grad_() for t in rg.state(b)]
+    par = [t.clone().requires_grad_() for t in rg.parameters(b)]
+    P = [torch.tensor(a, device="cuda", requires_grad=True) for a in progs]
+    tg = torch.tensor(tgt, device="cuda", dtype=torch.float32)
+    cur = st
+    loss = 0.0
+    for f in range(F):
+        cur = rg.frame(b, cur, par, P[0][f], P[1][f], P[2][f], DT, S)
+        tip = cur[0].view(R, V, 3)[:, -1]
+        loss = loss + ((tip - tg[f]) ** 2).sum(-1).mean()
+    loss.backward()
+    g = {"g_p0": P[0].grad, "g_v0": P[1].grad, "g_p1": P[2].grad, "g_ea": par[0].grad, "g_ei": par[1].grad,
+         "g_mass": par[2].grad, "g_pos": st[0].grad, "g_vel": st[1].grad, "g_lvel": st[2].grad, "g_q": st[3].grad}
+    return float(loss.detach()), {k: v.detach().cpu().numpy().astype(np.float64) for k, v in g.items()}, b
+
+
+@pytest.mark.parametrize("kind", list(SCENES))
+def test_adjoint_matches_fp64_oracle(kind):
+    kw, pk = SCENES[kind]
+    kw = dict(material="c1", **kw)
+    ob, pos = ac.scene(R=R, V=V, **kw)
+    progs = ac.programs(pos, F, **pk)
+    tgt = ac.targets(pos, F)
+    L64, g64 = ac.oracle_loss_and_grad(ob, progs, tgt, DT, S, V)
+    ob32, _ = ac.scene(R=R, V=V, precision="f32", **kw)
+    _, g32 = ac.oracle_loss_and_grad(ob32, progs, tgt, DT, S, V)
+    L, g, _ = _gpu_loss_and_grad(pos, progs, tgt, **kw)
+    print(f"\n  [{kind}] loss gpu {L:.8e} fp64 {L64:.8e}")
+    assert abs(L - L64) <= 1e-4 * abs(L64)
+    for k in GROUPS:
+        e_gpu = ac.rel(g[k], g64[k])
+        e_32 = ac.rel(g32[k], g64[k])
+        print(f"  {k:7s} |g| {np.linalg.norm(g64[k]):.3e}  gpu-vs-fp64 {e_gpu:.2e}  fp32-oracle-vs-fp64 {e_32:.2e}")
+        assert np.isfinite(g[k]).all()
+        assert e_gpu <= max(1e-4, 4 * e_32), k
+
+
+def test_adjoint_matches_fp64_finite_differences():
+    kw = dict(material="c1", plane=False)
+    ob, pos = ac.scene(R=R, V=V, **kw)
+    progs = ac.programs(pos, F, v_std=0.3, p_std=0.02)
+    tgt = ac.targets(pos, F)
+    _, g, _ = _gpu_loss_and_grad(pos, progs, tgt, **kw)
+    ob32, _ = ac.scene(R=R, V=V, precision="f32", **kw)
+    _, g32 = ac.oracle_loss_and_grad(ob32, progs, tgt, DT, S, V)
+    s = ob._s
+    st0, par0 = s.get_state(), s.get_params()
+    l = s.rest_lengths()
+    seg = np.ones(R * V, bool)
+    seg[V - 1::V] = False
+
+    def loss(pr, par):
+        s.set_state(*st0)
+        s.set_params(*par)
+        val = 0.0
+        for f in range(F):
+            s.step_program_rows(np.concatenate([pr[0][f].ravel(), pr[1][f].ravel(), pr[2][f].ravel()]).astype(np.float64), DT, S)
+            x = s.get_state()[0].reshape(R, V, 3)
+            val += ((x[:, -1] - tgt[f]) ** 2).sum(-1).mean()
+        return val
+
+    rng = np.random.default_rng(3)
+    progs64 = [a.astype(np.float64) for a in progs]
+    ea0, ei0 = par0[0] / l, par0[1] * l / 4
+    cases = []
+    for k, name in enumerate(("g_p0", "g_v0", "g_p1")):
+        u = rng.standard_normal(progs64[k].shape)
+        cases.append((name, u, lambda e, u=u, k=k: loss([p + e * u if j == k else p for j, p in enumerate(progs64)], par0), 1e-4))
+    u = rng.standard_normal(R * V) * seg * ea0
+    cases.append(("g_ea", u, lambda e, u=u: loss(progs64, [(ea0 + e * u) * l, par0[1], par0[2]]), 1e-4))
+    u = rng.standard_normal(R * V) * seg * ei0
+    cases.append(("g_ei", u, lambda e, u=u: loss(progs64, [par0[0], (ei0 + e * u) * 4 / l, par0[2]]), 1e-3))
+    for name, u, fn, eps in cases:
+        d1 = (fn(eps) - fn(-eps)) / (2 * eps)
+        d2 = (fn(eps / 2) - fn(-eps / 2)) / eps
+        fd = (4 * d2 - d1) / 3
+        ad = float((g[name] * u.reshape(g[name].shape)).sum())
+        a32 = float((g32[name] * u.reshape(g32[name].shape)).sum())
+        floor = abs(a32 - fd) / abs(fd)
+        print(f"\n  {name}: gpu {ad:+.8e} fd64 {fd:+.8e} rel {abs(ad - fd) / abs(fd):.2e} (fp32 oracle {floor:.2e})")
+        assert abs(ad - fd) <= max(1e-4, 4 * floor) * abs(fd), name
+
+
+def test_differentiable_frame_forward_is_the_step():
+    """rg.frame advances like RopeBatch.step (same kernel; state and parameters round-tripped)."""
+    import torch
+
+    import ropesim.grad as rg
+
+    _, pos = ac.scene(R=R, V=V, plane=True, material="c1")
+    progs = ac.programs(pos, 2)
+    a = _gpu_batch(pos)
+    b = _gpu_batch(pos)
+    st = rg.state(b)
+    par = rg.parameters(b)
+    for f in range(2):
+        p0, v0, p1 = (torch.tensor(x[f], device="cuda") for x in progs)
+        a.step(p0, v0, DT, S, root_pos_end=p1)
+        with torch.no_grad():
+            st = rg.frame(b, st, par, p0, v0, p1, DT, S)
+        xa = torch.as_tensor(a.positions()).reshape(-1, 3)
+        # EA, EI and mass round-trip through EA l, 4 EI / l and 1 / m (a rounding each)
+        assert float((xa - st[0]).abs().max()) <= 1e-5
+
+
+def test_adjoint_refuses_contact_it_does_not_differentiate():
+    import torch
+
+    import ropesim.grad as rg
+
+    _, pos = ac.scene(R=R, V=V, plane=True, material="c1")
+    progs = ac.programs(pos, 1)
+    b = _gpu_batch(pos)
+    b.set_rope_contact(True, 2e-3, 1e-3, 1e-5, 0.1, 5.0, 1.2, 1)
+    st = [t.requires_grad_() for t in rg.state(b)]
+    par = rg.parameters(b)
+    p0, v0, p1 = (torch.tensor(x[0], device="cuda") for x in progs)
+    out = rg.frame(b, st, par, p0, v0, p1, DT, 10)
+    with pytest.raises(ValueError, match="rope-rope"):
+        out[0].sum().backward()
