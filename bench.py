@@ -519,6 +519,111 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_config4(args):
+    """Config 4: differentiable rollouts of 1024 ropes x 64 vertices (config-1 rope: 3 cm segments,
+    0.1 kg/m, EA 500 N, EI 1e-4 N m^2), 30 control frames x 100 substeps, program roots, loss = mean
+    squared tip distance to a seeded target curve. One step = one 30-frame rollout: forward only
+    (RopeBatch.step), forward + backward (ropesim.grad.frame + loss.backward(), gradients of the
+    programs, EA, EI, mass and the initial state), and the plain per-substep path's forward."""
+    import torch
+
+    import ropesim
+    import ropesim.grad as rg
+
+    torch.cuda.set_device(0)
+    R = args.ropes if args.ropes != 4096 else 1024
+    V, F, S4 = 64, 30, 100
+    seg, density, ea, ei = 0.03, 0.1, 500.0, 1e-4
+    rng = np.random.default_rng(4)
+    roots = np.stack([rng.uniform(-0.5, 0.5, R), rng.uniform(-0.5, 0.5, R), rng.uniform(2.5, 3.5, R)], 1).astype(np.float32)
+    pos = np.repeat(roots[:, None], V, 1) - np.array([0, 0, seg], np.float32) * np.arange(V, dtype=np.float32)[None, :, None]
+    pos[:, 1:] += rng.normal(0, 1e-3, (R, V - 1, 3)).astype(np.float32)
+    prog = []
+    cur = roots.copy()
+    for f in range(F):
+        v0 = rng.normal(0, 0.3, (R, 3)).astype(np.float32)
+        p1 = (cur + rng.normal(0, 0.02, (R, 3))).astype(np.float32)
+        prog.append((cur.copy(), v0, p1))
+        cur = p1
+    P = [torch.tensor(np.stack([p[k] for p in prog]), device="cuda") for k in range(3)]
+    t_amp = rng.normal(0, 0.05, (1, R, 3))
+    tgt = pos[:, -1][None] + t_amp * np.sin(2 * np.pi * np.arange(1, F + 1)[:, None, None] / F)
+    tgt = torch.tensor(tgt, device="cuda", dtype=torch.float32)
+
+    def make(engine):
+        b = ropesim.RopeBatch.from_positions(pos, density, ea, ei, 1 / 6000, ITERS)
+        b.set_gravity(np.array([0, 0, -9.81], np.float32))
+        b.damping = 0.0
+        b.drag = 0.2
+        if engine == "plain":
+            b.set_engine("plain")
+        return b
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    nv = R * V
+
+    def timed(fn, rollouts):
+        ms = []
+        for k in range(rollouts):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    out = {}
+    for engine in ("persistent", "plain"):
+        b = make(engine)
+        st0 = rg.state(b)
+
+        def fwd(b=b, st0=st0):
+            b.set_state(*st0)
+            for f in range(F):
+                b.step(P[0][f], P[1][f], DT, S4, root_pos_end=P[2][f])
+
+        timed(fwd, args.warmup)
+        ms = timed(fwd, args.steps)
+        out[engine] = {"ms_per_rollout": float(np.mean(ms)), "value": nv * S4 * F * len(ms) / (sum(ms) * 1e-3)}
+        if engine == "persistent":
+            par0 = rg.parameters(b)
+            grads = {}
+
+            def fwd_bwd(b=b, st0=st0, par0=par0):
+                st = [t.clone().requires_grad_() for t in st0]
+                par = [t.clone().requires_grad_() for t in par0]
+                pr = [t.clone().requires_grad_() for t in P]
+                cur = st
+                loss = 0.0
+                for f in range(F):
+                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4)
+                    loss = loss + ((cur[0].view(R, V, 3)[:, -1] - tgt[f]) ** 2).sum(-1).mean()
+                loss.backward()
+                grads["finite"] = bool(all(torch.isfinite(t.grad).all() for t in st + par + pr))
+                grads["loss"] = float(loss.detach())
+
+            timed(fwd_bwd, args.warmup)
+            msb = timed(fwd_bwd, args.steps)
+            out["fwd_bwd"] = {"ms_per_rollout": float(np.mean(msb)), "value": nv * S4 * F * len(msb) / (sum(msb) * 1e-3),
+                              "grads_finite": grads["finite"], "loss": grads["loss"]}
+        del b
+    line = {"metric": "vertex-substeps/s (fwd+bwd)", "value": out["fwd_bwd"]["value"], "unit": "vertex-substeps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["fwd_bwd"]["ms_per_rollout"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config-4 rollouts)",
+            "config": {"workload": f"config4-diff-{R}x{V}", "ropes": R, "verts_per_rope": V, "frames": F,
+                       "substeps": S4, "num_itr": ITERS, "step": "one 30-frame rollout",
+                       "counted": "forward vertex-substeps of the rollout", "l2": "flushed between rollouts (256 MB write)"},
+            "forward": out["persistent"], "fwd_bwd": out["fwd_bwd"], "plain_path_forward": out["plain"],
+            "fwd_bwd_over_fwd": out["fwd_bwd"]["ms_per_rollout"] / out["persistent"]["ms_per_rollout"],
+            "fwd_bwd_speedup_vs_plain_fwd": out["fwd_bwd"]["value"] / out["plain"]["value"],
+            "fwd_speedup_vs_plain": out["persistent"]["value"] / out["plain"]["value"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_ROPES
     ap = argparse.ArgumentParser()
@@ -531,8 +636,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     ap.add_argument("--block", type=int, default=0, help="bin size (CTA threads); 0 = the library's choice")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3"],
-                    help="config2 (the headline line) or config3 (uneven ropes, planes and meshes vs the plain path)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
+                    help="config2 (the headline line), config3 (uneven ropes, planes and meshes vs the plain path) "
+                         "or config4 (differentiable rollouts: forward and forward + backward)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -541,6 +647,8 @@ def main():
         run_reference(args)
     elif args.workload == "config3":
         run_config3(args)
+    elif args.workload == "config4":
+        run_config4(args)
     else:
         run_ours(args)
 

@@ -10,8 +10,9 @@
 // active, friction regime, frame-step signs, clamps) are held where the forward pass took them.
 //
 // Data flow of one frame's backward (Batch::backward_program):
-//   1. the frame is replayed by frame_kernel from the frame-start checkpoint, writing the state
-//      after each substep's root program to a tape [S][4][n] (x, v, lv, q) in HBM;
+//   1. the state after each substep's root program is taped [S][4][n] (x, v, lv, q; caller
+//      order, so the tape outlives a repacking of the bins) in HBM: by the forward step itself
+//      when the caller kept a tape, else by a replay of the frame from its start state;
 //   2. adjoint_kernel (one CTA per bin, one thread per vertex, like the forward) walks the
 //      substeps backwards: it recomputes the substep's iterates d^k, q^k into shared memory
 //      from the tape, then reverses end -> frame/position steps -> init -> root program.
@@ -78,12 +79,12 @@ __device__ __forceinline__ void surface_contact_bwd(f3 n, float gap, f3 d, float
 }
 
 // Shared memory of the adjoint kernel, in float4 units (BLOCK = bin size, I = iterations):
-//   X, QR, KC, EA, EB, EC, EF, ES   one slot per vertex each
-//   LD [I+1][BLOCK]   displacement iterates d^k
-//   LE [I][BLOCK]     increments δ^k = d^{k+1} - d^k as the solve produced them
+//   X, QR, KC, EA, EB, EC, EF   one slot per vertex each
+//   LD [I+1][BLOCK]   displacement iterates d^k (the solve's increment is d^{k+1} - d^k)
 //   LQ [I+1][BLOCK]   frame iterates q^k
+// 64-thread bins at 8 iterations: 25.6 KB, 8 CTAs (16 warps) per SM with <= 128 registers.
 template <int BLOCK, int SURF>
-__global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const AdjArgs g) {
+__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoint_kernel(const FrameArgs a, const AdjArgs g) {
     extern __shared__ float4 smem[];
     const int I = a.iters;
     float4* X = smem;
@@ -93,10 +94,8 @@ __global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const
     float4* EB = EA + BLOCK;
     float4* EC = EB + BLOCK;
     float4* EF = EC + BLOCK;
-    float4* ES = EF + BLOCK;
-    float4* LD = ES + BLOCK;
-    float4* LE = LD + (size_t)(I + 1) * BLOCK;
-    float4* LQ = LE + (size_t)I * BLOCK;
+    float4* LD = EF + BLOCK;
+    float4* LQ = LD + (size_t)(I + 1) * BLOCK;
 
     const Bin bin = a.bins[blockIdx.x];
     const int t = threadIdx.x;
@@ -141,7 +140,7 @@ __global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const
         f3 p = zero3(), v = zero3(), lvin = zero3();
         float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
         if (act) {
-            const float4* tp = g.tape + (size_t)s * 4 * n + dv;
+            const float4* tp = g.tape + (size_t)s * 4 * n + uidx;
             p = xyz(tp[0]); v = xyz(tp[n]); lvin = xyz(tp[2 * n]); q = tp[3 * n];
         }
         f3 dx, y;
@@ -167,10 +166,7 @@ __global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const
                 f += xyz(fa);
                 H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
             }
-            f3 del = zero3();
-            if (im != 0.f) del = sym_solve(H, f) * a.accel;
-            dx += del;
-            LE[(size_t)k * BLOCK + t] = f4(del, 0.f);
+            if (im != 0.f) dx += sym_solve(H, f) * a.accel;
             LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, 0.f);
             __syncthreads();
             if (upd) {
@@ -312,7 +308,7 @@ __global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const
                     H.xx += dd; H.yy += dd; H.zz += dd;
                 }
                 const f3 e = sym_solve(H, db);
-                const f3 del = xyz(LE[(size_t)k * BLOCK + t]);
+                const f3 del = xyz(LD[(size_t)(k + 1) * BLOCK + t]) - dk;
                 Fb = e * a.accel;
                 trH = -dot(e, del);
                 yb += Fb * c.fm;
@@ -337,9 +333,9 @@ __global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const
             // segment t's residual c = ((x1 - x) + (d1 - d)) / l - t(q), read before the barrier:
             // after it a neighbour may already be writing the next substep's iterates
             const float4 qk = Lq[t];
-            const f3 cc = hasNext ? ((p1 - p) + (xyz(LD[(size_t)k * BLOCK + t + 1]) - dk)) * c.invl - qtangent(qk) : zero3();
+            const f3 dkn = hasNext ? xyz(LD[(size_t)k * BLOCK + t + 1]) : zero3();
+            const f3 cc = hasNext ? ((p1 - p) + (dkn - dk)) * c.invl - qtangent(qk) : zero3();
             EF[t] = f4(Fb, trH);
-            ES[t].x = dot(dk, Fb);
             __syncthreads();
             if (hasNext) {
                 const float4 Fn4 = EF[t + 1];
@@ -348,7 +344,7 @@ __global__ void __launch_bounds__(BLOCK) adjoint_kernel(const FrameArgs a, const
                 const f3 dF = Fb - Fn;
                 const f3 cb = dF * kk;
                 ksb += dot(cc, dF) * c.invl +
-                       (-damp * (dot(dk, Fb) + ES[t + 1].x) + (1.f + damp) * (trH + Fn4.w)) * c.invl * c.invl;
+                       (-damp * (dot(dk, Fb) + dot(dkn, Fn)) + (1.f + damp) * (trH + Fn4.w)) * c.invl * c.invl;
                 qb = add4(qb, scale4(tangent_vjp(qk, cb), -1.f));
                 dn -= cb * c.invl;
                 xb -= cb * c.invl;
@@ -456,10 +452,11 @@ __global__ void state_out_kernel(const int4* topo, const float4* pos, const floa
     if (o_lvel) st3(o_lvel, u, xyz(lvel[d]));
     if (o_q) reinterpret_cast<float4*>(o_q)[u] = q[d];
 }
-// Per-vertex parameters in caller order: EA (kStretch = EA lRest), EI (|qRest| = 4 EI / lRest)
-// on vertices that own a segment, mass (invMass = 1 / mass) on free vertices.
+// Per-vertex parameters in caller order: EA (kStretch = EA lRest), EI (qRest = its unit direction
+// scaled by 4 EI / lRest, so that setting the same EI twice gives the same rotor) on vertices
+// that own a segment, mass (invMass = 1 / mass) on free vertices.
 __global__ void params_in_kernel(const int4* topo, const float* ea, const float* ei, const float* mass, float4* pos,
-                                 const float4* vel, float4* lvel, float4* qrest, int n) {
+                                 const float4* vel, float4* lvel, float4* qrest, const float4* qdir, int n) {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
     const int4 tp = topo[d];
@@ -467,7 +464,7 @@ __global__ void params_in_kernel(const int4* topo, const float* ea, const float*
     const bool seg = (tp.x & F_NEXT) != 0;
     const float lr = vel[d].w;
     if (ea && seg) lvel[d].w = ea[u] * lr;
-    if (ei && seg) qrest[d] = scale4(normalize4(qrest[d]), 4.f * ei[u] / lr);
+    if (ei && seg) qrest[d] = scale4(qdir[d], 4.f * ei[u] / lr);
     if (mass && pos[d].w != 0.f) pos[d].w = 1.f / mass[u];
 }
 __global__ void params_out_kernel(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,
@@ -485,7 +482,7 @@ __global__ void params_out_kernel(const int4* topo, const float4* pos, const flo
 
 }  // namespace
 
-size_t adjoint_smem_bytes(int block, int iters) { return sizeof(float4) * (size_t)block * (size_t)(3 * iters + 10); }
+size_t adjoint_smem_bytes(int block, int iters) { return sizeof(float4) * (size_t)block * (size_t)(2 * iters + 9); }
 
 cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int num_bins, cudaStream_t s) {
     switch (block) {
@@ -509,8 +506,8 @@ cudaError_t launch_state_out(const int4* topo, const float4* pos, const float4* 
     return cudaGetLastError();
 }
 cudaError_t launch_params_in(const int4* topo, const float* ea, const float* ei, const float* mass, float4* pos,
-                             const float4* vel, float4* lvel, float4* qrest, int n, cudaStream_t s) {
-    params_in_kernel<<<(n + 255) / 256, 256, 0, s>>>(topo, ea, ei, mass, pos, vel, lvel, qrest, n);
+                             const float4* vel, float4* lvel, float4* qrest, const float4* qdir, int n, cudaStream_t s) {
+    params_in_kernel<<<(n + 255) / 256, 256, 0, s>>>(topo, ea, ei, mass, pos, vel, lvel, qrest, qdir, n);
     return cudaGetLastError();
 }
 cudaError_t launch_params_out(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,

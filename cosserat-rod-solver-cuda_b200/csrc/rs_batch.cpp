@@ -82,7 +82,11 @@ Batch::Batch(int num_ropes, const int* rope_verts, const float* positions, const
             for (int i = ustart_[r]; i + 1 < ustart_[r + 1]; i++) qrest_[i] = V4{0.f, 0.f, 0.f, 1.f};
     for (int i = 0; i < n_; i++) ks_[i] = k_stretch * lr_[i];       // setKStretch
     const float kb4 = k_bend * 4.f;                                   // setKBend
-    for (int i = 0; i < n_; i++) qrest_[i] = scale4(normalize4(qrest_[i]), kb4 / lr_[i]);
+    qdir_.resize(n_);
+    for (int i = 0; i < n_; i++) {
+        qdir_[i] = normalize4(qrest_[i]);  // kept: set_parameters scales these directions
+        qrest_[i] = scale4(qdir_[i], kb4 / lr_[i]);
+    }
     for (int r = 0; r < R_; r++) fl_[ustart_[r]] |= F_ROOT;
     max_h = max_h_in;
     h_ = max_h_in;   // seed lastH like a fresh sim (bindings.cpp:249-253)
@@ -104,7 +108,7 @@ Batch::Batch(int num_ropes, const int* rope_verts, const float* positions, const
 Batch::~Batch() {
     if (stream_) cudaStreamSynchronize(stream_);
     for (auto& g : grids_) cudaFree(const_cast<float*>(g.v));
-    void* bufs[] = {d_bins_, d_ropes_, d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, d_qrest_, d_init_pos_, d_init_q_,
+    void* bufs[] = {d_bins_, d_ropes_, d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, d_qrest_, d_qdir_, d_init_pos_, d_init_q_,
                     d_out_pos_, d_out_vel_, d_out_q_, d_prog_, d_status_, d_ranges_, d_boxes_, d_cur_, d_tgt_,
                     d_tele_, d_motion_, d_poses_, d_stage_, d_stage_tele_, d_force_, d_wrench_};
     for (void* p : bufs)
@@ -286,6 +290,7 @@ void Batch::alloc_device() {
         alloc((void**)&d_lvel_, n4, "cudaMalloc(lvel)");
         alloc((void**)&d_q_, n4, "cudaMalloc(q)");
         alloc((void**)&d_qrest_, n4, "cudaMalloc(qrest)");
+        alloc((void**)&d_qdir_, n4, "cudaMalloc(qrest directions)");
         alloc((void**)&d_init_pos_, n4, "cudaMalloc(init pos)");
         alloc((void**)&d_init_q_, n4, "cudaMalloc(init q)");
         alloc((void**)&d_out_pos_, sizeof(float) * 3 * n_, "cudaMalloc(view pos)");
@@ -345,7 +350,7 @@ void Batch::ensure_device() {
         device_valid_ = false;
     }
     if (!device_valid_) {
-        std::vector<float4> P(n_), Vv(n_), L(n_), Q(n_), QR(n_);
+        std::vector<float4> P(n_), Vv(n_), L(n_), Q(n_), QR(n_), QD(n_);
         std::vector<int4> topo(n_);
         for (int u = 0; u < n_; u++) {
             const int d = u2d_[u];
@@ -354,6 +359,7 @@ void Batch::ensure_device() {
             L[d] = make_float4(lvel_[u].x, lvel_[u].y, lvel_[u].z, ks_[u]);
             Q[d] = make_float4(q_[u].x, q_[u].y, q_[u].z, q_[u].w);
             QR[d] = make_float4(qrest_[u].x, qrest_[u].y, qrest_[u].z, qrest_[u].w);
+            QD[d] = make_float4(qdir_[u].x, qdir_[u].y, qdir_[u].z, qdir_[u].w);
         }
         for (const Bin& b : bins_)
             for (int r = b.rstart; r < b.rstart + b.rcount; r++) {
@@ -366,6 +372,7 @@ void Batch::ensure_device() {
         check(cudaMemcpy(d_lvel_, L.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(lvel)");
         check(cudaMemcpy(d_q_, Q.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(q)");
         check(cudaMemcpy(d_qrest_, QR.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(qrest)");
+        check(cudaMemcpy(d_qdir_, QD.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(qrest directions)");
         device_valid_ = true;
     }
 }
@@ -546,7 +553,8 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     // uploadMeta bookkeeping, batch.cu:57-62 / step.cpp:41-42
     last_h_ = h_;
     h_ = h;
-    const FrameArgs a = frame_args(root_mode, has_q0, has_q1, dt, steps);
+    FrameArgs a = frame_args(root_mode, has_q0, has_q1, dt, steps);
+    a.tape = pending_tape_;
     const bool timed = timing_ || tuning();
     if (timed) check(cudaEventRecord(ev0_, stream_), "event");
     if (engine_ == 1 || (rope_contact_ && oversize_)) run_frame_plain(a);
@@ -1082,7 +1090,7 @@ void Batch::set_parameters(const float* ea, const float* ei, const float* mass, 
         return;
     }
     ensure_device();
-    check(launch_params_in(d_topo_, ea, ei, mass, d_pos_, d_vel_, d_lvel_, d_qrest_, n_, stream_), "set parameters");
+    check(launch_params_in(d_topo_, ea, ei, mass, d_pos_, d_vel_, d_lvel_, d_qrest_, d_qdir_, n_, stream_), "set parameters");
     check(cudaStreamSynchronize(stream_), "set parameters");
     host_const_stale_ = true;
 }
@@ -1106,6 +1114,22 @@ void Batch::get_parameters(float* ea, float* ei, float* mass, bool on_device) {
     }
 }
 
+void Batch::step_program_taped(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1,
+                               float dt, int substeps, float* tape) {
+    if (!tape) throw std::invalid_argument("null tape");
+    if (engine_ != 0) throw std::invalid_argument("a taped step runs the persistent engine only");
+    if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
+    if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
+    pending_tape_ = reinterpret_cast<float4*>(tape);
+    try {
+        step_program(p0, v0, p1, q0, q1, dt, substeps, false);
+    } catch (...) {
+        pending_tape_ = nullptr;
+        throw;
+    }
+    pending_tape_ = nullptr;
+}
+
 void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h) {
     if (!(dt > 0.f)) throw std::invalid_argument("dt must be > 0");
     if (substeps < 1) throw std::invalid_argument("substeps must be >= 1");
@@ -1121,20 +1145,25 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h)
         throw std::invalid_argument("the adjoint runs bins of at most 256 vertices (set_block(256) or smaller)");
     if (adjoint_smem_bytes(block_, num_itr) > 227 * 1024)
         throw std::invalid_argument("num_itr too large for the adjoint's shared memory at this bin size");
-    grad_alloc(substeps);
+    grad_alloc(io.tape ? 0 : substeps);
     if (io.p0) stage_rows(io.p0, io.v0, io.p1, io.q0, io.q1, false);
-    check(launch_state_in(d_topo_, io.pos, io.vel, io.lvel, io.q, d_pos_, d_vel_, d_lvel_, gs_pos_, gs_vel_, gs_lvel_, gs_q_,
-                          n_, stream_), "replay state");
     FrameArgs a = frame_args(io.p0 ? ROOT_PROGRAM : ROOT_NONE, io.q0 != nullptr, io.q1 != nullptr, dt, substeps);
     a.h = dt / (float)substeps;
     a.last_h = last_h;
-    a.pos = gs_pos_; a.vel = gs_vel_; a.lvel = gs_lvel_; a.q = gs_q_;
-    a.out_pos = gs_buf_; a.out_vel = gs_buf_ + 3 * (size_t)n_; a.out_q = gs_buf_ + 6 * (size_t)n_;
-    a.forces_on = 0; a.out_force = nullptr; a.wrench = nullptr;
-    a.tape = d_tape_;
-    check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame replay");
+    const float4* tape = reinterpret_cast<const float4*>(io.tape);
+    if (!tape) {  // replay the frame from its start state to record the tape
+        check(launch_state_in(d_topo_, io.pos, io.vel, io.lvel, io.q, d_pos_, d_vel_, d_lvel_, gs_pos_, gs_vel_, gs_lvel_,
+                              gs_q_, n_, stream_), "replay state");
+        FrameArgs r = a;
+        r.pos = gs_pos_; r.vel = gs_vel_; r.lvel = gs_lvel_; r.q = gs_q_;
+        r.out_pos = gs_buf_; r.out_vel = gs_buf_ + 3 * (size_t)n_; r.out_q = gs_buf_ + 6 * (size_t)n_;
+        r.forces_on = 0; r.out_force = nullptr; r.wrench = nullptr;
+        r.tape = d_tape_;
+        check(launch_frame(r, block_, (int)bins_.size(), stream_), "frame replay");
+        tape = d_tape_;
+    }
     AdjArgs g{};
-    g.tape = d_tape_;
+    g.tape = tape;
     g.g_pos = io.g_pos; g.g_vel = io.g_vel; g.g_lvel = io.g_lvel; g.g_q = io.g_q;
     g.o_pos = io.o_pos; g.o_vel = io.o_vel; g.o_lvel = io.o_lvel; g.o_q = io.o_q;
     g.o_ea = io.o_ea; g.o_ei = io.o_ei; g.o_mass = io.o_mass;

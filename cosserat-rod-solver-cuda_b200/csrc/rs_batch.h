@@ -106,14 +106,20 @@ public:
     // One frame reversed: replays it from the frame-start state (io.pos ...) with the program
     // rows io.p0 / v0 / p1 (null p0 = a free frame), recording a tape, then runs the adjoint
     // kernel. All pointers are device, caller order. The batch's own state is not touched.
+    // With io.tape (the tape a step_program_taped of this frame recorded) the replay is skipped.
     struct BackwardIO {
         const float *pos, *vel, *lvel, *q;
         const float *p0, *v0, *p1, *q0, *q1;
         const float *g_pos, *g_vel, *g_lvel, *g_q;
         float *o_pos, *o_vel, *o_lvel, *o_q;
         float *o_ea, *o_ei, *o_mass, *o_p0, *o_v0, *o_p1;
+        const float* tape;
     };
     void backward(const BackwardIO& io, float dt, int substeps, float last_h);
+    // step_program that also records the frame's substep tape (device, 16 * substeps * n
+    // floats, caller order) for a later backward of this frame.
+    void step_program_taped(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1,
+                            float dt, int substeps, float* tape);
 
     // ---- views (device, caller order, stable for the object's life)
     float* out_pos() const { return d_out_pos_; }
@@ -188,6 +194,7 @@ private:
     std::vector<float> im_, lr_, ks_;
     std::vector<uint32_t> fl_;
     std::vector<V4> qrest_;
+    std::vector<V4> qdir_;     // unit rest rotors of construction (the direction EI scales)
     std::vector<V4> init_pos_, init_q_;
     float min_seg_ = 0.f, max_seg_ = 0.f;
     // caller-order mirror: dynamic state (valid while host_dyn_valid_)
@@ -211,6 +218,7 @@ private:
     Rope* d_ropes_ = nullptr;
     int4* d_topo_ = nullptr;
     float4 *d_pos_ = nullptr, *d_vel_ = nullptr, *d_lvel_ = nullptr, *d_q_ = nullptr, *d_qrest_ = nullptr;
+    float4* d_qdir_ = nullptr;      // unit rest rotors: set_parameters scales these (idempotent)
     float4 *d_init_pos_ = nullptr, *d_init_q_ = nullptr;
     float *d_out_pos_ = nullptr, *d_out_vel_ = nullptr, *d_out_q_ = nullptr;
     float* d_prog_ = nullptr;       // [R, 17]
@@ -278,6 +286,7 @@ private:
     float* gs_buf_ = nullptr;       // [13 n] host-call staging / replay views
     float4* d_tape_ = nullptr;      // [tape_steps_][4][n]
     int tape_steps_ = 0;
+    float4* pending_tape_ = nullptr;  // tape of the frame being launched (step_program_taped)
     void grad_alloc(int substeps);
 };
 

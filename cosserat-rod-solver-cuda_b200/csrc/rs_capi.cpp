@@ -607,9 +607,21 @@ int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int subst
         need(io != nullptr, "null argument");
         rs::Batch::BackwardIO x{io->pos, io->vel, io->lvel, io->q, io->p0, io->v0, io->p1, io->q0, io->q1,
                                 io->g_pos, io->g_vel, io->g_lvel, io->g_q, io->o_pos, io->o_vel, io->o_lvel, io->o_q,
-                                io->o_ea, io->o_ei, io->o_mass, io->o_p0, io->o_v0, io->o_p1};
+                                io->o_ea, io->o_ei, io->o_mass, io->o_p0, io->o_v0, io->o_p1, io->tape};
         std::lock_guard<std::mutex> g(s.mutex());
         s.backward(x, dt, substeps, last_h);
+    });
+}
+int rs_batch_step_program_taped(rs_batch* b, const float* p0, const float* v0, const float* p1, const float* q0,
+                                const float* q1, float dt, int substeps, float* tape) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        need(p0 && v0 && p1 && tape, "null argument");
+        need(dt > 0, "dt must be > 0");
+        need(substeps >= 1, "substeps must be >= 1");
+        need(!(q1 && !q0), "root_q_end requires root_q");
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.step_program_taped(p0, v0, p1, q0, q1, dt, substeps, tape);
     });
 }
 

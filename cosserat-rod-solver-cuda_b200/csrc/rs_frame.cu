@@ -130,8 +130,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             root_program(a, row, s, S, h, p, v, q);
             if (a.has_q0) sm.q[cur][t] = q;
         }
-        if (a.tape && act) {  // differentiable replay: this substep's start state
-            float4* tp = a.tape + (size_t)s * 4 * a.n + dv;
+        if (a.tape && act) {  // differentiable frames: this substep's start state, caller order
+            float4* tp = a.tape + (size_t)s * 4 * a.n + a.topo[dv].z;
             tp[0] = f4(p, 0.f);
             tp[a.n] = f4(v, 0.f);
             tp[2 * (size_t)a.n] = sm.lv[t];

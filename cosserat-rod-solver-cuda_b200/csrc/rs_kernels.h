@@ -42,7 +42,7 @@ cudaError_t launch_state_out(const int4* topo, const float4* pos, const float4* 
                              float* o_pos, float* o_vel, float* o_lvel, float* o_q, int n, cudaStream_t s);
 // Per-vertex EA / EI / mass in caller order -> device constants, and back.
 cudaError_t launch_params_in(const int4* topo, const float* ea, const float* ei, const float* mass, float4* pos,
-                             const float4* vel, float4* lvel, float4* qrest, int n, cudaStream_t s);
+                             const float4* vel, float4* lvel, float4* qrest, const float4* qdir, int n, cudaStream_t s);
 cudaError_t launch_params_out(const int4* topo, const float4* pos, const float4* vel, const float4* lvel,
                               const float4* qrest, float* ea, float* ei, float* mass, int n, cudaStream_t s);
 // FP32 FMA throughput probe (16 * 8 FMAs per thread per iteration).

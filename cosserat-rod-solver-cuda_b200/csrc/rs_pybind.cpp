@@ -15,7 +15,7 @@
 #include "../../include/ropesim_b200.h"
 
 namespace py = pybind11;
-static_assert(sizeof(rs_backward_io) == 23 * sizeof(const float*), "rs_backward_io is 23 pointers");
+static_assert(sizeof(rs_backward_io) == 24 * sizeof(const float*), "rs_backward_io is 24 pointers");
 using farray = py::array_t<float, py::array::c_style | py::array::forcecast>;
 
 namespace {
@@ -712,18 +712,34 @@ PYBIND11_MODULE(_ropesim, m) {
                                    ok(rs_batch_get_param(b.h, RS_P_H, &v));
                                    return v;
                                })
-        // Low-level reverse of one frame: 23 device pointers in rs_backward_io order (0 = NULL);
+        // Low-level reverse of one frame: 24 device pointers in rs_backward_io order (0 = NULL);
         // ropesim.grad validates the tensors behind them.
         .def("_backward",
              [](RopeBatch& b, std::vector<uintptr_t> ptrs, float dt, int substeps, float last_h) {
-                 if (ptrs.size() != 23) throw py::value_error("_backward expects 23 pointers");
+                 if (ptrs.size() != 24) throw py::value_error("_backward expects 24 pointers");
                  rs_backward_io io;
                  const float** c = reinterpret_cast<const float**>(&io);
-                 for (int i = 0; i < 23; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
+                 for (int i = 0; i < 24; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
                  py::gil_scoped_release rel;
                  ok(rs_batch_backward(b.h, &io, dt, substeps, last_h));
              },
              py::arg("ptrs"), py::arg("dt"), py::arg("substeps"), py::arg("last_h"))
+        // Program step recording the substep tape into a caller buffer of 16 * substeps * n floats.
+        .def("_step_taped",
+             [](RopeBatch& b, py::object root_pos, py::object root_vel, py::object root_pos_end, float dt, int substeps,
+                uintptr_t tape) {
+                 if (!(dt > 0) || substeps < 1) throw py::value_error("dt > 0 and substeps >= 1 required");
+                 if (!b.rootsPinned) throw py::value_error("the program step drives every rope's root");
+                 const uintptr_t p = parse_cai(root_pos, {b.R, 3}, "root_pos");
+                 const uintptr_t v = parse_cai(root_vel, {b.R, 3}, "root_vel");
+                 const uintptr_t p1 = parse_cai(root_pos_end, {b.R, 3}, "root_pos_end");
+                 b.stepped = true;
+                 py::gil_scoped_release rel;
+                 ok(rs_batch_step_program_taped(b.h, (const float*)p, (const float*)v, (const float*)p1, nullptr, nullptr,
+                                                dt, substeps, (float*)tape));
+             },
+             py::arg("root_pos"), py::arg("root_vel"), py::arg("root_pos_end"), py::arg("dt"), py::arg("substeps"),
+             py::arg("tape"))
         .def("set_velocities",
              [](RopeBatch& b, farray v) {
                  if (b.V > 0) {

@@ -130,15 +130,16 @@ struct FrameArgs {
     float* maxstep;          // [n] step limits (plain engine)
     float* pad;              // [n] detection paddings (plain engine)
     GridDesc grids[kMaxSdf];
-    // differentiable replay: when set, the state after each substep's root program is written to
-    // tape[(s * 4 + f) * n + i] for f = x, v, lv (previous substep's start velocity), q
+    // differentiable frames: when set, the state after each substep's root program is written to
+    // tape[(s * 4 + f) * n + u] for f = x, v, lv (previous substep's start velocity), q and the
+    // caller-order index u
     float4* tape;
 };
 
 // One frame's backward (rs_adjoint.cu). Arrays are caller order; null outputs are skipped and
 // null upstream adjoints read as zero.
 struct AdjArgs {
-    const float4* tape;                          // [S][4][n] written by the frame replay
+    const float4* tape;                          // [S][4][n] caller order, written by a frame launch
     const float *g_pos, *g_vel, *g_lvel, *g_q;   // adjoints of the frame-end state [n,3] x3, [n,4]
     float *o_pos, *o_vel, *o_lvel, *o_q;         // adjoints of the frame-start state
     float *o_ea, *o_ei, *o_mass;                 // [n] adjoints of EA, EI (segment i -> i+1), mass

@@ -222,7 +222,8 @@ RS_API int rs_batch_get_parameters(rs_batch* b, float* ea, float* ei, float* mas
  * state (required) and, where non-NULL, of ea / ei / mass [n] and of p0 / v0 / p1 [R,3].
  * dt / substeps are the frame's; last_h is RS_P_H read before the frame was stepped. The frame
  * is replayed from the given state (the handle's own state is left untouched), recording each
- * substep's start state in a device tape of 64 B per vertex-substep, then reversed. */
+ * substep's start state in a device tape of 64 B per vertex-substep, then reversed; with
+ * io->tape set (recorded by rs_batch_step_program_taped) the replay is skipped. */
 typedef struct rs_backward_io {
     const float *pos, *vel, *lvel, *q;
     const float *p0, *v0, *p1, *q0, *q1;
@@ -230,8 +231,14 @@ typedef struct rs_backward_io {
     float *o_pos, *o_vel, *o_lvel, *o_q;
     float *o_ea, *o_ei, *o_mass;
     float *o_p0, *o_v0, *o_p1;
+    const float* tape;  /* NULL = replay the frame; else this frame's rs_batch_step_program_taped tape */
 } rs_backward_io;
 RS_API int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
+/* rs_batch_step_program that also records the frame's substep tape for rs_batch_backward:
+ * tape = device buffer of 16 * substeps * n floats (the state after each substep's root
+ * program, caller order), so that the backward need not replay the frame. */
+RS_API int rs_batch_step_program_taped(rs_batch* b, const float* p0, const float* v0, const float* p1,
+                                       const float* q0, const float* q1, float dt, int substeps, float* tape);
 
 /* ---------------------------------------------------------------- measurement
  * Measured FP32 FMA throughput of the current device in TFLOP/s (2 FLOP per FMA), from a

@@ -10,8 +10,10 @@ The oracle adjoint is pinned on the CPU by FP64 finite differences and by FP64 t
 (test_adjoint_oracle.py); here the GPU's FP32 gradients are compared with it. Tolerance, per
 gradient group (norm-wise relative): 1e-4, or 4x the deviation of the oracle's own FP32
 adjoint from FP64 when that FP32 noise floor is larger (an FP32 gradient linearises the FP32
-trajectory, which itself deviates from the FP64 one). A direct check against FP64 central
-finite differences of the oracle's forward along seeded directions uses the same rule.
+trajectory, which itself deviates from the FP64 one, and the bin size the autotuner picks
+changes the adjoint's rounding). A direct check against FP64 central finite differences of the
+oracle's forward along seeded directions uses the same rule, the floor taken as the larger of
+the FP32 oracle's error along the direction and over the gradient group.
 
 Scenes whose FP64 loss is itself ill-conditioned are not usable here: with the stiff config-2
 rope (EA 11473 N on 2 cm segments) and no damping, 8 Jacobi sweeps leave the stiffest stretch
@@ -49,7 +51,7 @@ def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clear
     return b
 
 
-def _gpu_loss_and_grad(pos, progs, tgt, **kw):
+def _gpu_loss_and_grad(pos, progs, tgt, tape=True, **kw):
     import torch
 
     import ropesim.grad as rg
@@ -62,7 +64,7 @@ def _gpu_loss_and_grad(pos, progs, tgt, **kw):
     cur = st
     loss = 0.0
     for f in range(F):
-        cur = rg.frame(b, cur, par, P[0][f], P[1][f], P[2][f], DT, S)
+        cur = rg.frame(b, cur, par, P[0][f], P[1][f], P[2][f], DT, S, tape=tape)
         tip = cur[0].view(R, V, 3)[:, -1]
         loss = loss + ((tip - tg[f]) ** 2).sum(-1).mean()
     loss.backward()
@@ -101,7 +103,8 @@ def test_adjoint_matches_fp64_finite_differences():
     ob32, _ = ac.scene(R=R, V=V, precision="f32", **kw)
     _, g32 = ac.oracle_loss_and_grad(ob32, progs, tgt, DT, S, V)
     s = ob._s
-    st0, par0 = s.get_state(), s.get_params()
+    st0, par0 = s.get_state(), s.get_params()  # the start state, before any stepping
+    _, g64 = ac.oracle_loss_and_grad(ob, progs, tgt, DT, S, V)
     l = s.rest_lengths()
     seg = np.ones(R * V, bool)
     seg[V - 1::V] = False
@@ -120,9 +123,11 @@ def test_adjoint_matches_fp64_finite_differences():
     progs64 = [a.astype(np.float64) for a in progs]
     ea0, ei0 = par0[0] / l, par0[1] * l / 4
     cases = []
-    for k, name in enumerate(("g_p0", "g_v0", "g_p1")):
+    # p0 moves the root's position at the frame start (a jump from the previous frame's end), so
+    # the loss is sharply curved along it: its differences need a 1e-6 step
+    for k, name, eps in ((0, "g_p0", 1e-6), (1, "g_v0", 1e-4), (2, "g_p1", 1e-4)):
         u = rng.standard_normal(progs64[k].shape)
-        cases.append((name, u, lambda e, u=u, k=k: loss([p + e * u if j == k else p for j, p in enumerate(progs64)], par0), 1e-4))
+        cases.append((name, u, lambda e, u=u, k=k: loss([p + e * u if j == k else p for j, p in enumerate(progs64)], par0), eps))
     u = rng.standard_normal(R * V) * seg * ea0
     cases.append(("g_ea", u, lambda e, u=u: loss(progs64, [(ea0 + e * u) * l, par0[1], par0[2]]), 1e-4))
     u = rng.standard_normal(R * V) * seg * ei0
@@ -133,9 +138,29 @@ def test_adjoint_matches_fp64_finite_differences():
         fd = (4 * d2 - d1) / 3
         ad = float((g[name] * u.reshape(g[name].shape)).sum())
         a32 = float((g32[name] * u.reshape(g32[name].shape)).sum())
-        floor = abs(a32 - fd) / abs(fd)
+        # FP32 noise floor: the FP32 oracle's error along u and over the whole group
+        floor = max(abs(a32 - fd) / abs(fd), ac.rel(g32[name], g64[name]))
         print(f"\n  {name}: gpu {ad:+.8e} fd64 {fd:+.8e} rel {abs(ad - fd) / abs(fd):.2e} (fp32 oracle {floor:.2e})")
+        assert floor < 1e-2, name  # the rule must not be vacuous
         assert abs(ad - fd) <= max(1e-4, 4 * floor) * abs(fd), name
+
+
+def test_taped_and_replayed_backward_agree():
+    """The backward from the forward's own tape equals the one that replays the frame."""
+    kw = dict(material="c1", plane=True, clearance=-0.002)
+    _, pos = ac.scene(R=R, V=V, **kw)
+    progs = ac.programs(pos, 3, v_std=0.05, p_std=0.01)
+    tgt = ac.targets(pos, 3)
+    global F
+    F0, F = F, 3
+    try:
+        La, ga, _ = _gpu_loss_and_grad(pos, progs, tgt, tape=True, **kw)
+        Lb, gb, _ = _gpu_loss_and_grad(pos, progs, tgt, tape=False, **kw)
+    finally:
+        F = F0
+    assert La == Lb
+    for k in GROUPS:
+        assert np.array_equal(ga[k], gb[k]), k
 
 
 def test_differentiable_frame_forward_is_the_step():
@@ -172,6 +197,9 @@ def test_adjoint_refuses_contact_it_does_not_differentiate():
     st = [t.requires_grad_() for t in rg.state(b)]
     par = rg.parameters(b)
     p0, v0, p1 = (torch.tensor(x[0], device="cuda") for x in progs)
-    out = rg.frame(b, st, par, p0, v0, p1, DT, 10)
+    with pytest.raises(ValueError, match="rope-rope"):  # refused by the taped step or the backward
+        out = rg.frame(b, st, par, p0, v0, p1, DT, 10)
+        out[0].sum().backward()
     with pytest.raises(ValueError, match="rope-rope"):
+        out = rg.frame(b, st, par, p0, v0, p1, DT, 10, tape=False)
         out[0].sum().backward()
