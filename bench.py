@@ -532,7 +532,7 @@ def run_config4(args):
 
     torch.cuda.set_device(0)
     R = args.ropes if args.ropes != 4096 else 1024
-    V, F, S4 = 64, 30, 100
+    V, F, S4 = 64, args.frames, 100
     seg, density, ea, ei = 0.03, 0.1, 500.0, 1e-4
     rng = np.random.default_rng(4)
     roots = np.stack([rng.uniform(-0.5, 0.5, R), rng.uniform(-0.5, 0.5, R), rng.uniform(2.5, 3.5, R)], 1).astype(np.float32)
@@ -599,7 +599,7 @@ def run_config4(args):
                 cur = st
                 loss = 0.0
                 for f in range(F):
-                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4)
+                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4, tape=not args.no_tape)
                     loss = loss + ((cur[0].view(R, V, 3)[:, -1] - tgt[f]) ** 2).sum(-1).mean()
                 loss.backward()
                 grads["finite"] = bool(all(torch.isfinite(t.grad).all() for t in st + par + pr))
@@ -615,7 +615,8 @@ def run_config4(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded config-4 rollouts)",
             "config": {"workload": f"config4-diff-{R}x{V}", "ropes": R, "verts_per_rope": V, "frames": F,
-                       "substeps": S4, "num_itr": ITERS, "step": "one 30-frame rollout",
+                       "substeps": S4, "num_itr": ITERS, "step": f"one {F}-frame rollout",
+                       "backward": "replays each frame" if args.no_tape else "from the forward's substep tapes",
                        "counted": "forward vertex-substeps of the rollout", "l2": "flushed between rollouts (256 MB write)"},
             "forward": out["persistent"], "fwd_bwd": out["fwd_bwd"], "plain_path_forward": out["plain"],
             "fwd_bwd_over_fwd": out["fwd_bwd"]["ms_per_rollout"] / out["persistent"]["ms_per_rollout"],
@@ -636,6 +637,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     ap.add_argument("--block", type=int, default=0, help="bin size (CTA threads); 0 = the library's choice")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
+    ap.add_argument("--frames", type=int, default=30, help="config4: control frames per rollout")
+    ap.add_argument("--no-tape", action="store_true", help="config4: backward replays frames instead of keeping tapes")
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
                     help="config2 (the headline line), config3 (uneven ropes, planes and meshes vs the plain path) "
                          "or config4 (differentiable rollouts: forward and forward + backward)")

@@ -84,7 +84,7 @@ __device__ __forceinline__ void surface_contact_bwd(f3 n, float gap, f3 d, float
 //   LQ [I+1][BLOCK]   frame iterates q^k
 // 64-thread bins at 8 iterations: 25.6 KB, 8 CTAs (16 warps) per SM with <= 128 registers.
 template <int BLOCK, int SURF>
-__global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoint_kernel(const FrameArgs a, const AdjArgs g) {
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const FrameArgs a, const AdjArgs g) {
     extern __shared__ float4 smem[];
     const int I = a.iters;
     float4* X = smem;
@@ -115,7 +115,9 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
     const bool upd = hasNext && !(fl & F_FIX_ORIENT);
     const bool driven = (fl & F_ROOT) && a.root_mode == ROOT_PROGRAM;
     const VConst c = vertex_constants(a, im, lr, ks);
-    KC[t] = make_float4(ks, c.invl, im, 0.f);
+    const float4 qr_own = QR[t];
+    const float irho = hasNext ? 1.f / sqrtf(dot4(qr_own, qr_own)) : 0.f;  // 1 / |qRest| of segment t
+    KC[t] = make_float4(ks, c.invl, im, irho);
     const float h = a.h, invH = 1.f / h;
     const float damp = a.damping / h;
     const f3 gv = mk3(a.gx, a.gy, a.gz);
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
             f3 f, f2;
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(LD[(size_t)k * BLOCK + t + 1]) : zero3();
-            position_terms<SURF>(a, nullptr, 0ull, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            const bool touched = position_terms<SURF>(a, nullptr, 0ull, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
             EA[t] = f4(f2, H2.xx);
             EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
             EC[t].x = H2.yz;
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
                 f += xyz(fa);
                 H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
             }
-            if (im != 0.f) dx += sym_solve(H, f) * a.accel;
+            position_solve(dx, f, H, a.accel, im, !touched);
             LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, 0.f);
             __syncthreads();
             if (upd) {
@@ -256,15 +258,15 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
                 bb = add4(bb, scale4(qmul_pure(vv, Ab), -1.f)); // (vv, 0)* Ā = -(vv, 0) Ā
                 ksb += -2.f * dot(u, vvb);
                 su = vvb * (-2.f * ks * c.invl);
+                // b = sp q_{t-1} r_{t-1} + sn q_{t+1} r_t^*: the rotor adjoints b̄ r^(*) also give the
+                // rest-rotor magnitude adjoints, <q^* b̄, r> = <b̄ r^*, q> and <(q^* b̄)^*, r> = <b̄ r, q>
                 if (hasPrev) {
-                    const float4 bq = scale4(bb, sp);
-                    toL = qmul(bq, qconj(rp));
-                    rhobp += dot4(qmul(qconj(qp), bq), rp) / sqrtf(dot4(rp, rp));
+                    toL = qmul(scale4(bb, sp), qconj(rp));
+                    rhobp += dot4(toL, qp) * KC[t - 1].w;
                 }
                 if (nextOrient) {
-                    const float4 bq = scale4(bb, sn);
-                    toR = qmul(bq, rn);
-                    rhob += dot4(qconj(qmul(qconj(qn), bq)), rn) / sqrtf(dot4(rn, rn));
+                    toR = qmul(scale4(bb, sn), rn);
+                    rhob += dot4(toR, qn) * irho;
                 }
             }
             EA[t] = toL;
@@ -288,6 +290,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
             float trH = 0.f;
             if (im != 0.f) {
                 sym3 H = sym_diag(c.Hd);
+                bool touched = false;
                 if constexpr (SURF != SURF_NONE) {
                     f3 fdummy = zero3();
                     for (int pl = 0; pl < a.num_planes; pl++) {
@@ -296,6 +299,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
                         const float gap = (dot(nrm, p) - P.w) + dot(nrm, dk) - a.c_radius;
                         if (gap >= 0.f) continue;
                         surface_contact(nrm, gap, dk, c.kc, h, a.c_mu_s, a.c_mu_k, a.c_vslip, fdummy, H);
+                        touched = true;
                     }
                 }
                 if (hasNext) {
@@ -307,7 +311,7 @@ __global__ void __launch_bounds__(BLOCK, (BLOCK <= 256 ? 512 / BLOCK : 1)) adjoi
                     const float dd = kp.x * kp.y * kp.y * (1.f + damp);
                     H.xx += dd; H.yy += dd; H.zz += dd;
                 }
-                const f3 e = sym_solve(H, db);
+                const f3 e = touched ? sym_solve(H, db) : db * (1.f / H.xx);
                 const f3 del = xyz(LD[(size_t)(k + 1) * BLOCK + t]) - dk;
                 Fb = e * a.accel;
                 trH = -dot(e, del);
@@ -489,6 +493,7 @@ cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int 
         case 64: return launch_adjoint_b<64>(a, g, num_bins, s);
         case 128: return launch_adjoint_b<128>(a, g, num_bins, s);
         case 256: return launch_adjoint_b<256>(a, g, num_bins, s);
+        case 512: return launch_adjoint_b<512>(a, g, num_bins, s);
         default: return cudaErrorInvalidValue;
     }
 }

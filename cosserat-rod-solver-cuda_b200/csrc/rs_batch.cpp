@@ -1130,7 +1130,54 @@ void Batch::step_program_taped(const float* p0, const float* v0, const float* p1
     pending_tape_ = nullptr;
 }
 
-void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h) {
+float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synchronize) {
+    if (!(dt > 0.f)) throw std::invalid_argument("dt must be > 0");
+    if (substeps < 1) throw std::invalid_argument("substeps must be >= 1");
+    if (!io.pos || !io.vel || !io.lvel || !io.q || !io.p0 || !io.v0 || !io.p1)
+        throw std::invalid_argument("the frame-start state and the program rows are required");
+    if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the end-state outputs are required");
+    if (!roots_pinned()) throw std::invalid_argument("the program frame drives every rope's root");
+    if (io.tape) {
+        if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
+        if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
+    }
+    tune_before_frame();
+    ensure_device();
+    check(launch_state_in(d_topo_, io.pos, io.vel, io.lvel, io.q, d_pos_, d_vel_, d_lvel_, d_pos_, d_vel_, d_lvel_, d_q_, n_,
+                          stream_), "frame state");
+    if (io.ea || io.ei || io.mass) {
+        check(launch_params_in(d_topo_, io.ea, io.ei, io.mass, d_pos_, d_vel_, d_lvel_, d_qrest_, d_qdir_, n_, stream_),
+              "frame parameters");
+        host_const_stale_ = true;
+    }
+    stage_rows(io.p0, io.v0, io.p1, nullptr, nullptr, false);
+    sdf_begin();
+    const float last = h_;
+    pending_tape_ = reinterpret_cast<float4*>(io.tape);
+    const bool plain = engine_ == 1 || (rope_contact_ && oversize_);
+    if (io.tape && plain) { pending_tape_ = nullptr; throw std::invalid_argument("a taped frame runs the persistent engine only"); }
+    run_frame(ROOT_PROGRAM, false, false, dt, substeps, dt / (float)substeps);
+    pending_tape_ = nullptr;
+    time_ += dt;
+    sdf_end(substeps);
+    tune_after_frame();
+    check(launch_state_out(d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, io.o_pos, io.o_vel, io.o_lvel, io.o_q, n_, stream_),
+          "frame outputs");
+    if (synchronize) {
+        check(cudaMemcpyAsync(h_status_, d_status_, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream_), "status");
+        check(cudaStreamSynchronize(stream_), "frame");
+        if (h_status_[0] || h_status_[1] || h_status_[2]) {
+            if (h_status_[2]) nonfinite_ = 1;
+            if (h_status_[1]) last_warning_ = h_status_[1];
+            const int err = h_status_[0];
+            check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
+            if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
+        }
+    }
+    return last;
+}
+
+void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h, bool synchronize) {
     if (!(dt > 0.f)) throw std::invalid_argument("dt must be > 0");
     if (substeps < 1) throw std::invalid_argument("substeps must be >= 1");
     if (!(last_h > 0.f)) throw std::invalid_argument("last_h must be > 0");
@@ -1141,11 +1188,16 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h)
     if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
     if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
     ensure_device();
-    if (block_ > 256)
-        throw std::invalid_argument("the adjoint runs bins of at most 256 vertices (set_block(256) or smaller)");
+    if (block_ > 512)
+        throw std::invalid_argument("the adjoint runs bins of at most 512 vertices (ropes of at most 512 vertices)");
     if (adjoint_smem_bytes(block_, num_itr) > 227 * 1024)
         throw std::invalid_argument("num_itr too large for the adjoint's shared memory at this bin size");
     grad_alloc(io.tape ? 0 : substeps);
+    if (io.ea || io.ei || io.mass) {
+        check(launch_params_in(d_topo_, io.ea, io.ei, io.mass, d_pos_, d_vel_, d_lvel_, d_qrest_, d_qdir_, n_, stream_),
+              "backward parameters");
+        host_const_stale_ = true;
+    }
     if (io.p0) stage_rows(io.p0, io.v0, io.p1, io.q0, io.q1, false);
     FrameArgs a = frame_args(io.p0 ? ROOT_PROGRAM : ROOT_NONE, io.q0 != nullptr, io.q1 != nullptr, dt, substeps);
     a.h = dt / (float)substeps;
@@ -1174,7 +1226,7 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h)
         if (io.o_p1) check(cudaMemsetAsync(io.o_p1, 0, sizeof(float) * 3 * R_, stream_), "zero");
     }
     check(launch_adjoint(a, g, block_, (int)bins_.size(), stream_), "adjoint");
-    check(cudaStreamSynchronize(stream_), "backward");
+    if (synchronize) check(cudaStreamSynchronize(stream_), "backward");
 }
 
 }  // namespace rs

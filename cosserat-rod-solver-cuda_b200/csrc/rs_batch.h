@@ -106,7 +106,9 @@ public:
     // One frame reversed: replays it from the frame-start state (io.pos ...) with the program
     // rows io.p0 / v0 / p1 (null p0 = a free frame), recording a tape, then runs the adjoint
     // kernel. All pointers are device, caller order. The batch's own state is not touched.
-    // With io.tape (the tape a step_program_taped of this frame recorded) the replay is skipped.
+    // With io.tape (the tape a step_program_taped of this frame recorded) the replay is skipped;
+    // io.ea / ei / mass (optional) are the frame's parameters, applied first. With synchronize
+    // false the call returns with the work queued on the handle's stream.
     struct BackwardIO {
         const float *pos, *vel, *lvel, *q;
         const float *p0, *v0, *p1, *q0, *q1;
@@ -114,8 +116,19 @@ public:
         float *o_pos, *o_vel, *o_lvel, *o_q;
         float *o_ea, *o_ei, *o_mass, *o_p0, *o_v0, *o_p1;
         const float* tape;
+        const float *ea, *ei, *mass;
     };
-    void backward(const BackwardIO& io, float dt, int substeps, float last_h);
+    void backward(const BackwardIO& io, float dt, int substeps, float last_h, bool synchronize = true);
+    // One differentiable program frame in one call: load the state and (optional) parameters,
+    // step, write the end state (and the tape when given). Returns the frame's lastH.
+    struct FrameIO {
+        const float *pos, *vel, *lvel, *q;
+        const float *ea, *ei, *mass;
+        const float *p0, *v0, *p1;
+        float *o_pos, *o_vel, *o_lvel, *o_q;
+        float* tape;
+    };
+    float frame_forward(const FrameIO& io, float dt, int substeps, bool synchronize);
     // step_program that also records the frame's substep tape (device, 16 * substeps * n
     // floats, caller order) for a later backward of this frame.
     void step_program_taped(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1,

@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             f3 f, f2;
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
-            position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            const bool touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
             if constexpr (ROPE) {
                 if (ncol > 0) {
                     // even candidates join the own terms, odd ones a second partial added after
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
                 H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
             }
             if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
-            else position_solve(dx, f, H, a.accel, im);
+            else position_solve(dx, f, H, a.accel, im, !touched);
             if (act) sm.dx[t] = f4(dx, 0.f);
             __syncthreads();  // B2
 

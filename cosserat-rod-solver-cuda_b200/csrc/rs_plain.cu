@@ -119,6 +119,7 @@ __global__ void __launch_bounds__(kPosBlock) plain_position_kernel(const FrameAr
     f3 f = zero3(), f2 = zero3(), dx = zero3();
     sym3 H = sym_zero(), H2 = sym_zero();
     float im = 0.f;
+    bool touched = false;
     float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
     if (valid) {
         const int4 tp = a.topo[d];
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(kPosBlock) plain_position_kernel(const FrameAr
         const float4* cache = (SURF == SURF_MESHES) ? env_poses(a, b, tp.w) : nullptr;
         const uint64_t cand = (SURF == SURF_MESHES) ? b.cand[d] : 0ull;
         const float damp = a.damping / a.h;
-        position_terms<SURF>(a, cache, cand, c, hasNext, xyz(P), p1, dx, p1dx, xyz(b.y[d]), q, damp, f, H, f2, H2);
+        touched = position_terms<SURF>(a, cache, cand, c, hasNext, xyz(P), p1, dx, p1dx, xyz(b.y[d]), q, damp, f, H, f2, H2);
         if constexpr (ROPE) {
             const int nc = hasNext ? a.ncols[d] : 0;
             if (nc > 0) {
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(kPosBlock) plain_position_kernel(const FrameAr
         const float lim = (fl & F_PREV) ? fminf(a.maxstep[d], a.maxstep[d - 1]) : a.maxstep[d];
         position_solve_limited(dx, f, H, a.accel, im, lim);
     } else {
-        position_solve(dx, f, H, a.accel, im);
+        position_solve(dx, f, H, a.accel, im, !touched);
     }
     b.dxn[d] = f4(dx, 0.f);
     b.qprev[d] = q;

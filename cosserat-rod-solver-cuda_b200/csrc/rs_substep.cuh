@@ -102,16 +102,19 @@ __device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, 
 
 // Surfaces (planes, then candidate meshes in ascending index) at one probe point,
 // contact.cuh:141-163; with `wr` != nullptr it is the readout (contact.cuh:172-204): mesh
-// forces are added to *facc and their wrenches to wr[m * 6 ...].
+// forces are added to *facc and their wrenches to wr[m * 6 ...]. Returns whether any contact
+// term was added (H then stops being a multiple of the identity).
 template <int SURF>
-__device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
+__device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
                                          float h, f3& f, sym3& H, float* wr, f3* facc) {
+    bool touched = false;
     for (int pl = 0; pl < a.num_planes; pl++) {
         const float4 P = a.planes[pl];
         const f3 n = mk3(P.x, P.y, P.z);
         const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
         if (gap >= 0.f) continue;
         surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
+        touched = true;
     }
     if constexpr (SURF == SURF_MESHES) {
     for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
@@ -120,6 +123,7 @@ __device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache
         f3 n, dRel;
         float gap;
         if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, n, gap, dRel)) continue;
+        touched = true;
         if (wr) {
             f3 fm = zero3();
             sym3 Hs = sym_zero();
@@ -135,6 +139,7 @@ __device__ __forceinline__ void surfaces(const FrameArgs& a, const float4* cache
         }
     }
     }
+    return touched;
 }
 
 // Inertial target y and initial guess dx from the substep's start velocity, iteration.cu:34-68.
@@ -167,13 +172,15 @@ __device__ __forceinline__ VConst vertex_constants(const FrameArgs& a, float im,
 
 // Position-step terms of vertex i, cosserat.cu:37-88: own force f / Hessian H (inertia, then
 // surfaces, then the stretch of segment i) and the segment's share f2 / H2 on vertex i + 1.
+// Returns whether a surface contact touched H (otherwise H is a multiple of the identity).
 template <int SURF>
-__device__ __forceinline__ void position_terms(const FrameArgs& a, const float4* cache, uint64_t cand, const VConst& c,
+__device__ __forceinline__ bool position_terms(const FrameArgs& a, const float4* cache, uint64_t cand, const VConst& c,
                                                bool hasNext, f3 p, f3 p1, f3 dx, f3 p1dx, f3 y, float4 q, float damp,
                                                f3& f, sym3& H, f3& f2, sym3& H2) {
     f = (y - dx) * c.fm;
     H = sym_diag(c.Hd);
-    if (SURF != SURF_NONE && c.im != 0.f) surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr);
+    bool touched = false;
+    if (SURF != SURF_NONE && c.im != 0.f) touched = surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr);
     f2 = zero3();
     H2 = sym_zero();
     if (hasNext) {
@@ -186,6 +193,7 @@ __device__ __forceinline__ void position_terms(const FrameArgs& a, const float4*
         H.xx += dd; H.yy += dd; H.zz += dd;
         H2.xx += dd; H2.yy += dd; H2.zz += dd;
     }
+    return touched;
 }
 
 // One rope-rope candidate of segment (p, p1) with iterates (d, p1d) against the segment
@@ -248,9 +256,10 @@ __device__ __forceinline__ float step_limit_of(f3 a0, f3 a1, f3 pj0, f3 pj1) {
     return ((1.f - 0.1f) * 0.5f) * len(nn);
 }
 
-// Local solve dx += accel * H^-1 f of a free vertex, cosserat.cu:206-209.
-__device__ __forceinline__ void position_solve(f3& dx, f3 f, const sym3& H, float accel, float im) {
-    if (im != 0.f) dx += sym_solve(H, f) * accel;
+// Local solve dx += accel * H^-1 f of a free vertex, cosserat.cu:206-209. Without contact
+// terms (`diag`) H is a multiple of the identity and the solve is one division.
+__device__ __forceinline__ void position_solve(f3& dx, f3 f, const sym3& H, float accel, float im, bool diag) {
+    if (im != 0.f) dx += diag ? f * (accel / H.xx) : sym_solve(H, f) * accel;
 }
 // The same with the step limit of rope-rope contact, cosserat.cu:211-214.
 __device__ __forceinline__ void position_solve_limited(f3& dx, f3 f, const sym3& H, float accel, float im, float lim) {

@@ -69,7 +69,11 @@ def parameters(batch):
 
 
 class Frame(torch.autograd.Function):
-    """(pos, vel, lvel, q, ea, ei, mass, p0, v0, p1) -> frame-end (pos, vel, lvel, q)."""
+    """(pos, vel, lvel, q, ea, ei, mass, p0, v0, p1) -> frame-end (pos, vel, lvel, q).
+
+    Forward and backward are one library call each (rs_batch_frame_forward, rs_batch_backward),
+    queued on the batch's stream without host synchronization; torch's current stream and the
+    batch's stream are ordered with events on both sides."""
 
     @staticmethod
     def forward(ctx, batch, dt, substeps, tape, pos, vel, lvel, q, ea, ei, mass, p0, v0, p1):
@@ -79,27 +83,24 @@ class Frame(torch.autograd.Function):
         q = _check(q, (n, 4), "q")
         ea, ei, mass = (_check(t, (n,), k) for t, k in ((ea, "ea"), (ei, "ei"), (mass, "mass")))
         p0, v0, p1 = (_check(t, (R, 3), k) for t, k in ((p0, "p0"), (v0, "v0"), (p1, "p1")))
-        last_h = float(batch.current_h)
-        batch.set_state(pos, vel, lvel, q)
-        batch.set_parameters(ea, ei, mass)
-        ctx.tape = None
-        if tape:
-            # keep this frame's substep tape (64 B per vertex-substep) so the backward skips the replay
-            ctx.tape = torch.empty(16 * int(substeps) * n, device="cuda", dtype=torch.float32)
-            batch._step_taped(p0, v0, p1, dt, substeps, ctx.tape.data_ptr())
-        else:
-            batch.step(p0, v0, dt, substeps, root_pos_end=p1)
-        out = state(batch)
-        ctx.batch, ctx.dt, ctx.substeps, ctx.last_h = batch, float(dt), int(substeps), last_h
+        out = [torch.empty(n, k, device="cuda", dtype=torch.float32) for k in (3, 3, 3, 4)]
+        # the frame's substep tape (64 B per vertex-substep) lets the backward skip the replay
+        ctx.tape = torch.empty(16 * int(substeps) * n, device="cuda", dtype=torch.float32) if tape else None
+        cur, ext = _streams(batch)
+        ext.wait_stream(cur)
+        ptrs = [_ptr(t) for t in (pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)] + [_ptr(t) for t in out]
+        ptrs.append(_ptr(ctx.tape))
+        last_h = batch._frame_forward(ptrs, float(dt), int(substeps))
+        cur.wait_stream(ext)
+        ctx.batch, ctx.dt, ctx.substeps, ctx.last_h = batch, float(dt), int(substeps), float(last_h)
         ctx.save_for_backward(pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)
-        return out
+        return tuple(out)
 
     @staticmethod
     def backward(ctx, g_pos, g_vel, g_lvel, g_q):
         pos, vel, lvel, q, ea, ei, mass, p0, v0, p1 = ctx.saved_tensors
         b = ctx.batch
         n, R = pos.shape[0], p0.shape[0]
-        b.set_parameters(ea, ei, mass)
         g_in = [None if g is None else g.detach().contiguous().to(torch.float32) for g in (g_pos, g_vel, g_lvel, g_q)]
         o = [torch.empty(n, 3, device="cuda", dtype=torch.float32) for _ in range(3)]
         o.append(torch.empty(n, 4, device="cuda", dtype=torch.float32))
@@ -107,11 +108,26 @@ class Frame(torch.autograd.Function):
         og = [torch.empty(R, 3, device="cuda", dtype=torch.float32) for _ in range(3)]
         ptrs = [_ptr(t) for t in (pos, vel, lvel, q, p0, v0, p1, None, None)]
         ptrs += [_ptr(t) for t in g_in] + [_ptr(t) for t in o] + [_ptr(t) for t in op] + [_ptr(t) for t in og]
-        ptrs.append(_ptr(ctx.tape))
+        ptrs += [_ptr(ctx.tape), _ptr(ea), _ptr(ei), _ptr(mass)]
+        cur, ext = _streams(b)
+        ext.wait_stream(cur)
         b._backward(ptrs, ctx.dt, ctx.substeps, ctx.last_h)
+        cur.wait_stream(ext)
         ctx.tape = None
         grads = [t.reshape(sh) for t, sh in zip(o + op + og, ctx.shapes)]
         return (None, None, None, None, *grads)
+
+
+def _streams(batch):
+    cur = torch.cuda.current_stream()
+    ext = getattr(batch, "_torch_stream", None)
+    if ext is None:
+        ext = torch.cuda.ExternalStream(batch.stream_ptr())
+        try:
+            batch._torch_stream = ext
+        except AttributeError:
+            pass
+    return cur, ext
 
 
 def frame(batch, st, params, p0, v0, p1, dt, substeps, tape=True):

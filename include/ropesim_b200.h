@@ -231,9 +231,25 @@ typedef struct rs_backward_io {
     float *o_pos, *o_vel, *o_lvel, *o_q;
     float *o_ea, *o_ei, *o_mass;
     float *o_p0, *o_v0, *o_p1;
-    const float* tape;  /* NULL = replay the frame; else this frame's rs_batch_step_program_taped tape */
+    const float* tape;  /* NULL = replay the frame; else this frame's recorded tape */
+    const float *ea, *ei, *mass;  /* the frame's parameters (NULL = the handle's current ones) */
 } rs_backward_io;
 RS_API int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
+/* The same, returning with the work queued on the handle's stream (no host synchronization). */
+RS_API int rs_batch_backward_async(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
+/* One differentiable program frame in one call (device pointers, caller order): loads the
+ * frame-start state and the parameters (NULL = keep), steps with the program rows p0 / v0 / p1
+ * [R,3], writes the end state to out_* and, when tape != NULL (16 * substeps * n floats), the
+ * substep tape for rs_batch_backward. *last_h receives the frame's lastH (RS_P_H before the
+ * frame). Queued on the handle's stream without host synchronization. */
+typedef struct rs_frame_io {
+    const float *pos, *vel, *lvel, *q;
+    const float *ea, *ei, *mass;
+    const float *p0, *v0, *p1;
+    float *out_pos, *out_vel, *out_lvel, *out_q;
+    float* tape;
+} rs_frame_io;
+RS_API int rs_batch_frame_forward(rs_batch* b, const rs_frame_io* io, float dt, int substeps, float* last_h);
 /* rs_batch_step_program that also records the frame's substep tape for rs_batch_backward:
  * tape = device buffer of 16 * substeps * n floats (the state after each substep's root
  * program, caller order), so that the backward need not replay the frame. */
