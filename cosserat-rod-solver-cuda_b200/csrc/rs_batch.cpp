@@ -107,7 +107,10 @@ Batch::Batch(int num_ropes, const int* rope_verts, const float* positions, const
 
 Batch::~Batch() {
     if (stream_) cudaStreamSynchronize(stream_);
-    for (auto& g : grids_) cudaFree(const_cast<float*>(g.v));
+    for (auto& g : grids_) {
+        cudaFree(const_cast<float*>(g.v));
+        cudaFree(const_cast<float*>(g.bmin));
+    }
     void* bufs[] = {d_bins_, d_ropes_, d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, d_qrest_, d_qdir_, d_init_pos_, d_init_q_,
                     d_out_pos_, d_out_vel_, d_out_q_, d_prog_, d_status_, d_ranges_, d_boxes_, d_cur_, d_tgt_,
                     d_tele_, d_motion_, d_poses_, d_stage_, d_stage_tele_, d_force_, d_wrench_};
@@ -546,6 +549,12 @@ FrameArgs Batch::frame_args(int root_mode, bool has_q0, bool has_q1, float dt, i
     a.det_radius = rc_radius_ + 0.5f * rc_barrier_;          // uploadMeta, YarnBall.cu:262-263
     a.sdet_radius = a.det_radius * rc_scaler_;
     a.grp = d_grp_; a.cols = d_cols_; a.ncols = d_ncols_; a.maxstep = d_maxstep_; a.pad = d_pad_;
+    a.sdf_skip = 1;
+    // stage the lattices' block bounds in each CTA's shared memory when they take <= 48 KB and
+    // the CTA's shared memory (frame state 144 B per thread, pose cache, bounds) stays <= 200 KB
+    const size_t btot = grids_.empty() ? 0 : (size_t)(grids_.back().boff + grids_.back().bcount);
+    const size_t smem = (size_t)144 * block_ + (size_t)2 * a.pose_cache * sizeof(Pose) + btot * sizeof(float);
+    a.sdf_btab = (btot * sizeof(float) <= 48 * 1024 && smem <= 200 * 1024) ? (int)btot : 0;
     return a;
 }
 
@@ -592,6 +601,7 @@ void Batch::run_frame_plain(const FrameArgs& a) {
     plain_alloc();
     check(cudaStreamSynchronize(stream_), "plain args reuse");  // the previous frame read h_pl_args_
     *h_pl_args_ = a;
+    h_pl_args_->sdf_skip = 0;  // the plain path samples every candidate lattice, as the reference does
     check(cudaMemcpyAsync(d_pl_args_, h_pl_args_, sizeof(FrameArgs), cudaMemcpyHostToDevice, stream_), "upload(args)");
     const int surf = a.num_sdf > 0 ? 2 : (a.num_planes > 0 ? 1 : 0);
     const std::string key = std::to_string(a.iters) + ":" + std::to_string(surf) + ":" + std::to_string(a.rope_contact);
@@ -919,6 +929,30 @@ int Batch::add_mesh(const float* values, int nx, int ny, int nz, const float* or
     g.v = d; g.nx = nx; g.ny = ny; g.nz = nz;
     g.ox = origin[0]; g.oy = origin[1]; g.oz = origin[2];
     g.h = spacing; g.invH = 1.f / spacing; g.muS = mu_s; g.muK = mu_k;
+    // lower bounds of the field per block of kSdfBlock^3 cells (the persistent kernel's exact
+    // early out; the block's face nodes are shared with its neighbours)
+    const int bnx = (nx - 2) / kSdfBlock + 1, by = (ny - 2) / kSdfBlock + 1, bz = (nz - 2) / kSdfBlock + 1;
+    std::vector<float> bmin((size_t)bnx * by * bz, std::numeric_limits<float>::infinity());
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const float val = values[((size_t)i * ny + j) * nz + k];
+                // node i belongs to the blocks of cells i - 1 and i
+                for (int ci = std::max(0, i - 1); ci <= std::min(i, nx - 2); ci++)
+                    for (int cj = std::max(0, j - 1); cj <= std::min(j, ny - 2); cj++)
+                        for (int ck = std::max(0, k - 1); ck <= std::min(k, nz - 2); ck++) {
+                            float& m = bmin[((size_t)(ci / kSdfBlock) * by + cj / kSdfBlock) * bz + ck / kSdfBlock];
+                            m = std::min(m, val);
+                        }
+            }
+    float* db = nullptr;
+    const cudaError_t e2 = cudaMalloc(&db, sizeof(float) * bmin.size());
+    if (e2 != cudaSuccess) { cudaFree(d); check(e2, "cudaMalloc(sdf block bounds)"); }
+    const cudaError_t e3 = cudaMemcpy(db, bmin.data(), sizeof(float) * bmin.size(), cudaMemcpyHostToDevice);
+    if (e3 != cudaSuccess) { cudaFree(d); cudaFree(db); check(e3, "upload(sdf block bounds)"); }
+    g.bmin = db; g.by = by; g.bz = bz;
+    g.bcount = (int)bmin.size();
+    g.boff = grids_.empty() ? 0 : grids_.back().boff + grids_.back().bcount;
     grids_.push_back(g);
     const float bx[6] = {origin[0], origin[1], origin[2], origin[0] + float(nx - 1) * spacing,
                          origin[1] + float(ny - 1) * spacing, origin[2] + float(nz - 1) * spacing};
@@ -980,7 +1014,10 @@ void Batch::set_mesh_targets(int index, const float* pos, const float* quat, int
 
 void Batch::clear_meshes() {
     check(cudaStreamSynchronize(stream_), "clear_meshes");
-    for (auto& g : grids_) cudaFree(const_cast<float*>(g.v));
+    for (auto& g : grids_) {
+        cudaFree(const_cast<float*>(g.v));
+        cudaFree(const_cast<float*>(g.bmin));
+    }
     grids_.clear();
     boxes_.clear();
     pending_set_ = false;

@@ -189,12 +189,28 @@ __device__ __forceinline__ void world_box(f3 lo_o, f3 hi_o, f3 pos, float4 q, f3
     }
 }
 
+// Exact early out: the trilinear field inside a lattice block is at least the block's smallest
+// node value, so a block whose bound clears the radius (by more than the rounding of the
+// interpolation, 1e-5) cannot produce gap < 0.
+// `btab`: the CTA's shared-memory copy of the bound tables (nullptr: read them from L2).
+__device__ __forceinline__ bool sdf_block_clear(const rs::GridDesc& g, const float* btab, f3 p, float R) {
+    const f3 u = (p - mk3(g.ox, g.oy, g.oz)) * g.invH;
+    if (!(u.x >= 0.f && u.y >= 0.f && u.z >= 0.f && u.x < float(g.nx - 1) && u.y < float(g.ny - 1) &&
+          u.z < float(g.nz - 1)))
+        return true;  // outside the lattice: sdf_sample reports no contact either
+    const int bi = (int)u.x / rs::kSdfBlock, bj = (int)u.y / rs::kSdfBlock, bk = (int)u.z / rs::kSdfBlock;
+    const int idx = (bi * g.by + bj) * g.bz + bk;
+    return (btab ? btab[g.boff + idx] : __ldg(g.bmin + idx)) - R > 1e-5f;
+}
+
 // Contact of a vertex with one posed lattice at probe (pos - P.pos) + d, contact.cuh:94-110.
 __device__ __forceinline__ bool sdf_contact_at(const rs::GridDesc& g, const PoseV& P, f3 pos, f3 d, float h, float R,
-                                               bool moving, f3& n, float& gap, f3& dRel) {
+                                               bool moving, bool skip, const float* btab, f3& n, float& gap, f3& dRel) {
     float phi;
     f3 gr;
-    if (!sdf_sample(g, qrot(qconj(P.q), (pos - P.pos) + d), phi, gr)) return false;
+    const f3 po = qrot(qconj(P.q), (pos - P.pos) + d);
+    if (skip && sdf_block_clear(g, btab, po, R)) return false;
+    if (!sdf_sample(g, po, phi, gr)) return false;
     gap = phi - R;
     if (gap >= 0.f) return false;
     const float gl = len(gr);

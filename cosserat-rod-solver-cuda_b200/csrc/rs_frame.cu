@@ -44,6 +44,9 @@ struct FrameSmem {
     int flg[BLOCK];       // vertex flags (rope-rope detection reads the group's)
 };
 
+// The host sizes the CTA's shared memory with 144 B of frame state per thread (rs_batch.cpp).
+static_assert(sizeof(FrameSmem<64>) == 144 * 64 && sizeof(FrameSmem<1024>) == 144 * 1024, "FrameSmem layout");
+
 // Resident CTAs per SM the register allocation targets: 28 warps per SM (<= 72 registers;
 // 24 warps for 256-thread CTAs) without meshes, 16 warps per SM (<= 128 registers) with meshes.
 #ifndef RS_MIN_BLOCKS
@@ -52,7 +55,8 @@ struct FrameSmem {
 
 template <int BLOCK, int SURF, bool ROPE>
 __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame_kernel(const FrameArgs a) {
-    extern __shared__ float4 dyn_smem[];  // FrameSmem<BLOCK>, then the pose cache [2][pose_cache][kPoseF4]
+    // FrameSmem<BLOCK>, the pose cache [2][pose_cache][kPoseF4], then the lattice block bounds
+    extern __shared__ float4 dyn_smem[];
     FrameSmem<BLOCK>& sm = *reinterpret_cast<FrameSmem<BLOCK>*>(dyn_smem);
     float4* pose_smem = dyn_smem + sizeof(FrameSmem<BLOCK>) / sizeof(float4);
 
@@ -117,6 +121,16 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
 #pragma unroll
             for (int k = 0; k < kPoseF4; k++) { cache0[e * kPoseF4 + k] = src[k]; cache1[e * kPoseF4 + k] = src[k]; }
         }
+    }
+    // lattice block bounds staged once per frame (read before the first iteration, after B0)
+    const float* btab = nullptr;
+    if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_btab > 0) {
+        float* bt = reinterpret_cast<float*>(pose_smem + (size_t)2 * a.pose_cache * kPoseF4);
+        for (int m = 0; m < nsdf; m++) {
+            const GridDesc& gd = a.grids[m];
+            for (int e = t; e < gd.bcount; e += BLOCK) bt[gd.boff + e] = __ldg(gd.bmin + e);
+        }
+        btab = bt;
     }
     uint64_t cand = all_meshes(nsdf);  // the first substep of a frame visits every mesh
     f3 facc = zero3();
@@ -191,7 +205,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             f3 f, f2;
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
-            const bool touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            const bool touched =
+                position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2, btab);
             if constexpr (ROPE) {
                 if (ncol > 0) {
                     // even candidates join the own terms, odd ones a second partial added after
@@ -242,7 +257,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             if (SURF != SURF_NONE && a.forces_on) {
                 f3 fv = zero3();
                 sym3 Hs = sym_zero();
-                surfaces<SURF>(a, mycache, cand, p, dx, c.kc, h, fv, Hs, wrow, &fv);
+                surfaces<SURF>(a, mycache, cand, p, dx, c.kc, h, fv, Hs, wrow, &fv, btab);
                 facc += fv;
             }
         }
@@ -287,7 +302,8 @@ static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_
 template <int BLOCK, bool ROPE>
 static cudaError_t launch_frame_r(const FrameArgs& a, int num_bins, cudaStream_t s) {
     if (a.num_sdf > 0)
-        return launch_frame_t<BLOCK, SURF_MESHES, ROPE>(a, num_bins, (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4), s);
+        return launch_frame_t<BLOCK, SURF_MESHES, ROPE>(
+            a, num_bins, (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4) + (size_t)a.sdf_btab * sizeof(float), s);
     if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES, ROPE>(a, num_bins, 0, s);
     return launch_frame_t<BLOCK, SURF_NONE, ROPE>(a, num_bins, 0, s);
 }

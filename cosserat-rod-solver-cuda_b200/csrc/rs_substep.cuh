@@ -106,7 +106,7 @@ __device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, 
 // term was added (H then stops being a multiple of the identity).
 template <int SURF>
 __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
-                                         float h, f3& f, sym3& H, float* wr, f3* facc) {
+                                         float h, f3& f, sym3& H, float* wr, f3* facc, const float* btab = nullptr) {
     bool touched = false;
     for (int pl = 0; pl < a.num_planes; pl++) {
         const float4 P = a.planes[pl];
@@ -122,7 +122,8 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
         const PoseV P = load_pose(cache + m * kPoseF4);
         f3 n, dRel;
         float gap;
-        if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, n, gap, dRel)) continue;
+        if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, a.sdf_skip != 0, btab, n, gap, dRel))
+            continue;
         touched = true;
         if (wr) {
             f3 fm = zero3();
@@ -176,11 +177,12 @@ __device__ __forceinline__ VConst vertex_constants(const FrameArgs& a, float im,
 template <int SURF>
 __device__ __forceinline__ bool position_terms(const FrameArgs& a, const float4* cache, uint64_t cand, const VConst& c,
                                                bool hasNext, f3 p, f3 p1, f3 dx, f3 p1dx, f3 y, float4 q, float damp,
-                                               f3& f, sym3& H, f3& f2, sym3& H2) {
+                                               f3& f, sym3& H, f3& f2, sym3& H2, const float* btab = nullptr) {
     f = (y - dx) * c.fm;
     H = sym_diag(c.Hd);
     bool touched = false;
-    if (SURF != SURF_NONE && c.im != 0.f) touched = surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr);
+    if (SURF != SURF_NONE && c.im != 0.f)
+        touched = surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr, btab);
     f2 = zero3();
     H2 = sym_zero();
     if (hasNext) {

@@ -48,13 +48,18 @@ struct Rope {
 };
 
 // A signed-distance lattice: values[nx, ny, nz] (C order) at origin + ijk * h, object frame.
+// bmin[bx, by, bz]: the smallest node value of each block of kSdfBlock^3 cells (nodes of the
+// block's faces included), a lower bound of the trilinear field inside the block.
+constexpr int kSdfBlock = 8;
 struct GridDesc {
     const float* v;
+    const float* bmin;
     int nx, ny, nz;
     float ox, oy, oz;
     float h, invH;
     float muS, muK;
-    float pad_;
+    int by, bz;
+    int bcount, boff;  // blocks of this lattice, and its offset in the CTA-staged bound tables
 };
 
 // Kinematic pose of (env, mesh) at the end of a substep: position, rotor (x, y, z, w),
@@ -130,6 +135,8 @@ struct FrameArgs {
     float* maxstep;          // [n] step limits (plain engine)
     float* pad;              // [n] detection paddings (plain engine)
     GridDesc grids[kMaxSdf];
+    int sdf_skip;            // 1: a lattice block whose lower bound clears the radius skips the sample
+    int sdf_btab;            // floats of block bounds staged per CTA in shared memory (0 = read from L2)
     // differentiable frames: when set, the state after each substep's root program is written to
     // tape[(s * 4 + f) * n + u] for f = x, v, lv (previous substep's start velocity), q and the
     // caller-order index u
