@@ -227,7 +227,7 @@ void Batch::pack() {
     block_ = std::min(blk, 1024);
     const int M = (int)grids_.size();
     int cap = max_ropes_per_bin_;
-    if (M > 0) cap = std::min(cap, std::max(1, (96 * 1024) / (2 * M * (int)sizeof(Pose))));
+    if (M > 0) cap = std::min(cap, std::max(1, (96 * 1024) / (2 * M * (int)(sizeof(Pose) + 2 * sizeof(float4)))));
     std::vector<int> order(units.size());
     std::iota(order.begin(), order.end(), 0);
     if (!oversize_)
@@ -553,7 +553,8 @@ FrameArgs Batch::frame_args(int root_mode, bool has_q0, bool has_q1, float dt, i
     // stage the lattices' block bounds in each CTA's shared memory when they take <= 48 KB and
     // the CTA's shared memory (frame state 144 B per thread, pose cache, bounds) stays <= 200 KB
     const size_t btot = grids_.empty() ? 0 : (size_t)(grids_.back().boff + grids_.back().bcount);
-    const size_t smem = (size_t)144 * block_ + (size_t)2 * a.pose_cache * sizeof(Pose) + btot * sizeof(float);
+    const size_t smem = (size_t)144 * block_ + (size_t)2 * a.pose_cache * (sizeof(Pose) + 2 * sizeof(float4)) +
+                        btot * sizeof(float);
     a.sdf_btab = (btot * sizeof(float) <= 48 * 1024 && smem <= 200 * 1024) ? (int)btot : 0;
     return a;
 }
@@ -909,6 +910,36 @@ void Batch::set_block(int block) {
 // ------------------------------------------------------------------ contact
 void Batch::set_contact(float radius, float mu_s, float mu_k, float v_slip, float kappa) {
     c_radius_ = radius; c_mu_s_ = mu_s; c_mu_k_ = mu_k; c_vslip_ = v_slip; c_kappa_ = kappa;
+    refresh_contact_boxes();
+}
+// The union of the lattice blocks whose lower bound does not clear the contact radius: outside
+// it no probe can reach gap < 0 (the persistent kernel's exact per-iteration rejection).
+void Batch::refresh_contact_boxes() {
+    for (size_t m = 0; m < grids_.size(); m++) {
+        GridDesc& g = grids_[m];
+        const std::vector<float>& b = bmin_host_[m];
+        const int bx = (g.nx - 2) / kSdfBlock + 1;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        const int n[3] = {g.nx, g.ny, g.nz}, bn[3] = {bx, g.by, g.bz};
+        const float o[3] = {g.ox, g.oy, g.oz};
+        bool any = false;
+        for (int i = 0; i < bn[0]; i++)
+            for (int j = 0; j < bn[1]; j++)
+                for (int k = 0; k < bn[2]; k++) {
+                    if (b[((size_t)i * g.by + j) * g.bz + k] - c_radius_ > 1e-5f) continue;
+                    any = true;
+                    const int ijk[3] = {i, j, k};
+                    for (int a = 0; a < 3; a++) {
+                        lo[a] = std::min(lo[a], o[a] + float(ijk[a] * kSdfBlock) * g.h);
+                        hi[a] = std::max(hi[a], o[a] + float(std::min(ijk[a] * kSdfBlock + kSdfBlock, n[a] - 1)) * g.h);
+                    }
+                }
+        g.never = any ? 0 : 1;
+        for (int a = 0; a < 3; a++) {
+            g.tlo[a] = any ? lo[a] - 1e-4f : 0.f;
+            g.thi[a] = any ? hi[a] + 1e-4f : 0.f;
+        }
+    }
 }
 void Batch::set_planes(int count, const float* rows) {
     for (int p = 0; p < count; p++)
@@ -954,6 +985,8 @@ int Batch::add_mesh(const float* values, int nx, int ny, int nz, const float* or
     g.bcount = (int)bmin.size();
     g.boff = grids_.empty() ? 0 : grids_.back().boff + grids_.back().bcount;
     grids_.push_back(g);
+    bmin_host_.push_back(std::move(bmin));
+    refresh_contact_boxes();
     const float bx[6] = {origin[0], origin[1], origin[2], origin[0] + float(nx - 1) * spacing,
                          origin[1] + float(ny - 1) * spacing, origin[2] + float(nz - 1) * spacing};
     boxes_.insert(boxes_.end(), bx, bx + 6);
@@ -966,7 +999,7 @@ int Batch::add_mesh(const float* values, int nx, int ny, int nz, const float* or
     pending_set_ = pending;
     // the per-CTA pose cache must still fit: repack with fewer ropes per bin if needed
     const int M = (int)grids_.size();
-    const int cap = std::max(1, (96 * 1024) / (2 * M * (int)sizeof(Pose)));
+    const int cap = std::max(1, (96 * 1024) / (2 * M * (int)(sizeof(Pose) + 2 * sizeof(float4))));
     if (max_rcount_ > cap) {
         ensure_host();
         layout_valid_ = false;
@@ -1019,6 +1052,7 @@ void Batch::clear_meshes() {
         cudaFree(const_cast<float*>(g.bmin));
     }
     grids_.clear();
+    bmin_host_.clear();
     boxes_.clear();
     pending_set_ = false;
     moving_ = false;

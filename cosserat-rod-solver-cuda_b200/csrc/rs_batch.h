@@ -197,6 +197,8 @@ private:
     void sdf_end(int substeps);
     void check(cudaError_t e, const char* what);
     int pose_cache_entries() const;
+    void refresh_contact_boxes();   // GridDesc::tlo/thi/never for the current contact radius
+    std::vector<std::vector<float>> bmin_host_;   // per lattice: the block bounds (host copy)
 
     std::mutex mtx_;
     int R_ = 0, n_ = 0;

@@ -113,6 +113,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
     const int nPose = bin.rcount * nsdf;
     float4* cache0 = pose_smem;
     float4* cache1 = pose_smem + (size_t)a.pose_cache * kPoseF4;
+    float4* tbox0 = pose_smem + (size_t)2 * a.pose_cache * kPoseF4;  // contact boxes [2][pose_cache][2]
+    float4* tbox1 = tbox0 + (size_t)2 * a.pose_cache;
     if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && !a.sdf_moving) {
         for (int e = t; e < nPose; e += BLOCK) {
             const int r = e / nsdf, m = e % nsdf;
@@ -120,12 +122,16 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             const float4* src = reinterpret_cast<const float4*>(a.poses + (size_t)en * kMaxSdf + m);
 #pragma unroll
             for (int k = 0; k < kPoseF4; k++) { cache0[e * kPoseF4 + k] = src[k]; cache1[e * kPoseF4 + k] = src[k]; }
+            const PoseV P = load_pose(src);
+            contact_box(a.grids[m], P.pos, P.q, tbox0 + 2 * e);
+            tbox1[2 * e] = tbox0[2 * e];
+            tbox1[2 * e + 1] = tbox0[2 * e + 1];
         }
     }
     // lattice block bounds staged once per frame (read before the first iteration, after B0)
     const float* btab = nullptr;
     if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_btab > 0) {
-        float* bt = reinterpret_cast<float*>(pose_smem + (size_t)2 * a.pose_cache * kPoseF4);
+        float* bt = reinterpret_cast<float*>(tbox0 + (size_t)4 * a.pose_cache);
         for (int m = 0; m < nsdf; m++) {
             const GridDesc& gd = a.grids[m];
             for (int e = t; e < gd.bcount; e += BLOCK) bt[gd.boff + e] = __ldg(gd.bmin + e);
@@ -152,13 +158,17 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             tp[3 * (size_t)a.n] = q;
         }
         float4* cache = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
+        float4* tbox = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? tbox1 : tbox0) : tbox0;
         if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_moving) {
             for (int e = t; e < nPose; e += BLOCK) {
                 const int r = e / nsdf, m = e % nsdf;
                 compute_pose(a, a.ropes[bin.rstart + r].user, m, s, S, h, cache + e * kPoseF4);
+                const PoseV P = load_pose(cache + e * kPoseF4);
+                contact_box(a.grids[m], P.pos, P.q, tbox + 2 * e);
             }
         }
         const float4* mycache = cache + lrope * nsdf * kPoseF4;
+        const float4* mytbox = (SURF == SURF_MESHES) ? tbox + lrope * nsdf * 2 : nullptr;
 
         // ---- inertial prediction and initial guess
         f3 dx, y;
@@ -206,7 +216,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
             const bool touched =
-                position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2, btab);
+                position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2, btab, mytbox);
             if constexpr (ROPE) {
                 if (ncol > 0) {
                     // even candidates join the own terms, odd ones a second partial added after
@@ -257,7 +267,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             if (SURF != SURF_NONE && a.forces_on) {
                 f3 fv = zero3();
                 sym3 Hs = sym_zero();
-                surfaces<SURF>(a, mycache, cand, p, dx, c.kc, h, fv, Hs, wrow, &fv, btab);
+                surfaces<SURF>(a, mycache, cand, p, dx, c.kc, h, fv, Hs, wrow, &fv, btab, mytbox);
                 facc += fv;
             }
         }
@@ -303,7 +313,7 @@ template <int BLOCK, bool ROPE>
 static cudaError_t launch_frame_r(const FrameArgs& a, int num_bins, cudaStream_t s) {
     if (a.num_sdf > 0)
         return launch_frame_t<BLOCK, SURF_MESHES, ROPE>(
-            a, num_bins, (size_t)2 * a.pose_cache * kPoseF4 * sizeof(float4) + (size_t)a.sdf_btab * sizeof(float), s);
+            a, num_bins, (size_t)2 * a.pose_cache * (kPoseF4 + 2) * sizeof(float4) + (size_t)a.sdf_btab * sizeof(float), s);
     if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES, ROPE>(a, num_bins, 0, s);
     return launch_frame_t<BLOCK, SURF_NONE, ROPE>(a, num_bins, 0, s);
 }

@@ -104,9 +104,12 @@ __device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, 
 // contact.cuh:141-163; with `wr` != nullptr it is the readout (contact.cuh:172-204): mesh
 // forces are added to *facc and their wrenches to wr[m * 6 ...]. Returns whether any contact
 // term was added (H then stops being a multiple of the identity).
+// `tbox` (persistent kernel): per mesh the world AABB of its contact box (GridDesc::tlo/thi at
+// this substep's pose), an exact early out before the probe is rotated into the lattice.
 template <int SURF>
 __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d, float k,
-                                         float h, f3& f, sym3& H, float* wr, f3* facc, const float* btab = nullptr) {
+                                         float h, f3& f, sym3& H, float* wr, f3* facc, const float* btab = nullptr,
+                                         const float4* tbox = nullptr) {
     bool touched = false;
     for (int pl = 0; pl < a.num_planes; pl++) {
         const float4 P = a.planes[pl];
@@ -119,6 +122,11 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
     if constexpr (SURF == SURF_MESHES) {
     for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
         const int m = __ffsll((long long)mm) - 1;
+        if (tbox) {
+            const float4 lo = tbox[2 * m], hi = tbox[2 * m + 1];
+            const f3 pr = pos + d;
+            if (!(pr.x >= lo.x && pr.x <= hi.x && pr.y >= lo.y && pr.y <= hi.y && pr.z >= lo.z && pr.z <= hi.z)) continue;
+        }
         const PoseV P = load_pose(cache + m * kPoseF4);
         f3 n, dRel;
         float gap;
@@ -141,6 +149,20 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
     }
     }
     return touched;
+}
+
+// World AABB of a lattice's contact box under the pose (pos, q); an empty box when the lattice
+// can never reach the contact radius.
+__device__ __forceinline__ void contact_box(const GridDesc& g, f3 pos, float4 q, float4* out) {
+    if (g.never) {
+        out[0] = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        out[1] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        return;
+    }
+    f3 lo, hi;
+    world_box(mk3(g.tlo[0], g.tlo[1], g.tlo[2]), mk3(g.thi[0], g.thi[1], g.thi[2]), pos, q, lo, hi);
+    out[0] = f4(lo, 0.f);
+    out[1] = f4(hi, 0.f);
 }
 
 // Inertial target y and initial guess dx from the substep's start velocity, iteration.cu:34-68.
@@ -177,12 +199,13 @@ __device__ __forceinline__ VConst vertex_constants(const FrameArgs& a, float im,
 template <int SURF>
 __device__ __forceinline__ bool position_terms(const FrameArgs& a, const float4* cache, uint64_t cand, const VConst& c,
                                                bool hasNext, f3 p, f3 p1, f3 dx, f3 p1dx, f3 y, float4 q, float damp,
-                                               f3& f, sym3& H, f3& f2, sym3& H2, const float* btab = nullptr) {
+                                               f3& f, sym3& H, f3& f2, sym3& H2, const float* btab = nullptr,
+                                               const float4* tbox = nullptr) {
     f = (y - dx) * c.fm;
     H = sym_diag(c.Hd);
     bool touched = false;
     if (SURF != SURF_NONE && c.im != 0.f)
-        touched = surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr, btab);
+        touched = surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr, btab, tbox);
     f2 = zero3();
     H2 = sym_zero();
     if (hasNext) {

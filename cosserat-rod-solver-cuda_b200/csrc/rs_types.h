@@ -60,6 +60,10 @@ struct GridDesc {
     float muS, muK;
     int by, bz;
     int bcount, boff;  // blocks of this lattice, and its offset in the CTA-staged bound tables
+    // object-frame box of the blocks where contact at the current radius is possible (their
+    // bound <= radius + 1e-5), padded by 1e-4; never = 1 when no block qualifies
+    float tlo[3], thi[3];
+    int never;
 };
 
 // Kinematic pose of (env, mesh) at the end of a substep: position, rotor (x, y, z, w),
