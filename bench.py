@@ -359,6 +359,20 @@ def run_config3(args):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x, dist, device):
+    """The maximum of a per-rank scalar over every rank: whole-job times are the slowest rank's."""
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, seconds):
+    """Whole-job throughput: every rank processes its own shard of ropes (weak scaling)."""
+    return world * units_per_rank / seconds
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -416,12 +430,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     total_ms = float(sum(frame_ms))
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, dist, dev)
         dist.barrier()
     vs_per_rank = N_ROPES * V * S * args.steps
-    value = world * vs_per_rank / (total_ms * 1e-3)
+    value = job_rate(world, vs_per_rank, total_ms * 1e-3)
 
     # ---- end-to-end leg: host inputs in, host positions out, through the public API
     if args.no_e2e:
@@ -444,10 +456,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * vs_per_rank / e2e_s if not args.no_e2e else None
+        e2e_s = max_over_ranks(e2e_s, dist, dev)
+    e2e_value = job_rate(world, vs_per_rank, e2e_s) if not args.no_e2e else None
     h2d = 3 * N_ROPES * 3 * 4
     d2h = N_ROPES * V * 3 * 4
 
