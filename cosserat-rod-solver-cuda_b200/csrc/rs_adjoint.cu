@@ -45,11 +45,13 @@ __device__ __forceinline__ float4 tangent_vjp(float4 q, f3 tb) {
                        2.f * (-q.z * tb.x + q.w * tb.y + q.x * tb.z), 2.f * (q.w * tb.x + q.z * tb.y - q.y * tb.z));
 }
 
-// Plane contact (contact.cuh:27-46) reversed, given F̄ and the contractions n·H̄n and tr H̄:
-// adds to d̄, returns the adjoints of the gap and of the penalty stiffness k.
+// Contact law (contact.cuh:27-46) reversed: f += n N - ut kt, H += k nnᵀ - kt (nnᵀ - I), with
+// N = -k gap and ut = d - n (n.d). Given F̄ and H̄ = -e δᵀ: adds to d̄, returns the adjoints of
+// the gap, of the penalty stiffness k and of the normal n.
 __device__ __forceinline__ void surface_contact_bwd(f3 n, float gap, f3 d, float k, float h, float muS, float muK,
-                                                    float eps, f3 Fb, float nHn, float trHb, f3& db, float& gapb,
-                                                    float& kb) {
+                                                    float eps, f3 Fb, f3 e, f3 del, f3& db, float& gapb, float& kb,
+                                                    f3& nb) {
+    const float nHn = -dot(n, e) * dot(n, del), trHb = -dot(e, del);
     const float N = -k * gap;
     const f3 ut = d - n * dot(n, d);
     const float ul = len(ut);
@@ -76,6 +78,65 @@ __device__ __forceinline__ void surface_contact_bwd(f3 n, float gap, f3 d, float
     db += utb - n * dot(n, utb);
     kb += -gap * Nb;
     gapb = -k * Nb;
+    // normal: f's n N, ut's -n (n.d), H's (k - kt) nnᵀ with (H̄ + H̄ᵀ) n = -e (δ.n) - δ (e.n)
+    nb = Fb * N - utb * dot(n, d) - d * dot(utb, n) + (e * (-dot(del, n)) - del * dot(e, n)) * (k - kt);
+}
+
+// Trilinear sample (contact.cuh:57-76) with the field's Hessian in lattice-fraction coordinates
+// (zero diagonal): hxy, hxz, hyz of d²φ / df_a df_b.
+__device__ __forceinline__ bool sdf_sample_hess(const GridDesc& g, f3 p, float& phi, f3& grad, float& hxy, float& hxz,
+                                                float& hyz) {
+    if (!sdf_sample(g, p, phi, grad)) return false;
+    const f3 o = mk3(g.ox, g.oy, g.oz);
+    const f3 u = (p - o) * g.invH;
+    const int i = (int)u.x, j = (int)u.y, k = (int)u.z;
+    const f3 fr = (p - (o + mk3(float(i), float(j), float(k)) * g.h)) * g.invH;
+    const float fx = fminf(fmaxf(fr.x, 0.f), 1.f), fy = fminf(fmaxf(fr.y, 0.f), 1.f), fz = fminf(fmaxf(fr.z, 0.f), 1.f);
+    const int sy = g.nz, sx = g.ny * g.nz;
+    const float* c = g.v + (size_t)i * sx + (size_t)j * sy + k;
+    const float c000 = __ldg(c), c001 = __ldg(c + 1), c010 = __ldg(c + sy), c011 = __ldg(c + sy + 1);
+    const float c100 = __ldg(c + sx), c101 = __ldg(c + sx + 1), c110 = __ldg(c + sx + sy), c111 = __ldg(c + sx + sy + 1);
+    const float dx00 = c100 - c000, dx01 = c101 - c001, dx10 = c110 - c010, dx11 = c111 - c011;
+    const float D = (dx11 - dx01) - (dx10 - dx00);
+    hxy = (dx10 - dx00) + fz * D;
+    hxz = (dx01 - dx00) + fy * D;
+    hyz = ((c011 - c001) + fx * (dx11 - dx01)) - ((c010 - c000) + fx * (dx10 - dx00));
+    return true;
+}
+
+// Mesh contacts of one vertex reversed (static poses; contact.cuh:94-110, then the contact law):
+// p_o = R(q)ᵀ((x - P) + d), gap = φ(p_o) - r, n = R(q) ∇φ / |∇φ|. Adds to d̄ and x̄, returns the
+// adjoint of the penalty stiffness.
+__device__ __forceinline__ float mesh_contact_bwd(const FrameArgs& a, const float4* cache, uint64_t cand, f3 x, f3 d,
+                                                  float kc, float h, f3 Fb, f3 e, f3 del, f3& db, f3& xb) {
+    float kbs = 0.f;
+    for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
+        const int m = __ffsll((long long)mm) - 1;
+        const PoseV P = load_pose(cache + m * kPoseF4);
+        const GridDesc& G = a.grids[m];
+        const f3 po = qrot(qconj(P.q), (x - P.pos) + d);
+        float phi, hxy, hxz, hyz;
+        f3 gr;
+        if (!sdf_sample_hess(G, po, phi, gr, hxy, hxz, hyz)) continue;
+        const float gap = phi - a.c_radius;
+        if (gap >= 0.f) continue;
+        const float gl = len(gr);
+        if (!(gl > 0.f)) continue;
+        const f3 gh = gr / gl;
+        const f3 nrm = qrot(P.q, gh);
+        float gapb, kb;
+        f3 nb;
+        surface_contact_bwd(nrm, gap, d, kc, h, G.muS, G.muK, a.c_vslip, Fb, e, del, db, gapb, kb, nb);
+        kbs += kb;
+        const f3 ghb = qrot(qconj(P.q), nb);
+        const f3 grb = (ghb - gh * dot(gh, ghb)) / gl;
+        const float inv2 = G.invH * G.invH;
+        const f3 pob = gr * gapb + mk3(hxy * grb.y + hxz * grb.z, hxy * grb.x + hyz * grb.z, hxz * grb.x + hyz * grb.y) * inv2;
+        const f3 wv = qrot(P.q, pob);
+        xb += wv;
+        db += wv;
+    }
+    return kbs;
 }
 
 // Shared memory of the adjoint kernel, in float4 units (BLOCK = bin size, I = iterations):
@@ -96,18 +157,28 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
     float4* EF = EC + BLOCK;
     float4* LD = EF + BLOCK;
     float4* LQ = LD + (size_t)(I + 1) * BLOCK;
+    float4* PC = LQ + (size_t)(I + 1) * BLOCK;  // static mesh poses of the bin's ropes [rope][mesh]
 
     const Bin bin = a.bins[blockIdx.x];
     const int t = threadIdx.x;
     const bool act = t < bin.vcount;
     const int dv = bin.vstart + t;
     uint32_t fl = 0;
-    int uidx = 0, env = 0;
+    int uidx = 0, env = 0, lrope = 0;
     float im = 0.f, lr = 1.f, ks = 0.f;
     QR[t] = make_float4(0.f, 0.f, 0.f, 1.f);
+    const int nsdf = (SURF == SURF_MESHES) ? a.num_sdf : 0;
+    if constexpr (SURF == SURF_MESHES) {
+        for (int e = t; e < bin.rcount * nsdf; e += BLOCK) {
+            const int r = e / nsdf, m = e % nsdf;
+            const float4* src = reinterpret_cast<const float4*>(a.poses + (size_t)a.ropes[bin.rstart + r].user * kMaxSdf + m);
+#pragma unroll
+            for (int k = 0; k < kPoseF4; k++) PC[e * kPoseF4 + k] = src[k];
+        }
+    }
     if (act) {
         const int4 tp = a.topo[dv];
-        fl = (uint32_t)tp.x; uidx = tp.z; env = tp.w;
+        fl = (uint32_t)tp.x; lrope = tp.y; uidx = tp.z; env = tp.w;
         im = a.pos[dv].w; lr = a.vel[dv].w; ks = a.lvel[dv].w;
         QR[t] = a.qrest[dv];
     }
@@ -141,10 +212,14 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
         // ---- the substep's start state (after its root program) from the tape
         f3 p = zero3(), v = zero3(), lvin = zero3();
         float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
+        uint64_t cand = 0ull;  // the forward's broad-phase mask of this substep (tape .w lanes)
         if (act) {
             const float4* tp = g.tape + (size_t)s * 4 * n + uidx;
-            p = xyz(tp[0]); v = xyz(tp[n]); lvin = xyz(tp[2 * n]); q = tp[3 * n];
+            const float4 t0 = tp[0], t1 = tp[n];
+            p = xyz(t0); v = xyz(t1); lvin = xyz(tp[2 * n]); q = tp[3 * n];
+            cand = (uint64_t)(uint32_t)__float_as_int(t0.w) | ((uint64_t)(uint32_t)__float_as_int(t1.w) << 32);
         }
+        const float4* mycache = PC + (size_t)lrope * nsdf * kPoseF4;
         f3 dx, y;
         init_vertex(v, lvin, im, h, a.last_h, gv, g2, dx, y);
         X[t] = f4(p, 0.f);
@@ -158,7 +233,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
             f3 f, f2;
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(LD[(size_t)k * BLOCK + t + 1]) : zero3();
-            const bool touched = position_terms<SURF>(a, nullptr, 0ull, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            const bool touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
             EA[t] = f4(f2, H2.xx);
             EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
             EC[t].x = H2.yz;
@@ -293,14 +368,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                 bool touched = false;
                 if constexpr (SURF != SURF_NONE) {
                     f3 fdummy = zero3();
-                    for (int pl = 0; pl < a.num_planes; pl++) {
-                        const float4 P = a.planes[pl];
-                        const f3 nrm = mk3(P.x, P.y, P.z);
-                        const float gap = (dot(nrm, p) - P.w) + dot(nrm, dk) - a.c_radius;
-                        if (gap >= 0.f) continue;
-                        surface_contact(nrm, gap, dk, c.kc, h, a.c_mu_s, a.c_mu_k, a.c_vslip, fdummy, H);
-                        touched = true;
-                    }
+                    touched = surfaces<SURF>(a, mycache, cand, p, dk, c.kc, h, fdummy, H, nullptr, nullptr);
                 }
                 if (hasNext) {
                     const float dd = ks * c.invl * c.invl * (1.f + damp);
@@ -325,13 +393,16 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                         const float gap = (dot(nrm, p) - P.w) + dot(nrm, dk) - a.c_radius;
                         if (gap >= 0.f) continue;
                         float gapb, kb;
-                        surface_contact_bwd(nrm, gap, dk, c.kc, h, a.c_mu_s, a.c_mu_k, a.c_vslip, Fb,
-                                            -dot(nrm, e) * dot(nrm, del), trH, dn, gapb, kb);
+                        f3 nb;
+                        surface_contact_bwd(nrm, gap, dk, c.kc, h, a.c_mu_s, a.c_mu_k, a.c_vslip, Fb, e, del, dn, gapb,
+                                            kb, nb);
                         dn += nrm * gapb;
                         xb += nrm * gapb;
                         wsum += kb * (-c.kc / im);
                     }
                 }
+                if constexpr (SURF == SURF_MESHES)
+                    wsum += mesh_contact_bwd(a, mycache, cand, p, dk, c.kc, h, Fb, e, del, dn, xb) * (-c.kc / im);
                 wb += wsum;
             }
             // segment t's residual c = ((x1 - x) + (d1 - d)) / l - t(q), read before the barrier:
@@ -419,7 +490,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
 template <int BLOCK, int SURF>
 cudaError_t launch_adjoint_t(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
     auto k = adjoint_kernel<BLOCK, SURF>;
-    const size_t bytes = adjoint_smem_bytes(BLOCK, a.iters);
+    const size_t bytes = adjoint_smem_bytes(BLOCK, a.iters) +
+                         (SURF == SURF_MESHES ? (size_t)a.pose_cache * kPoseF4 * sizeof(float4) : 0);
     if (bytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         if (e != cudaSuccess) return e;
@@ -429,6 +501,7 @@ cudaError_t launch_adjoint_t(const FrameArgs& a, const AdjArgs& g, int num_bins,
 }
 template <int BLOCK>
 cudaError_t launch_adjoint_b(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
+    if (a.num_sdf > 0) return launch_adjoint_t<BLOCK, SURF_MESHES>(a, g, num_bins, s);
     if (a.num_planes > 0) return launch_adjoint_t<BLOCK, SURF_PLANES>(a, g, num_bins, s);
     return launch_adjoint_t<BLOCK, SURF_NONE>(a, g, num_bins, s);
 }

@@ -1190,7 +1190,7 @@ void Batch::step_program_taped(const float* p0, const float* v0, const float* p1
     if (!tape) throw std::invalid_argument("null tape");
     if (engine_ != 0) throw std::invalid_argument("a taped step runs the persistent engine only");
     if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
-    if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
+    if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     pending_tape_ = reinterpret_cast<float4*>(tape);
     try {
         step_program(p0, v0, p1, q0, q1, dt, substeps, false);
@@ -1210,7 +1210,7 @@ float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synch
     if (!roots_pinned()) throw std::invalid_argument("the program frame drives every rope's root");
     if (io.tape) {
         if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
-        if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
+        if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     }
     tune_before_frame();
     ensure_device();
@@ -1257,11 +1257,11 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
     if (io.p0 && (!io.v0 || !io.p1)) throw std::invalid_argument("a program frame needs p0, v0 and p1");
     if (io.q1 && !io.q0) throw std::invalid_argument("root_q_end requires root_q");
     if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
-    if (!grids_.empty()) throw std::invalid_argument("the adjoint does not differentiate mesh contact");
+    if (!grids_.empty() && (pending_set_ || sdf_moving_)) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     ensure_device();
     if (block_ > 512)
         throw std::invalid_argument("the adjoint runs bins of at most 512 vertices (ropes of at most 512 vertices)");
-    if (adjoint_smem_bytes(block_, num_itr) > 227 * 1024)
+    if (adjoint_smem_bytes(block_, num_itr) + (size_t)pose_cache_entries() * 5 * sizeof(float4) > 227 * 1024)
         throw std::invalid_argument("num_itr too large for the adjoint's shared memory at this bin size");
     grad_alloc(io.tape ? 0 : substeps);
     if (io.ea || io.ei || io.mass) {

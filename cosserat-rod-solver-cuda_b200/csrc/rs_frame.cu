@@ -152,8 +152,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         }
         if (a.tape && act) {  // differentiable frames: this substep's start state, caller order
             float4* tp = a.tape + (size_t)s * 4 * a.n + a.topo[dv].z;
-            tp[0] = f4(p, 0.f);
-            tp[a.n] = f4(v, 0.f);
+            tp[0] = f4(p, __int_as_float((int)(uint32_t)cand));  // broad-phase mask of this substep
+            tp[a.n] = f4(v, __int_as_float((int)(uint32_t)(cand >> 32)));
             tp[2 * (size_t)a.n] = sm.lv[t];
             tp[3 * (size_t)a.n] = q;
         }

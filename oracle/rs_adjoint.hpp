@@ -59,8 +59,8 @@ public:
     // program rows (zero when prog == nullptr: a free frame) and g.ks/rho/w have been ADDED to.
     // The Sim is left at the frame's end state. prog is [p0 (3R), v0 (3R), p1 (3R)].
     void frame_backward(const T* prog, bool has_q0, const float* q0, const float* q1, float dt, int S, FrameGrad<T>& g) {
-        if (s.ropeContact || !s.grids.empty())
-            throw std::invalid_argument("oracle adjoint: rope-rope and mesh contact are not differentiated");
+        if (s.ropeContact) throw std::invalid_argument("oracle adjoint: rope-rope contact is not differentiated");
+        if (s.pendingSet) throw std::invalid_argument("oracle adjoint: only static meshes are differentiated");
         const int n = s.n;
         s.sdf_begin_step();
         s.prepare(T(dt / (float)S));
@@ -89,16 +89,24 @@ private:
     struct State {
         std::vector<V3<T>> pos, vel, lastVel;
         std::vector<Q4<T>> q;
-        void save(const Sim<T>& m) { pos = m.pos; vel = m.vel; lastVel = m.lastVel; q = m.q; }
-        void load(Sim<T>& m) const { m.pos = pos; m.vel = vel; m.lastVel = lastVel; m.q = q; }
+        std::vector<int> numCand;              // broad-phase candidate lists of the substep
+        std::vector<std::vector<int>> cand;
+        void save(const Sim<T>& m) {
+            pos = m.pos; vel = m.vel; lastVel = m.lastVel; q = m.q; numCand = m.numCand; cand = m.cand;
+        }
+        void load(Sim<T>& m) const {
+            m.pos = pos; m.vel = vel; m.lastVel = lastVel; m.q = q; m.numCand = numCand; m.cand = cand;
+        }
     };
 
     bool has(int i, uint32_t f) const { return (s.flags[i] & f) != 0; }
 
-    // Plane contact reverse (contact.cuh:27-46) given F̄ and the two contractions of H̄ the
-    // contact Hessian k nnᵀ - kt (nnᵀ - I) needs: nᵀH̄n and tr H̄.
-    void surface_contact_bwd(const V3<T>& nrm, T gap, const V3<T>& d, T k, T muS, T muK, const V3<T>& Fb, T nHn, T trHb,
-                             V3<T>& db, T& gapb, T& kb) const {
+    // Contact reverse (contact.cuh:27-46): f += n N - ut kt, H += k nnᵀ - kt (nnᵀ - I), with
+    // N = -k gap and ut = d - n (n.d). Given F̄ and H̄ = -e δᵀ, adds to d̄ and returns the adjoints
+    // of the gap, of the penalty stiffness k and of the normal n.
+    void surface_contact_bwd(const V3<T>& nrm, T gap, const V3<T>& d, T k, T muS, T muK, const V3<T>& Fb,
+                             const V3<T>& e, const V3<T>& delta, V3<T>& db, T& gapb, T& kb, V3<T>& nb) const {
+        const T nHn = -dot(nrm, e) * dot(nrm, delta), trHb = -dot(e, delta);
         const T eps = s.cVSlip, h = s.h;
         const T N = -k * gap;
         const V3<T> ut = d - nrm * dot(nrm, d);
@@ -127,6 +135,73 @@ private:
         db += utb - nrm * dot(nrm, utb);
         kb += -gap * Nb;
         gapb = -k * Nb;
+        // normal: f's n N, ut's -n (n.d), H's (k - kt) nnᵀ with (H̄ + H̄ᵀ) n = -e (δ.n) - δ (e.n)
+        nb = Fb * N - utb * dot(nrm, d) - d * dot(utb, nrm) +
+             (e * (-dot(delta, nrm)) - delta * dot(e, nrm)) * (k - kt);
+    }
+    // Trilinear sample with the field's Hessian in lattice-fraction coordinates (zero diagonal):
+    // hxy, hxz, hyz of d²φ/df_a df_b, contact.cuh:57-76.
+    static bool sdf_sample_hess(const typename Sim<T>::Grid& g, const V3<T>& p, T& phi, V3<T>& grad, T& hxy, T& hxz,
+                                T& hyz) {
+        if (!Sim<T>::sdf_sample(g, p, phi, grad)) return false;
+        const V3<T> u = (p - g.origin) * g.inv;
+        const int i = (int)u.x, j = (int)u.y, k = (int)u.z;
+        const V3<T> fr = (p - (g.origin + V3<T>(T(i), T(j), T(k)) * g.sp)) * g.inv;
+        const T fy = std::min(std::max(fr.y, T(0)), T(1)), fz = std::min(std::max(fr.z, T(0)), T(1));
+        const T fx = std::min(std::max(fr.x, T(0)), T(1));
+        const size_t sy = (size_t)g.nz, sx = (size_t)g.ny * g.nz;
+        const float* c = g.v.data() + (size_t)i * sx + (size_t)j * sy + k;
+        const T c000 = c[0], c001 = c[1], c010 = c[sy], c011 = c[sy + 1];
+        const T c100 = c[sx], c101 = c[sx + 1], c110 = c[sx + sy], c111 = c[sx + sy + 1];
+        const T dx00 = c100 - c000, dx01 = c101 - c001, dx10 = c110 - c010, dx11 = c111 - c011;
+        const T D = (dx11 - dx01) - (dx10 - dx00);
+        hxy = (dx10 - dx00) + fz * D;
+        hxz = (dx01 - dx00) + fy * D;
+        const T dy0 = (c010 - c000) + fx * (dx10 - dx00), dy1 = (c011 - c001) + fx * (dx11 - dx01);
+        hyz = dy1 - dy0;
+        return true;
+    }
+    // Mesh contact of vertex i reversed (contact.cuh:94-110 then the contact law): adds to d̄, x̄
+    // and returns the stiffness adjoint. p_o = R(q)ᵀ((x - P) + d); n = R(q) ∇φ/|∇φ|; gap = φ - r;
+    // dRel = d - h (v_P + ω × (x - P)) for a moving mesh.
+    T mesh_contact_bwd(int i, const V3<T>& x, const V3<T>& d, T kc, const V3<T>& Fb, const V3<T>& e, const V3<T>& delta,
+                       V3<T>& db, V3<T>& xb) const {
+        T kbs = 0;
+        const int cnt = s.cand_count(i);
+        for (int c = 0; c < cnt; c++) {
+            const int m = s.cand_at(i, c);
+            const auto& P = s.poses[(size_t)s.env[i] * kMaxSdf + m];
+            const auto& G = s.grids[m];
+            const V3<T> po = qrot(P.q.inv(), (x - P.pos) + d);
+            T phi, hxy, hxz, hyz;
+            V3<T> gr;
+            if (!sdf_sample_hess(G, po, phi, gr, hxy, hxz, hyz)) continue;
+            const T gap = phi - s.cR;
+            if (gap >= 0) continue;
+            const T gl = len(gr);
+            if (!(gl > 0)) continue;
+            const V3<T> gh = gr / gl;
+            const V3<T> nrm = qrot(P.q, gh);
+            V3<T> dRel = d;
+            if (s.sdfMoving) dRel -= (P.vel + cross(P.omega, x - P.pos)) * s.h;
+            V3<T> dRelb, nb;
+            T gapb, kb = 0;
+            surface_contact_bwd(nrm, gap, dRel, kc, G.muS, G.muK, Fb, e, delta, dRelb, gapb, kb, nb);
+            kbs += kb;
+            db += dRelb;
+            if (s.sdfMoving) xb += cross(P.omega, dRelb) * s.h;
+            // n = R(q) ĝ: the object-frame gradient's adjoint
+            const V3<T> ghb = qrot(P.q.inv(), nb);
+            const V3<T> grb = (ghb - gh * dot(gh, ghb)) / gl;
+            // φ and ∇φ (= G inv) at p_o: d φ/dp_o = ∇φ, d ∇φ/dp_o = inv² Hf
+            const T inv2 = G.inv * G.inv;
+            const V3<T> pob = gr * gapb + V3<T>(hxy * grb.y + hxz * grb.z, hxy * grb.x + hyz * grb.z,
+                                                 hxz * grb.x + hyz * grb.y) * inv2;
+            const V3<T> wb = qrot(P.q, pob);
+            xb += wb;
+            db += wb;
+        }
+        return kbs;
     }
 
     void substep_backward(int sub, int S, float dtf, const T* prog, bool q0set, const float* q0, const float* q1,
@@ -315,16 +390,11 @@ private:
             if (w == 0) continue;
             const T a = T(1) / (w * h * h);
             S3<T> H(a);
-            const bool surf = s.numPlanes > 0;
+            const bool surf = s.numPlanes > 0 || !s.grids.empty();
             const T kap = s.cKappa / h, kc = kap * kap / w;
             if (surf) {
                 V3<T> fdummy;
-                for (int pl = 0; pl < s.numPlanes; pl++) {
-                    const V3<T> nrm(s.planes[pl][0], s.planes[pl][1], s.planes[pl][2]);
-                    const T gap = (dot(nrm, x[i]) - s.planes[pl][3]) + dot(nrm, dk[i]) - s.cR;
-                    if (gap >= 0) continue;
-                    s.surface_contact(nrm, gap, dk[i], kc, s.cMuS, s.cMuK, fdummy, H);
-                }
+                s.surfaces_at(i, x[i], dk[i], kc, fdummy, H);
             }
             if (has(i, F_NEXT)) H.add_diag(s.kStretch[i] / s.lRest[i] / s.lRest[i] * (T(1) + damp));
             if (has(i, F_PREV)) H.add_diag(s.kStretch[i - 1] / s.lRest[i - 1] / s.lRest[i - 1] * (T(1) + damp));
@@ -340,13 +410,14 @@ private:
                     const V3<T> nrm(s.planes[pl][0], s.planes[pl][1], s.planes[pl][2]);
                     const T gap = (dot(nrm, x[i]) - s.planes[pl][3]) + dot(nrm, dk[i]) - s.cR;
                     if (gap >= 0) continue;
-                    const T nHn = -dot(nrm, e) * dot(nrm, delta);
                     T gapb, kb;
-                    surface_contact_bwd(nrm, gap, dk[i], kc, s.cMuS, s.cMuK, Fb[i], nHn, trH[i], dnew[i], gapb, kb);
+                    V3<T> nb;
+                    surface_contact_bwd(nrm, gap, dk[i], kc, s.cMuS, s.cMuK, Fb[i], e, delta, dnew[i], gapb, kb, nb);
                     dnew[i] += nrm * gapb;
                     xb[i] += nrm * gapb;
                     wb += kb * (-kc / w);
                 }
+                if (!s.grids.empty()) wb += mesh_contact_bwd(i, x[i], dk[i], kc, Fb[i], e, delta, dnew[i], xb[i]) * (-kc / w);
             }
             g.w[i] += wb;
         }

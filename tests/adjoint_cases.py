@@ -17,9 +17,25 @@ import ropesim_oracle as ro
 MATERIALS = {"c1": (0.03, 0.1, 500.0, 1e-4), "c2": (0.02, 0.117, 11473.0, 4.48e-3)}
 
 
+def mesh_setup(pos):
+    """A static mesh under every rope's tip: a 0.2 x 0.2 x 0.1 m box lattice (64^3, edges rounded
+    by 1 cm), its flat top 2 mm above the tip (the tip sits inside the 5 mm contact band, so the
+    contact stays on, as with the plane scenes), rotated 0.6 rad about z. Returns (lattice args,
+    positions [R, 3], rotors [R, 4])."""
+    from ropesim import sdf
+
+    R = pos.shape[0]
+    g = sdf.from_function(sdf.sdf_box([0.1, 0.1, 0.05], round=0.01), [-0.14] * 3, [0.14] * 3, 0.28 / 63)
+    tips = pos[:, -1].astype(np.float64)
+    mp = np.stack([tips[r] + np.array([0.01 * ((r % 3) - 1), 0.0, 0.002 - 0.05]) for r in range(R)]).astype(np.float32)
+    quat = np.tile(np.array([0, 0, np.sin(0.3), np.cos(0.3)], np.float32), (R, 1))
+    return g.as_args(), mp, quat
+
+
 def scene(R=8, V=16, seed=0, plane=True, damping=0.0, drag_quad=0.0, num_itr=8, precision="f64", material="c2",
-          clearance=0.004):
-    """R hanging ropes of V vertices, tips `clearance` above a plane at z = 0 (when `plane`)."""
+          clearance=0.004, mesh=False):
+    """R hanging ropes of V vertices, tips `clearance` above a plane at z = 0 (when `plane`), or
+    resting on a static mesh (when `mesh`, see mesh_setup)."""
     seg, density, ea, ei = MATERIALS[material]
     rng = np.random.default_rng(seed)
     pos = np.zeros((R, V, 3), np.float32)
@@ -36,6 +52,10 @@ def scene(R=8, V=16, seed=0, plane=True, damping=0.0, drag_quad=0.0, num_itr=8, 
     b.drag_quad_t = 0.5 * drag_quad
     if plane:
         b.set_planes([[0.0, 0.0, 1.0, 0.0]], radius=0.00635, mu_s=0.5, mu_k=0.3)
+    if mesh:  # frictionless: with friction the FP32 gradient of this resting contact is ill-conditioned
+        args, mp, quat = mesh_setup(pos)
+        b.set_contact(0.005, mu_s=0.0, mu_k=0.0)
+        b.add_mesh(*args, pos=mp, quat=quat, mu_s=0.0, mu_k=0.0)
     return b, pos
 
 

@@ -151,3 +151,73 @@ def test_oracle_adjoint_matches_finite_differences():
         ad = float((g[name] * u.reshape(g[name].shape)).sum())
         scale = np.linalg.norm(g[name]) * np.linalg.norm(u)  # bound of the directional derivative
         assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-7 * scale + 1e-14, (name, ad, fd, scale)
+
+
+def test_oracle_adjoint_with_mesh_contact_matches_finite_differences():
+    """Mesh (SDF) contact differentiated: three config-1 ropes whose tips rest on a static
+    r = 0.3 m sphere lattice (64^3), rotated about z; contact carries force during the frames."""
+    from ropesim import sdf
+
+    R, V, I, S, dt, F = 3, 8, 4, 20, 1 / 300, 2
+    b, pos = ac.scene(R=R, V=V, seed=3, plane=False, material="c1", num_itr=I, clearance=0.0)
+    g = sdf.from_function(sdf.sdf_sphere(0.3), [-0.32] * 3, [0.32] * 3, 0.64 / 63)
+    b.set_contact(0.005, mu_s=0.5, mu_k=0.3)
+    tips = pos[:, -1].astype(np.float64)
+    mp = np.stack([tips[r] + np.array([0.0, 0.002 * (r - 1), -0.3045]) for r in range(R)]).astype(np.float32)
+    quat = np.tile(np.array([0, 0, np.sin(0.3), np.cos(0.3)], np.float32), (R, 1))
+    b.add_mesh(*g.as_args(), pos=mp, quat=quat, mu_s=0.5, mu_k=0.3)
+    s = b._s
+    progs = ac.programs(pos, F + 1, v_std=0.02, p_std=0.002)
+    s.step_program_rows(np.concatenate([a[0].ravel() for a in progs]).astype(np.float64), dt, S)
+    progs = [a[1:] for a in progs]
+    tgt = ac.targets(pos, F)
+    st0, par0 = s.get_state(), s.get_params()
+    wr = np.random.default_rng(7)
+    w_end = (1e-2 * wr.standard_normal((R * V, 3)), 1e-3 * wr.standard_normal((R * V, 3)))
+    L0, gr = ac.oracle_loss_and_grad(b, progs, tgt, dt, S, V, w_end=w_end)
+
+    def loss(progs_, st_, par_, forces=False):
+        s.set_state(*st_)
+        s.set_params(*par_)
+        s.enable_forces(forces)
+        P0, V0, P1 = progs_
+        val, fsum = 0.0, 0.0
+        for f in range(F):
+            s.step_program_rows(np.concatenate([P0[f].ravel(), V0[f].ravel(), P1[f].ravel()]).astype(np.float64), dt, S)
+            x = s.get_state()[0].reshape(R, V, 3)
+            val += ((x[:, -1] - tgt[f]) ** 2).sum(-1).mean()
+            if forces:
+                fsum += float(np.linalg.norm(s.contact_forces(), axis=1).sum())
+        s.enable_forces(False)
+        xF, vF = s.get_state()[:2]
+        return (val + float((w_end[0] * xF).sum() + (w_end[1] * vF).sum())), fsum
+
+    assert loss(progs, st0, par0, forces=True)[1] > 0.1  # the meshes push on the ropes
+    rng = np.random.default_rng(11)
+    l = s.rest_lengths()
+    w = par0[2]
+    free = w != 0
+    ea0 = par0[0] / l
+    m0 = np.where(free, 1 / np.where(free, w, 1), 0)
+    seg = np.ones(R * V, bool)
+    seg[V - 1::V] = False
+    cases = []
+    for k, name in enumerate(("g_p0", "g_v0", "g_p1")):
+        u = rng.standard_normal(progs[k].shape)
+        cases.append((name, u, lambda e, u=u, k=k: loss([p + (e * u if j == k else 0) for j, p in enumerate(progs)], st0, par0)[0], 1e-6))
+    for k, name, eps in ((0, "g_pos", 1e-6), (1, "g_vel", 1e-4), (3, "g_q", 1e-4)):
+        u = rng.standard_normal(st0[k].shape)
+        if name == "g_pos":
+            u[::V] = 0
+        cases.append((name, u, lambda e, u=u, k=k: loss(progs, [a + e * u if j == k else a for j, a in enumerate(st0)], par0)[0], eps))
+    u = rng.standard_normal(R * V) * seg * ea0
+    cases.append(("g_ea", u, lambda e, u=u: loss(progs, st0, [(ea0 + e * u) * l, par0[1], w])[0], 1e-5))
+    u = rng.standard_normal(R * V) * free * m0
+    cases.append(("g_mass", u, lambda e, u=u: loss(progs, st0, [par0[0], par0[1], np.where(free, 1 / np.where(free, m0 + e * u, 1), 0)])[0], 1e-5))
+    for name, u, fn, eps in cases:
+        d1 = (fn(eps) - fn(-eps)) / (2 * eps)
+        d2 = (fn(eps / 2) - fn(-eps / 2)) / eps
+        fd = (4 * d2 - d1) / 3
+        ad = float((gr[name] * u.reshape(gr[name].shape)).sum())
+        scale = np.linalg.norm(gr[name]) * np.linalg.norm(u)
+        assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-7 * scale + 1e-14, (name, ad, fd, scale)

@@ -4,7 +4,12 @@ Workload: the differentiable configuration's check size, 8 ropes x 16 vertices o
 config-1 rope (3 cm segments, density 0.1, EA 500, EI 1e-4, 8 iterations), program roots,
 5 control frames x 100 substeps of 1/6000 s, loss = mean squared distance of the rope tips to
 a seeded target curve summed over frames. Gradients with respect to the root programs
-(p0, v0, p1 of every frame), EA, EI, per-vertex mass and the initial state.
+(p0, v0, p1 of every frame), EA, EI, per-vertex mass and the initial state. Scenes: free ropes,
+ropes resting on a plane, damped ropes with quadratic drag, ropes resting on a static SDF mesh
+(a box lattice whose flat top holds the tips in contact, frictionless: with mesh friction the
+FP32 and FP64 gradients of this resting contact already differ by 2e-3 .. 1e-2, so FP32 cannot
+be checked there; curved mesh contact with friction is checked against FP64 finite differences
+on the CPU, test_adjoint_oracle.py).
 
 The oracle adjoint is pinned on the CPU by FP64 finite differences and by FP64 torch autograd
 (test_adjoint_oracle.py); here the GPU's FP32 gradients are compared with it. Tolerance, per
@@ -33,10 +38,11 @@ SCENES = {
     "free": (dict(plane=False), dict(v_std=0.3, p_std=0.02)),
     "resting_on_plane": (dict(plane=True, clearance=-0.002), dict(v_std=0.05, p_std=0.01)),
     "damped_quadratic_drag": (dict(plane=False, damping=0.01, drag_quad=2.0), dict(v_std=0.3, p_std=0.02)),
+    "resting_on_mesh": (dict(plane=False, mesh=True, clearance=0.0), dict(v_std=0.05, p_std=0.01)),
 }
 
 
-def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clearance=None):
+def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clearance=None, mesh=False):
     import ropesim
 
     _, density, ea, ei = ac.MATERIALS[material]
@@ -48,6 +54,10 @@ def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clear
     b.drag_quad_t = 0.5 * drag_quad
     if plane:
         b.set_planes(np.array([[0.0, 0.0, 1.0, 0.0]], np.float32), radius=0.00635, mu_s=0.5, mu_k=0.3)
+    if mesh:
+        args, mp, quat = ac.mesh_setup(pos)
+        b.set_contact(0.005, mu_s=0.0, mu_k=0.0)
+        b.add_mesh(*args, pos=mp, quat=quat, mu_s=0.0, mu_k=0.0)
     return b
 
 
