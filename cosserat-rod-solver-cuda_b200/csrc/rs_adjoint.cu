@@ -139,13 +139,202 @@ __device__ __forceinline__ float mesh_contact_bwd(const FrameArgs& a, const floa
     return kbs;
 }
 
+// seg_closest (Common.h:327-345, with a0 = 0) reversed: given the adjoints of the returned
+// (u, v), adds those of a1 = A, b0 = B0, b1 = B1. Each clamp passes its adjoint inside [0, 1],
+// ends included; the fallback for parallel segments (a non-finite first v) is a constant.
+__device__ __forceinline__ void seg_closest_bwd(f3 A, f3 B0, f3 B1, float ub, float vb, f3& Ab, f3& B0b, f3& B1b) {
+    const f3 E = B1 - B0;
+    const float a = dot(A, A), b = dot(A, E), c = dot(E, E);
+    const float AB0 = dot(A, B0), EB0 = dot(E, B0);
+    const float Den = a * c - b * b, t0 = (b * AB0 - a * EB0) / Den;
+    const bool fin = isfinite(t0);
+    const float v0 = fin ? t0 : 0.5f;
+    const float v0c = fminf(fmaxf(v0, 0.f), 1.f);
+    const f3 Bv = lerp3(B0, B1, v0c);
+    const float tu = dot(Bv, A) / a;
+    const float u = fminf(fmaxf(tu, 0.f), 1.f);
+    const f3 Au = lerp3(zero3(), A, u) - B0;
+    const float tv = dot(Au, E) / c;
+    f3 Ea = zero3(), Aa = zero3(), B0a = zero3();  // adjoints in the (A, B0, E = B1 - B0) parametrisation
+    if (tv >= 0.f && tv <= 1.f) {
+        const float Nb = vb / c;
+        ub += Nb * dot(A, E);
+        Aa += E * (Nb * u);
+        B0a -= E * Nb;
+        Ea += Au * Nb + E * (-2.f * vb * tv / c);
+    }
+    if (tu >= 0.f && tu <= 1.f) {
+        const float Mb = ub / a;
+        const f3 Bvb = A * Mb;
+        B0a += Bvb;
+        Ea += Bvb * v0c;
+        Aa += Bv * Mb + A * (-2.f * ub * tu / a);
+        if (fin && v0 >= 0.f && v0 <= 1.f) {
+            const float t0b = dot(Bvb, E);
+            const float Numb = t0b / Den, Denb = -t0b * t0 / Den;
+            const float bb = Numb * AB0 - 2.f * b * Denb, aa = -Numb * EB0 + Denb * c, cc = Denb * a;
+            const float AB0b = Numb * b, EB0b = -Numb * a;
+            Aa += E * bb + A * (2.f * aa) + B0 * AB0b;
+            Ea += A * bb + E * (2.f * cc) + B0 * EB0b;
+            B0a += A * AB0b + E * EB0b;
+        }
+    }
+    Ab += Aa;
+    B1b += Ea;
+    B0b += B0a - Ea;
+}
+
+// One rope-rope candidate reversed (cosserat.cu:99-157). Segment (x0, x1) with iterates
+// (d0, d1) against segment (y0, y1) with iterates (e0, e1): the term adds f, H to the segment's
+// first vertex with weight wa = 1 - u and f2, H2 to its second with weight wb = u. Given F̄ and
+// H̄ = -e δᵀ of both (Fa, ea, la; Fc, ec, lc), adds the adjoints of the eight inputs. Barrier:
+// s = (|n| - 2r) / b clamped below at 1e-3, force ff and stiffness dH of the log barrier; friction
+// f1 = min(kf, μ ff / |uu|) along the tangential slip uu.
+struct PairGrad {
+    f3 x0, x1, y0, y1, d0, d1, e0, e1;
+};
+__device__ __forceinline__ void collision_bwd(const FrameArgs& a, float damp, f3 x0, f3 x1, f3 y0, f3 y1, f3 d0, f3 d1,
+                                              f3 e0, f3 e1, f3 Fa, f3 ea, f3 la, f3 Fc, f3 ec, f3 lc, PairGrad& o) {
+    const f3 A = (x1 - x0) + (d1 - d0), B0 = (y0 - x0) + (e0 - d0), B1 = (y1 - x0) + (e1 - d0);
+    float u, v;
+    seg_closest(zero3(), A, B0, B1, u, v);
+    const f3 dpos = lerp3(x0, x1, u) - lerp3(y0, y1, v);
+    const f3 ddpos = lerp3(d0, d1, u) - lerp3(e0, e1, v);
+    const f3 raw = dpos + ddpos;
+    const float dist = len(raw);
+    if (!(dist > 0.f)) return;
+    const f3 nr = raw * (1.f / dist);
+    const float wb = u, wa = 1.f - u;
+    const float invb = 1.f / a.rc_barrier, kCol = a.rc_kcol * invb;
+    const float sr = (dist - 2.f * a.rc_radius) * invb;
+    if (sr > 1.f) return;
+    const float sd = fmaxf(sr, 1e-3f);
+    const float invd = 1.f / sd, logd = logf(sd);
+    const float dH = (-3.f + (2.f + invd) * invd - 2.f * logd) * kCol * invb;
+    const float ff = -(1.f - sd) * (sd - 1.f + 2.f * sd * logd) * invd * kCol;
+    const float Ga = dot(Fa, nr), Gc = dot(Fc, nr), nd0 = dot(nr, d0), nd1 = dot(nr, d1);
+    const float nHa = -dot(nr, ea) * dot(nr, la), nHc = -dot(nr, ec) * dot(nr, lc);
+    const float trA = -dot(ea, la), trC = -dot(ec, lc);
+    // (H̄ + H̄ᵀ) n for H̄ = -e δᵀ
+    const f3 symS = (ea * (-dot(la, nr)) - la * dot(ea, nr)) * (wa * wa) + (ec * (-dot(lc, nr)) - lc * dot(ec, nr)) * (wb * wb);
+    const float nHs = wa * wa * nHa + wb * wb * nHc, trS = wa * wa * trA + wb * wb * trC;
+    const float dp = 1.f + damp;
+    float ffb = Ga * wa + Gc * wb;
+    const float dHb = -damp * (Ga * wa * wa * nd0 + Gc * wb * wb * nd1) + dp * nHs;
+    float wab = Ga * ff - 2.f * damp * dH * wa * Ga * nd0 + 2.f * wa * dp * dH * nHa;
+    float wbb = Gc * ff - 2.f * damp * dH * wb * Gc * nd1 + 2.f * wb * dp * dH * nHc;
+    f3 nb = Fa * (ff * wa - damp * dH * wa * wa * nd0) + Fc * (ff * wb - damp * dH * wb * wb * nd1) +
+            d0 * (-damp * dH * wa * wa * Ga) + d1 * (-damp * dH * wb * wb * Gc) + symS * (dp * dH);
+    f3 d0b = nr * (-damp * dH * wa * wa * Ga), d1b = nr * (-damp * dH * wb * wb * Gc);
+    f3 ddb = zero3();  // adjoint of ddpos
+    const f3 uu = ddpos - nr * dot(nr, ddpos);
+    const float ul = len(uu);
+    if (ul > 0.f) {
+        const float ratio = a.rc_mu * ff / ul;
+        const float f1 = fminf(a.rc_kfric, ratio);
+        const f3 Fu = Fa * wa + Fc * wb;
+        const float f1b = -dot(uu, Fu) - (nHs - trS);
+        wab += -f1 * dot(uu, Fa) - 2.f * wa * f1 * (nHa - trA);
+        wbb += -f1 * dot(uu, Fc) - 2.f * wb * f1 * (nHc - trC);
+        nb -= symS * f1;
+        f3 uub = Fu * (-f1);
+        if (!(a.rc_kfric < ratio)) {  // f1 = μ ff / |uu|
+            ffb += f1b * a.rc_mu / ul;
+            uub += uu * (-f1b * ratio / (ul * ul));
+        }
+        ddb += uub - nr * dot(nr, uub);
+        nb -= uub * dot(nr, ddpos) + ddpos * dot(nr, uub);
+    }
+    float ub = wbb - wab, distb = 0.f;
+    if (sr >= 1e-3f) {
+        const float pm = 1.f - sd, qv = sd - 1.f + 2.f * sd * logd;
+        const float ffp = -kCol * ((-qv + pm * (3.f + 2.f * logd)) * invd - pm * qv * invd * invd);
+        const float dHp = -2.f * (invd * invd + invd * invd * invd + invd) * kCol * invb;
+        distb = (ffb * ffp + dHb * dHp) * invb;
+    }
+    const f3 rawb = (nb - nr * dot(nr, nb)) * (1.f / dist) + nr * distb;
+    ddb += rawb;
+    o.x0 += rawb * wa;
+    o.x1 += rawb * wb;
+    o.y0 -= rawb * (1.f - v);
+    o.y1 -= rawb * v;
+    ub += dot(rawb, x1 - x0) + dot(ddb, d1 - d0);
+    const float vbv = -dot(rawb, y1 - y0) - dot(ddb, e1 - e0);
+    d0b += ddb * wa;
+    d1b += ddb * wb;
+    o.e0 -= ddb * (1.f - v);
+    o.e1 -= ddb * v;
+    f3 Ab = zero3(), B0b = zero3(), B1b = zero3();
+    seg_closest_bwd(A, B0, B1, ub, vbv, Ab, B0b, B1b);
+    o.x1 += Ab;
+    d1b += Ab;
+    o.y0 += B0b;
+    o.e0 += B0b;
+    o.y1 += B1b;
+    o.e1 += B1b;
+    const f3 sb = Ab + B0b + B1b;
+    o.x0 -= sb;
+    d0b -= sb;
+    o.d0 += d0b;
+    o.d1 += d1b;
+}
+
+// Step limit of segment t reversed (recomputeStepLimitKernel, collision.cu:103-136): the limit is
+// the least of padding - detection radius (padding = scaled radius + |y|, y = v h + g h²) and
+// 0.45 x each listed candidate's distance at the substep start; its adjoint goes to the argument
+// that attained it (the first on ties, as the forward's running minimum). Returns the adjoint of
+// y (padding branch) and adds the position adjoints (candidate branch).
+__device__ __forceinline__ f3 step_limit_bwd(const FrameArgs& a, int dv, int ncol, const float4* X, f3 p, f3 p1, float pad,
+                                             f3 y, float limb, f3& xb0, f3& xb1, int& jo, f3& xbj0, f3& xbj1) {
+    jo = -1;
+    const f3 a1 = p1 - p;
+    float best = pad - a.det_radius;
+    int arg = -1;
+    for (int cc = 0; cc < ncol; cc++) {
+        const int j = a.cols[(size_t)cc * a.n + dv];
+        const float val = step_limit_of(p, a1, xyz(X[j]), xyz(X[j + 1]));
+        if (val < best) { best = val; arg = j; }
+    }
+    if (arg < 0) {
+        const float ly = len(y);
+        return ly > 0.f ? y * (limb / ly) : zero3();
+    }
+    const f3 b0 = xyz(X[arg]) - p, b1 = xyz(X[arg + 1]) - p;
+    float u, v;
+    seg_closest(zero3(), a1, b0, b1, u, v);
+    const f3 nn = a1 * u - lerp3(b0, b1, v);
+    const float l = len(nn);
+    if (!(l > 0.f)) return zero3();
+    const f3 nnb = nn * ((1.f - 0.1f) * 0.5f * limb / l);
+    f3 Ab = nnb * u, B0b = nnb * (-(1.f - v)), B1b = nnb * (-v);
+    seg_closest_bwd(a1, b0, b1, dot(nnb, a1), -dot(nnb, b1 - b0), Ab, B0b, B1b);
+    xb1 += Ab;
+    xb0 -= Ab + B0b + B1b;
+    jo = arg;
+    xbj0 = B0b;
+    xbj1 = B1b;
+    return zero3();
+}
+
+__device__ __forceinline__ void atomic_add3(float4* p, f3 v) {
+    atomicAdd(&p->x, v.x);
+    atomicAdd(&p->y, v.y);
+    atomicAdd(&p->z, v.z);
+}
+
 // Shared memory of the adjoint kernel, in float4 units (BLOCK = bin size, I = iterations):
 //   X, QR, KC, EA, EB, EC, EF   one slot per vertex each
-//   LD [I+1][BLOCK]   displacement iterates d^k (the solve's increment is d^{k+1} - d^k)
+//   with rope-rope contact, seven more: RP (padding, step limit, flags, limit adjoint handed to
+//   the previous vertex), EE (e = H⁻¹ z̄), HB0/HB1 (the segment's collision Hessian share of its
+//   second vertex), CD[2] (d̄ contributions of other segments' pairs, by iteration parity), CX
+//   (their x̄ contributions, per substep)
+//   LD [I+1][BLOCK]   displacement iterates d^k (.w: the step limit's scale, 1 when not limited)
 //   LQ [I+1][BLOCK]   frame iterates q^k
-// 64-thread bins at 8 iterations: 25.6 KB, 8 CTAs (16 warps) per SM with <= 128 registers.
-template <int BLOCK, int SURF>
-__global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const FrameArgs a, const AdjArgs g) {
+// 64-thread bins at 8 iterations: 25.6 KB, 8 CTAs per SM with <= 128 registers; with rope
+// contact 32.8 KB and 4 CTAs per SM with <= 255 registers (the pair reverse's working set).
+template <int BLOCK, int SURF, bool ROPE>
+__global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK) : 512 / BLOCK)
+    adjoint_kernel(const FrameArgs a, const AdjArgs g) {
     extern __shared__ float4 smem[];
     const int I = a.iters;
     float4* X = smem;
@@ -155,7 +344,13 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
     float4* EB = EA + BLOCK;
     float4* EC = EB + BLOCK;
     float4* EF = EC + BLOCK;
-    float4* LD = EF + BLOCK;
+    float4* RP = EF + BLOCK;
+    float4* EE = RP + BLOCK;
+    float4* HB0 = EE + BLOCK;
+    float4* HB1 = HB0 + BLOCK;
+    float4* CD = HB1 + BLOCK;  // [2][BLOCK]
+    float4* CX = CD + 2 * BLOCK;
+    float4* LD = ROPE ? CX + BLOCK : RP;
     float4* LQ = LD + (size_t)(I + 1) * BLOCK;
     float4* PC = LQ + (size_t)(I + 1) * BLOCK;  // static mesh poses of the bin's ropes [rope][mesh]
 
@@ -189,6 +384,17 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
     const float4 qr_own = QR[t];
     const float irho = hasNext ? 1.f / sqrtf(dot4(qr_own, qr_own)) : 0.f;  // 1 / |qRest| of segment t
     KC[t] = make_float4(ks, c.invl, im, irho);
+    // rope-rope contact group and rope of this vertex (CTA-local indices)
+    int g0 = 0, g1 = 0, r0 = 0, r1 = 0;
+    if constexpr (ROPE) {
+        CD[t] = zero4();
+        CD[BLOCK + t] = zero4();
+        CX[t] = zero4();
+        if (act) {
+            const int4 gr = a.grp[dv];
+            g0 = gr.x - bin.vstart; g1 = gr.y - bin.vstart; r0 = gr.z - bin.vstart; r1 = gr.w - bin.vstart;
+        }
+    }
     const float h = a.h, invH = 1.f / h;
     const float damp = a.damping / h;
     const f3 gv = mk3(a.gx, a.gy, a.gz);
@@ -223,17 +429,33 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
         f3 dx, y;
         init_vertex(v, lvin, im, h, a.last_h, gv, g2, dx, y);
         X[t] = f4(p, 0.f);
-        LD[t] = f4(dx, 0.f);
+        LD[t] = f4(dx, 1.f);
         LQ[t] = q;
+        if constexpr (ROPE) RP[t] = make_float4(a.sdet_radius + len(y), INFINITY, __int_as_float((int)fl), 0.f);
         __syncthreads();
         const f3 p1 = hasNext ? xyz(X[t + 1]) : zero3();
+
+        // ---- rope-rope detection and step limit (the frame kernel's, from the same inputs)
+        int ncol = 0;
+        float lim = INFINITY;
+        if constexpr (ROPE) {
+            if (hasNext) {
+                const int cnt = detect_group(
+                    a, t, dv, g0, g1, r0, r1, p, p1, [&](int j) { return RP[j].x; },
+                    [&](int j) { return __float_as_int(RP[j].z); }, [&](int j) { return xyz(X[j]); }, lim);
+                ncol = cnt < kMaxCols ? cnt : kMaxCols;
+            }
+            RP[t].y = lim;
+        }
 
         // ---- recompute the iterates (the frame kernel's arithmetic)
         for (int k = 0; k < I; k++) {
             f3 f, f2;
             sym3 H, H2;
-            const f3 p1dx = hasNext ? xyz(LD[(size_t)k * BLOCK + t + 1]) : zero3();
+            const float4* Dk = LD + (size_t)k * BLOCK;
+            const f3 p1dx = hasNext ? xyz(Dk[t + 1]) : zero3();
             const bool touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+            if constexpr (ROPE) collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, dx, p1dx, f, f2, H, H2);
             EA[t] = f4(f2, H2.xx);
             EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
             EC[t].x = H2.yz;
@@ -243,8 +465,10 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                 f += xyz(fa);
                 H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
             }
-            position_solve(dx, f, H, a.accel, im, !touched);
-            LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, 0.f);
+            float sc = 1.f;
+            if constexpr (ROPE) sc = position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, RP[t - 1].y) : lim);
+            else position_solve(dx, f, H, a.accel, im, !touched);
+            LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, sc);
             __syncthreads();
             if (upd) {
                 const f3 seg = (p1 - p) + (xyz(LD[(size_t)(k + 1) * BLOCK + t + 1]) - dx);
@@ -292,17 +516,19 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
             __syncthreads();
             if (hasNext) qb = add4(qb, EF[t + 1]);
         }
+        float msb = 0.f, msbp = 0.f;  // step-limit adjoints of this segment's limit and the previous one's
 
         // ---- iterations reversed
         for (int k = I - 1; k >= 0; k--) {
             const float4* Lq = LQ + (size_t)k * BLOCK;
+            const float4* Dk = LD + (size_t)k * BLOCK;
+            const float4* Dn = LD + (size_t)(k + 1) * BLOCK;
             // frame step k: q^{k+1}_t = normalize(vv b e1 + (|vv| + |b|) b)
             float4 own = qb, toL = zero4(), toR = zero4();
             f3 su = zero3();
             if (upd) {
                 own = zero4();
-                const float4* Ld = LD + (size_t)(k + 1) * BLOCK;
-                const f3 u = ((p1 - p) + (xyz(Ld[t + 1]) - xyz(Ld[t]))) * c.invl;
+                const f3 u = ((p1 - p) + (xyz(Dn[t + 1]) - xyz(Dn[t]))) * c.invl;
                 const f3 vv = u * (-2.f * ks);
                 const float4 q0 = Lq[t];
                 float4 b = zero4(), qp = zero4(), qn = zero4(), rp = zero4(), rn = zero4();
@@ -347,6 +573,16 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
             EA[t] = toL;
             EB[t] = toR;
             EC[t] = f4(su, 0.f);
+            // the segment's collision Hessians at d^k: its first vertex's share stays here, the
+            // second's goes to vertex t+1
+            sym3 HcA = sym_zero();
+            if constexpr (ROPE) {
+                f3 fd = zero3(), f2d = zero3();
+                sym3 HcB = sym_zero();
+                if (hasNext) collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, xyz(Dk[t]), xyz(Dk[t + 1]), fd, f2d, HcA, HcB);
+                HB0[t] = make_float4(HcB.xx, HcB.yy, HcB.zz, HcB.xy);
+                HB1[t] = make_float4(HcB.xz, HcB.yz, 0.f, 0.f);
+            }
             __syncthreads();
             qb = own;
             if (hasPrev) qb = add4(qb, EB[t - 1]);
@@ -357,11 +593,16 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                 db += dd;
                 xb += dd;
             }
+            if constexpr (ROPE) {  // pair contributions to d̄^{k+1} from the reverse of position step k+1
+                float4* cd = CD + ((k + 1) & 1) * BLOCK + t;
+                db += xyz(*cd);
+                *cd = zero4();
+            }
 
-            // position step k: d^{k+1}_t = d^k_t + a H_t^-1 F_t
-            const f3 dk = xyz(LD[(size_t)k * BLOCK + t]);
+            // position step k: d^{k+1}_t = limit(d^k_t + a H_t^-1 F_t)
+            const f3 dk = xyz(Dk[t]);
             f3 dn = db;
-            f3 Fb = zero3();
+            f3 Fb = zero3(), e = zero3(), del = zero3();
             float trH = 0.f;
             if (im != 0.f) {
                 sym3 H = sym_diag(c.Hd);
@@ -379,8 +620,31 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                     const float dd = kp.x * kp.y * kp.y * (1.f + damp);
                     H.xx += dd; H.yy += dd; H.zz += dd;
                 }
-                const f3 e = touched ? sym_solve(H, db) : db * (1.f / H.xx);
-                const f3 del = xyz(LD[(size_t)(k + 1) * BLOCK + t]) - dk;
+                f3 gb = db;
+                f3 zk = xyz(Dn[t]);  // the solve's result before the step limit
+                if constexpr (ROPE) {
+                    sym_add(H, HcA);
+                    if (hasPrev) {
+                        const float4 h0 = HB0[t - 1], h1 = HB1[t - 1];
+                        H.xx += h0.x; H.yy += h0.y; H.zz += h0.z; H.xy += h0.w; H.xz += h1.x; H.yz += h1.y;
+                    }
+                    touched = true;
+                    // d' = z lim / |z| when |z| > lim (cosserat.cu:211-214): z̄ = (lim/|z|)(I - ẑẑᵀ) d̄',
+                    // and ẑ.d̄' is the adjoint of the limit, min(own, previous segment's)
+                    const float sc = Dn[t].w;
+                    if (sc < 1.f) {
+                        const float l = len(zk);
+                        const f3 zh = zk * (1.f / l);
+                        const float zg = dot(zh, gb);
+                        if (hasPrev && RP[t - 1].y < lim) msbp += zg;
+                        else msb += zg;
+                        gb = (gb - zh * zg) * sc;
+                        zk = zk * (1.f / sc);
+                    }
+                    dn = gb;
+                }
+                e = touched ? sym_solve(H, gb) : gb * (1.f / H.xx);
+                del = zk - dk;
                 Fb = e * a.accel;
                 trH = -dot(e, del);
                 yb += Fb * c.fm;
@@ -408,9 +672,10 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
             // segment t's residual c = ((x1 - x) + (d1 - d)) / l - t(q), read before the barrier:
             // after it a neighbour may already be writing the next substep's iterates
             const float4 qk = Lq[t];
-            const f3 dkn = hasNext ? xyz(LD[(size_t)k * BLOCK + t + 1]) : zero3();
+            const f3 dkn = hasNext ? xyz(Dk[t + 1]) : zero3();
             const f3 cc = hasNext ? ((p1 - p) + (dkn - dk)) * c.invl - qtangent(qk) : zero3();
             EF[t] = f4(Fb, trH);
+            if constexpr (ROPE) EE[t] = f4(e, 0.f);
             __syncthreads();
             if (hasNext) {
                 const float4 Fn4 = EF[t + 1];
@@ -424,6 +689,30 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                 dn -= cb * c.invl;
                 xb -= cb * c.invl;
                 dn -= Fb * (damp * dd);
+                if constexpr (ROPE) {
+                    if (ncol > 0) {  // the segment's pairs reversed; other vertices' shares by shared-memory atomics
+                        const float4 zn4 = Dn[t + 1];
+                        const f3 lc = xyz(zn4) * (1.f / zn4.w) - dkn;
+                        const f3 ec = xyz(EE[t + 1]);
+                        PairGrad acc{};
+                        float4* cdk = CD + (k & 1) * BLOCK;
+                        for (int q2 = 0; q2 < ncol; q2++) {
+                            const int j = a.cols[(size_t)q2 * n + dv];
+                            PairGrad o{};
+                            collision_bwd(a, damp, p, p1, xyz(X[j]), xyz(X[j + 1]), dk, dkn, xyz(Dk[j]), xyz(Dk[j + 1]),
+                                          Fb, e, del, Fn, ec, lc, o);
+                            acc.x0 += o.x0; acc.d0 += o.d0; acc.x1 += o.x1; acc.d1 += o.d1;
+                            atomic_add3(cdk + j, o.e0);
+                            atomic_add3(cdk + j + 1, o.e1);
+                            atomic_add3(CX + j, o.y0);
+                            atomic_add3(CX + j + 1, o.y1);
+                        }
+                        dn += acc.d0;
+                        xb += acc.x0;
+                        atomic_add3(cdk + t + 1, acc.d1);
+                        atomic_add3(CX + t + 1, acc.x1);
+                    }
+                }
             }
             if (hasPrev) {
                 const float4 kp = KC[t - 1];
@@ -434,6 +723,30 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
                 dn -= Fb * (damp * ddp);
             }
             db = dn;
+        }
+
+        if constexpr (ROPE) {
+            // step-limit adjoints: the previous segment's share, then the limits reversed (the
+            // limit of segment t rests on the substep-start positions and the padding of y)
+            RP[t].w = msbp;
+            __syncthreads();
+            db += xyz(CD[t]);  // pair contributions to d̄^0
+            CD[t] = zero4();
+            if (hasNext) msb += RP[t + 1].w;
+            if (hasNext && msb != 0.f) {
+                f3 xb1 = zero3(), xj0 = zero3(), xj1 = zero3();
+                int jo;
+                const f3 ybl = step_limit_bwd(a, dv, ncol, X, p, p1, RP[t].x, y, msb, xb, xb1, jo, xj0, xj1);
+                vbn += ybl * h;  // y = v h + g h²
+                atomic_add3(CX + t + 1, xb1);
+                if (jo >= 0) {
+                    atomic_add3(CX + jo, xj0);
+                    atomic_add3(CX + jo + 1, xj1);
+                }
+            }
+            __syncthreads();
+            xb += xyz(CX[t]);
+            CX[t] = zero4();
         }
 
         // ---- inertial prediction reversed: d^0 = v h + g h² s(v, lv), y = v h + g h²
@@ -487,10 +800,10 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) adjoint_kernel(const Frame
     }
 }
 
-template <int BLOCK, int SURF>
+template <int BLOCK, int SURF, bool ROPE>
 cudaError_t launch_adjoint_t(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
-    auto k = adjoint_kernel<BLOCK, SURF>;
-    const size_t bytes = adjoint_smem_bytes(BLOCK, a.iters) +
+    auto k = adjoint_kernel<BLOCK, SURF, ROPE>;
+    const size_t bytes = adjoint_smem_bytes(BLOCK, a.iters, ROPE) +
                          (SURF == SURF_MESHES ? (size_t)a.pose_cache * kPoseF4 * sizeof(float4) : 0);
     if (bytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -499,11 +812,15 @@ cudaError_t launch_adjoint_t(const FrameArgs& a, const AdjArgs& g, int num_bins,
     k<<<num_bins, BLOCK, bytes, s>>>(a, g);
     return cudaGetLastError();
 }
+template <int BLOCK, bool ROPE>
+cudaError_t launch_adjoint_r(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
+    if (a.num_sdf > 0) return launch_adjoint_t<BLOCK, SURF_MESHES, ROPE>(a, g, num_bins, s);
+    if (a.num_planes > 0) return launch_adjoint_t<BLOCK, SURF_PLANES, ROPE>(a, g, num_bins, s);
+    return launch_adjoint_t<BLOCK, SURF_NONE, ROPE>(a, g, num_bins, s);
+}
 template <int BLOCK>
 cudaError_t launch_adjoint_b(const FrameArgs& a, const AdjArgs& g, int num_bins, cudaStream_t s) {
-    if (a.num_sdf > 0) return launch_adjoint_t<BLOCK, SURF_MESHES>(a, g, num_bins, s);
-    if (a.num_planes > 0) return launch_adjoint_t<BLOCK, SURF_PLANES>(a, g, num_bins, s);
-    return launch_adjoint_t<BLOCK, SURF_NONE>(a, g, num_bins, s);
+    return a.rope_contact ? launch_adjoint_r<BLOCK, true>(a, g, num_bins, s) : launch_adjoint_r<BLOCK, false>(a, g, num_bins, s);
 }
 
 // Caller-order state (pos / vel / lvel [n,3], q [n,4]) into device order, keeping the
@@ -559,7 +876,9 @@ __global__ void params_out_kernel(const int4* topo, const float4* pos, const flo
 
 }  // namespace
 
-size_t adjoint_smem_bytes(int block, int iters) { return sizeof(float4) * (size_t)block * (size_t)(2 * iters + 9); }
+size_t adjoint_smem_bytes(int block, int iters, bool rope) {
+    return sizeof(float4) * (size_t)block * (size_t)(2 * iters + 9 + (rope ? 7 : 0));
+}
 
 cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int num_bins, cudaStream_t s) {
     switch (block) {

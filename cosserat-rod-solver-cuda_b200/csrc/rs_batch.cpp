@@ -14,6 +14,12 @@
 namespace rs {
 
 namespace {
+// The adjoint runs whole rope-rope contact groups inside one CTA (the persistent engine's layout).
+constexpr const char* kOversizeGroup =
+    "the adjoint differentiates rope-rope contact groups that fit one CTA (bin); this group needs the plain engine";
+}  // namespace
+
+namespace {
 
 // Single-precision rotor helpers for the host setup. The setup follows YarnBall.cu:112-259
 // operation by operation (same order, IEEE float, no contraction) so that initial frames and
@@ -1189,7 +1195,7 @@ void Batch::step_program_taped(const float* p0, const float* v0, const float* p1
                                float dt, int substeps, float* tape) {
     if (!tape) throw std::invalid_argument("null tape");
     if (engine_ != 0) throw std::invalid_argument("a taped step runs the persistent engine only");
-    if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
+    if (rope_contact_ && oversize_) throw std::invalid_argument(kOversizeGroup);
     if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     pending_tape_ = reinterpret_cast<float4*>(tape);
     try {
@@ -1209,7 +1215,7 @@ float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synch
     if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the end-state outputs are required");
     if (!roots_pinned()) throw std::invalid_argument("the program frame drives every rope's root");
     if (io.tape) {
-        if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
+        if (rope_contact_ && oversize_) throw std::invalid_argument(kOversizeGroup);
         if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     }
     tune_before_frame();
@@ -1256,12 +1262,12 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
     if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the state adjoint outputs are required");
     if (io.p0 && (!io.v0 || !io.p1)) throw std::invalid_argument("a program frame needs p0, v0 and p1");
     if (io.q1 && !io.q0) throw std::invalid_argument("root_q_end requires root_q");
-    if (rope_contact_) throw std::invalid_argument("the adjoint does not differentiate rope-rope contact");
+    if (rope_contact_ && oversize_) throw std::invalid_argument(kOversizeGroup);
     if (!grids_.empty() && (pending_set_ || sdf_moving_)) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     ensure_device();
     if (block_ > 512)
         throw std::invalid_argument("the adjoint runs bins of at most 512 vertices (ropes of at most 512 vertices)");
-    if (adjoint_smem_bytes(block_, num_itr) + (size_t)pose_cache_entries() * 5 * sizeof(float4) > 227 * 1024)
+    if (adjoint_smem_bytes(block_, num_itr, rope_contact_) + (size_t)pose_cache_entries() * 5 * sizeof(float4) > 227 * 1024)
         throw std::invalid_argument("num_itr too large for the adjoint's shared memory at this bin size");
     grad_alloc(io.tape ? 0 : substeps);
     if (io.ea || io.ei || io.mass) {

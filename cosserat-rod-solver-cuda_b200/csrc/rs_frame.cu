@@ -188,22 +188,9 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             ncol = 0;
             lim = INFINITY;
             if (hasNext) {
-                const f3 a1 = p1 - p;
-                const float ri = fmaxf(sm.pad[t], sm.pad[t + 1]);
-                lim = sm.pad[t] - a.det_radius;
-                int cnt = 0;
-                for (int j = g0; j < g1; j++) {
-                    if (!(sm.flg[j] & F_NEXT)) continue;
-                    if (j >= r0 && j < r1 && abs(j - t) <= 2) continue;
-                    const f3 pj0 = xyz(sm.p[j]), pj1 = xyz(sm.p[j + 1]);
-                    if (rope_pair_candidate(p, a1, ri, pj0, pj1, fmaxf(sm.pad[j], sm.pad[j + 1]))) {
-                        if (cnt < kMaxCols) {
-                            a.cols[(size_t)cnt * a.n + dv] = j;
-                            lim = fminf(lim, step_limit_of(p, a1, pj0, pj1));
-                        }
-                        cnt++;
-                    }
-                }
+                const int cnt = detect_group(
+                    a, t, dv, g0, g1, r0, r1, p, p1, [&](int j) { return sm.pad[j]; }, [&](int j) { return sm.flg[j]; },
+                    [&](int j) { return xyz(sm.p[j]); }, lim);
                 if (cnt > kMaxCols) atomicMax(a.status, ERR_MAX_COLLISIONS);
                 ncol = cnt < kMaxCols ? cnt : kMaxCols;
             }
@@ -217,22 +204,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
             const bool touched =
                 position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2, btab, mytbox);
-            if constexpr (ROPE) {
-                if (ncol > 0) {
-                    // even candidates join the own terms, odd ones a second partial added after
-                    // them (the reference's two sectors, cosserat.cu:99-182)
-                    f3 fo = zero3(), f2o = zero3();
-                    sym3 Ho = sym_zero(), H2o = sym_zero();
-                    for (int cc = 0; cc < ncol; cc++) {
-                        const int j = a.cols[(size_t)cc * a.n + dv];
-                        const f3 b0 = xyz(sm.p[j]), b1 = xyz(sm.p[j + 1]);
-                        const f3 db0 = xyz(sm.dx[j]), db1 = xyz(sm.dx[j + 1]);
-                        if (cc & 1) collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, fo, f2o, Ho, H2o);
-                        else collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, f, f2, H, H2);
-                    }
-                    if (ncol > 1) { f += fo; f2 += f2o; sym_add(H, Ho); sym_add(H2, H2o); }
-                }
-            }
+            if constexpr (ROPE) collision_sectors(a, ncol, dv, sm.p, sm.dx, damp, p, p1, dx, p1dx, f, f2, H, H2);
             if (act) {
                 sm.fa[t] = f4(f2, H2.xx);
                 sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);

@@ -33,7 +33,7 @@ cudaError_t static_scratch_cols(int** ptr, int* max_verts);
 // Differentiable frames (rs_adjoint.cu): one frame's reverse sweep from the tape that a frame
 // launch with a.tape set wrote; shared memory it needs per CTA.
 cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int num_bins, cudaStream_t s);
-size_t adjoint_smem_bytes(int block, int iters);
+size_t adjoint_smem_bytes(int block, int iters, bool rope);
 // Caller-order state <-> device order (the .w constants of cst_* are kept).
 cudaError_t launch_state_in(const int4* topo, const float* pos, const float* vel, const float* lvel, const float* q,
                             const float4* cst_pos, const float4* cst_vel, const float4* cst_lvel, float4* o_pos,

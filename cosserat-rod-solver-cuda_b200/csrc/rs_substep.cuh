@@ -286,13 +286,66 @@ __device__ __forceinline__ float step_limit_of(f3 a0, f3 a1, f3 pj0, f3 pj1) {
 __device__ __forceinline__ void position_solve(f3& dx, f3 f, const sym3& H, float accel, float im, bool diag) {
     if (im != 0.f) dx += diag ? f * (accel / H.xx) : sym_solve(H, f) * accel;
 }
-// The same with the step limit of rope-rope contact, cosserat.cu:211-214.
-__device__ __forceinline__ void position_solve_limited(f3& dx, f3 f, const sym3& H, float accel, float im, float lim) {
+// The same with the step limit of rope-rope contact, cosserat.cu:211-214. Returns the limit's
+// scale lim / |dx| (1 when the step is not limited).
+__device__ __forceinline__ float position_solve_limited(f3& dx, f3 f, const sym3& H, float accel, float im, float lim) {
+    float sc = 1.f;
     if (im != 0.f) {
         dx += sym_solve(H, f) * accel;
         const float l = len(dx);
-        if (l > lim && l > 0.f) dx *= lim / l;
+        if (l > lim && l > 0.f) {
+            sc = lim / l;
+            dx *= sc;
+        }
     }
+    return sc;
+}
+
+// Rope-rope detection of segment t over its CTA-resident contact group [g0, g1) (CTA-local
+// indices; [r0, r1) is t's own rope, whose segments within two of t are skipped), ascending j,
+// capped at kMaxCols: writes the candidate list to cols[c * n + dv] and the segment's step limit
+// (padding - detection radius, and 0.45 x each listed candidate's distance), batch.cu:19-49 and
+// collision.cu:103-136. pad(j), flg(j) and pos(j) read the group's padded radii, flags and
+// substep-start positions. Returns the number of candidates found (the list keeps kMaxCols).
+template <class Pad, class Flg, class Pos>
+__device__ __forceinline__ int detect_group(const FrameArgs& a, int t, int dv, int g0, int g1, int r0, int r1, f3 p, f3 p1,
+                                           Pad pad, Flg flg, Pos pos, float& lim) {
+    const f3 a1 = p1 - p;
+    const float ri = fmaxf(pad(t), pad(t + 1));
+    lim = pad(t) - a.det_radius;
+    int cnt = 0;
+    for (int j = g0; j < g1; j++) {
+        if (!(flg(j) & F_NEXT)) continue;
+        if (j >= r0 && j < r1 && abs(j - t) <= 2) continue;
+        const f3 pj0 = pos(j), pj1 = pos(j + 1);
+        if (rope_pair_candidate(p, a1, ri, pj0, pj1, fmaxf(pad(j), pad(j + 1)))) {
+            if (cnt < kMaxCols) {
+                a.cols[(size_t)cnt * a.n + dv] = j;
+                lim = fminf(lim, step_limit_of(p, a1, pj0, pj1));
+            }
+            cnt++;
+        }
+    }
+    return cnt;
+}
+
+// Rope-rope terms of segment t over its ncol candidates, positions P and iterates D of the
+// CTA's vertices: even candidates join the own terms, odd ones a second partial added after them
+// (the reference's two sectors, cosserat.cu:99-182).
+__device__ __forceinline__ void collision_sectors(const FrameArgs& a, int ncol, int dv, const float4* P, const float4* D,
+                                                  float damp, f3 p, f3 p1, f3 dx, f3 p1dx, f3& f, f3& f2, sym3& H,
+                                                  sym3& H2) {
+    if (ncol <= 0) return;
+    f3 fo = zero3(), f2o = zero3();
+    sym3 Ho = sym_zero(), H2o = sym_zero();
+    for (int cc = 0; cc < ncol; cc++) {
+        const int j = a.cols[(size_t)cc * a.n + dv];
+        const f3 b0 = xyz(P[j]), b1 = xyz(P[j + 1]);
+        const f3 db0 = xyz(D[j]), db1 = xyz(D[j + 1]);
+        if (cc & 1) collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, fo, f2o, Ho, H2o);
+        else collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, f, f2, H, H2);
+    }
+    if (ncol > 1) { f += fo; f2 += f2o; sym_add(H, Ho); sym_add(H2, H2o); }
 }
 
 // Frame step of segment i, cosserat.cu:242-272: vv = -2 k ((p1 - p) + (p1dx - dx)) / l, b from

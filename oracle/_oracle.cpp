@@ -190,6 +190,11 @@ static void bind_sim(py::module_& m, const char* name) {
             d["ks"] = s_out(g.ks); d["rho"] = s_out(g.rho); d["w"] = s_out(g.w);
             return d;
         })
+        .def("rope_contact_counts", [](S& s) {  // (active rope-rope terms, limited steps) since the last call
+            const auto r = py::make_tuple(s.nCollisionTerms, s.nLimitedSteps);
+            s.nCollisionTerms = s.nLimitedSteps = 0;
+            return r;
+        })
         .def("contact_forces", [](S& s) { return v3_out(s.contactForce); })
         .def("wrenches", [](S& s) { return v3_out(s.wrench); });
 }

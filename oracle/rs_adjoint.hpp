@@ -59,7 +59,6 @@ public:
     // program rows (zero when prog == nullptr: a free frame) and g.ks/rho/w have been ADDED to.
     // The Sim is left at the frame's end state. prog is [p0 (3R), v0 (3R), p1 (3R)].
     void frame_backward(const T* prog, bool has_q0, const float* q0, const float* q1, float dt, int S, FrameGrad<T>& g) {
-        if (s.ropeContact) throw std::invalid_argument("oracle adjoint: rope-rope contact is not differentiated");
         if (s.pendingSet) throw std::invalid_argument("oracle adjoint: only static meshes are differentiated");
         const int n = s.n;
         s.sdf_begin_step();
@@ -86,6 +85,7 @@ public:
 
 private:
     Sim<T>& s;
+    std::vector<T> msb;  // adjoints of the substep's step limits (maxStep)
     struct State {
         std::vector<V3<T>> pos, vel, lastVel;
         std::vector<Q4<T>> q;
@@ -212,17 +212,21 @@ private:
         s.stage_poses(sub, S);
         const std::vector<V3<T>> x = s.pos, vin = s.vel, lvin = s.lastVel;
         s.init_itr();
+        if (s.ropeContact) s.brute_detect();
+        if (s.useStepLimit) s.step_limit();
         const std::vector<V3<T>> y = s.vel;  // the inertial target of free vertices
-        std::vector<std::vector<V3<T>>> d(I + 1);
+        std::vector<std::vector<V3<T>>> d(I + 1), z(I + 1);
         std::vector<std::vector<Q4<T>>> qk(I + 1);
         d[0] = s.dx;
         qk[0] = s.q;
         for (int it = 0; it < I; it++) {
             s.position_sweep();
+            z[it + 1] = s.dxRaw;
             s.frame_sweep();
             d[it + 1] = s.dx;
             qk[it + 1] = s.q;
         }
+        msb.assign(n, T(0));
         const T h = s.h, damp = s.damping / h, accel = s.accel;
         std::vector<V3<T>> db(n), xb(n), yb(n), vb(n), lvb(n);
         std::vector<Q4<T>> qb(n);
@@ -266,8 +270,9 @@ private:
         // -- iterations in reverse
         for (int it = I - 1; it >= 0; it--) {
             frame_reverse(x, d[it + 1], qk[it], qb, db, xb, g);
-            position_reverse(x, y, d[it], d[it + 1], qk[it], damp, accel, db, qb, xb, yb, g);
+            position_reverse(x, y, d[it], s.useStepLimit ? z[it + 1] : d[it + 1], qk[it], damp, accel, db, qb, xb, yb, g);
         }
+        if (s.useStepLimit) step_limit_reverse(x, vin, xb, vb);
         // -- init: d^0 = v h + g h² s, y = v h + g h²
         const V3<T> grav = s.gravity;
         const T g2 = len2(grav);
@@ -375,6 +380,204 @@ private:
         }
     }
 
+    // seg_closest (Common.h:327-345, with a0 = 0) reversed: given the adjoints of the returned
+    // (u, v), adds those of a1 = A, b0 = B0, b1 = B1. Each clamp passes its adjoint inside [0, 1],
+    // ends included; the fallback for parallel segments (a non-finite first v) is a constant.
+    static void seg_closest_bwd(const V3<T>& A, const V3<T>& B0, const V3<T>& B1, T ub, T vb, V3<T>& Ab, V3<T>& B0b,
+                                V3<T>& B1b) {
+        const V3<T> E = B1 - B0;
+        const T a = len2(A), b = dot(A, E), c = len2(E);
+        const T AB0 = dot(A, B0), EB0 = dot(E, B0);
+        const T Den = a * c - b * b, t0 = (b * AB0 - a * EB0) / Den;
+        const bool fin = m_isfinite(t0);
+        const T v0 = fin ? t0 : T(0.5);
+        const bool p0 = fin && v0 >= 0 && v0 <= 1;
+        const T v0c = std::min(std::max(v0, T(0)), T(1));
+        const V3<T> Bv = lerp(B0, B1, v0c);
+        const T tu = dot(Bv, A) / a;
+        const bool pu = tu >= 0 && tu <= 1;
+        const T u = std::min(std::max(tu, T(0)), T(1));
+        const V3<T> Au = lerp(V3<T>(), A, u) - B0;
+        const T tv = dot(Au, E) / c;
+        V3<T> Ea, Aa, B0a;  // adjoints in the (A, B0, E = B1 - B0) parametrisation
+        if (tv >= 0 && tv <= 1) {
+            const T Nb = vb / c;
+            ub += Nb * dot(A, E);
+            Aa += E * (Nb * u);
+            B0a -= E * Nb;
+            Ea += Au * Nb + E * (T(-2) * vb * tv / c);
+        }
+        if (pu) {
+            const T Mb = ub / a;
+            const V3<T> Bvb = A * Mb;
+            B0a += Bvb;
+            Ea += Bvb * v0c;
+            Aa += Bv * Mb + A * (T(-2) * ub * tu / a);
+            if (p0) {
+                const T t0b = dot(Bvb, E);
+                const T Numb = t0b / Den, Denb = -t0b * t0 / Den;
+                const T bb = Numb * AB0 - T(2) * b * Denb, aa = -Numb * EB0 + Denb * c, cc = Denb * a;
+                const T AB0b = Numb * b, EB0b = -Numb * a;
+                Aa += E * bb + A * (T(2) * aa) + B0 * AB0b;
+                Ea += A * bb + E * (T(2) * cc) + B0 * EB0b;
+                B0a += A * AB0b + E * EB0b;
+            }
+        }
+        Ab += Aa;
+        B1b += Ea;
+        B0b += B0a - Ea;
+    }
+    // Collision Hessians of every segment's candidates at iterate d^k: Ha to vertex i, Hb to i+1.
+    void collision_hessians(const std::vector<V3<T>>& dk, T damp, std::vector<S3<T>>& Ha, std::vector<S3<T>>& Hb) const {
+        const int n = s.n;
+        Ha.assign(n, S3<T>());
+        Hb.assign(n, S3<T>());
+        const std::vector<V3<T>> keep = s.dx;
+        s.dx = dk;
+        const T invb = T(1) / s.barrier, rad2 = T(2) * s.radius, kCol = s.kCollision * invb;
+        for (int i = 0; i < n; i++) {
+            if (!has(i, F_NEXT)) continue;
+            V3<T> f, f2;
+            for (int c = 0; c < s.numCols[i]; c++)
+                s.collision_term(i, s.cols[i][c], s.lastPos[i + 1], dk[i + 1], dk[i], invb, rad2, kCol, damp, f, f2, Ha[i], Hb[i]);
+        }
+        s.dx = keep;
+    }
+    // One rope-rope candidate reversed (cosserat.cu:99-157). Segment i's term with candidate o adds
+    // f, H to vertex i with weight wa = 1 - u and f2, H2 to vertex i+1 with weight wb = u; given F̄
+    // and H̄ = -e δᵀ of both vertices (Fa, ea, la for i; Fc, ec, lc for i+1), adds d̄ and x̄ of the
+    // four vertices i, i+1, o, o+1. Barrier: s = (|n| - 2r)/b clamped below at 1e-3, ff and dH of
+    // the log barrier; friction f1 = min(kf, μ ff / |uu|) along the tangential slip uu.
+    void collision_bwd(int i, int o, const std::vector<V3<T>>& x, const std::vector<V3<T>>& dk, T damp, const V3<T>& Fa,
+                       const V3<T>& ea, const V3<T>& la, const V3<T>& Fc, const V3<T>& ec, const V3<T>& lc,
+                       std::vector<V3<T>>& db, std::vector<V3<T>>& xb) const {
+        const T invb = T(1) / s.barrier, rad2 = T(2) * s.radius, kCol = s.kCollision * invb;
+        const V3<T> xi = x[i], x1 = x[i + 1], xo0 = x[o], xo1 = x[o + 1];
+        const V3<T> di = dk[i], d1 = dk[i + 1], do0 = dk[o], do1 = dk[o + 1];
+        const V3<T> A = (x1 - xi) + (d1 - di), B0 = (xo0 - xi) + (do0 - di), B1 = (xo1 - xi) + (do1 - di);
+        T u, v;
+        seg_closest(V3<T>(), A, B0, B1, u, v);
+        const V3<T> dpos = lerp(xi, x1, u) - lerp(xo0, xo1, v);
+        const V3<T> ddpos = lerp(di, d1, u) - lerp(do0, do1, v);
+        const V3<T> raw = dpos + ddpos;
+        const T dist = len(raw);
+        if (!(dist > 0)) return;
+        const V3<T> nr = raw * (T(1) / dist);
+        const T wb = u, wa = T(1) - u;
+        const T sr = (dist - rad2) * invb;
+        if (sr > 1) return;
+        const T sd = std::max(sr, T(1e-3));
+        const T invd = T(1) / sd, logd = m_log(sd);
+        const T dH = (T(-3) + (T(2) + invd) * invd - T(2) * logd) * kCol * invb;
+        const T ff = -(T(1) - sd) * (sd - T(1) + T(2) * sd * logd) * invd * kCol;
+        const T Ga = dot(Fa, nr), Gc = dot(Fc, nr), ndi = dot(nr, di), nd1 = dot(nr, d1);
+        const T nHa = -dot(nr, ea) * dot(nr, la), nHc = -dot(nr, ec) * dot(nr, lc);
+        const T trA = -dot(ea, la), trC = -dot(ec, lc);
+        // (H̄ + H̄ᵀ) n for H̄ = -e δᵀ
+        const V3<T> symA = ea * (-dot(la, nr)) - la * dot(ea, nr), symC = ec * (-dot(lc, nr)) - lc * dot(ec, nr);
+        const V3<T> symS = symA * (wa * wa) + symC * (wb * wb);
+        const T nHs = wa * wa * nHa + wb * wb * nHc, trS = wa * wa * trA + wb * wb * trC;
+        T ffb = Ga * wa + Gc * wb;
+        const T dHb = -damp * (Ga * wa * wa * ndi + Gc * wb * wb * nd1) + (T(1) + damp) * nHs;
+        T wab = Ga * ff - T(2) * damp * dH * wa * Ga * ndi + T(2) * wa * (T(1) + damp) * dH * nHa;
+        T wbb = Gc * ff - T(2) * damp * dH * wb * Gc * nd1 + T(2) * wb * (T(1) + damp) * dH * nHc;
+        V3<T> nb = Fa * (ff * wa - damp * dH * wa * wa * ndi) + Fc * (ff * wb - damp * dH * wb * wb * nd1) +
+                   di * (-damp * dH * wa * wa * Ga) + d1 * (-damp * dH * wb * wb * Gc) + symS * ((T(1) + damp) * dH);
+        V3<T> dib = nr * (-damp * dH * wa * wa * Ga), d1b = nr * (-damp * dH * wb * wb * Gc);
+        V3<T> ddb;  // adjoint of ddpos
+        const V3<T> uu = ddpos - nr * dot(nr, ddpos);
+        const T ul = len(uu);
+        if (ul > 0) {
+            const T ratio = s.fricMu * ff / ul;
+            const T f1 = std::min(s.kFriction, ratio);
+            const V3<T> Fu = Fa * wa + Fc * wb;
+            const T f1b = -dot(uu, Fu) - (nHs - trS);
+            wab += -f1 * dot(uu, Fa) - T(2) * wa * f1 * (nHa - trA);
+            wbb += -f1 * dot(uu, Fc) - T(2) * wb * f1 * (nHc - trC);
+            nb -= symS * f1;
+            V3<T> uub = Fu * (-f1);
+            if (!(s.kFriction < ratio)) {  // f1 = μ ff / |uu|
+                ffb += f1b * s.fricMu / ul;
+                uub += uu * (-f1b * ratio / (ul * ul));
+            }
+            ddb += uub - nr * dot(nr, uub);
+            nb -= uub * dot(nr, ddpos) + ddpos * dot(nr, uub);
+        }
+        T ub = wbb - wab, distb = 0;
+        if (sr >= T(1e-3)) {
+            const T p = T(1) - sd, qv = sd - T(1) + T(2) * sd * logd;
+            const T ffp = -kCol * ((-qv + p * (T(3) + T(2) * logd)) * invd - p * qv * invd * invd);
+            const T dHp = T(-2) * (invd * invd + invd * invd * invd + invd) * kCol * invb;
+            distb = (ffb * ffp + dHb * dHp) * invb;
+        }
+        const V3<T> rawb = (nb - nr * dot(nr, nb)) * (T(1) / dist) + nr * distb;
+        ddb += rawb;
+        xb[i] += rawb * wa;
+        xb[i + 1] += rawb * wb;
+        xb[o] -= rawb * (T(1) - v);
+        xb[o + 1] -= rawb * v;
+        ub += dot(rawb, x1 - xi) + dot(ddb, d1 - di);
+        const T vb = -dot(rawb, xo1 - xo0) - dot(ddb, do1 - do0);
+        dib += ddb * wa;
+        d1b += ddb * wb;
+        db[o] -= ddb * (T(1) - v);
+        db[o + 1] -= ddb * v;
+        V3<T> Ab, B0b, B1b;
+        seg_closest_bwd(A, B0, B1, ub, vb, Ab, B0b, B1b);
+        xb[i + 1] += Ab;
+        d1b += Ab;
+        xb[o] += B0b;
+        db[o] += B0b;
+        xb[o + 1] += B1b;
+        db[o + 1] += B1b;
+        const V3<T> sb = Ab + B0b + B1b;
+        xb[i] -= sb;
+        dib -= sb;
+        db[i] += dib;
+        db[i + 1] += d1b;
+    }
+    // Step limits reversed (recomputeStepLimitKernel, collision.cu:103-136): maxStep[i] is the
+    // least of padding[i] - detRadius, padding = scaledDetRadius + |v h + g h²| (initItr), and
+    // 0.45 times each candidate's closest distance at the substep start; its adjoint goes to the
+    // argument that attained it (the first, on ties, as the forward's running minimum).
+    void step_limit_reverse(const std::vector<V3<T>>& x, const std::vector<V3<T>>& vin, std::vector<V3<T>>& xb,
+                            std::vector<V3<T>>& vb) const {
+        const T h = s.h, fac = T((1 - 0.1f) * 0.5f);
+        for (int i = 0; i < s.n; i++) {
+            if (msb[i] == 0 || !has(i, F_NEXT)) continue;
+            const V3<T> a0 = x[i], a1 = x[i + 1] - a0;
+            T best = s.padding[i] - s.detRadius;
+            int arg = -1;
+            for (int c = 0; c < s.numCols[i]; c++) {
+                const int o = s.cols[i][c];
+                const V3<T> b0 = x[o] - a0, b1 = x[o + 1] - a0;
+                T u, v;
+                seg_closest(V3<T>(), a1, b0, b1, u, v);
+                const T val = fac * len(a1 * u - lerp(b0, b1, v));
+                if (val < best) { best = val; arg = c; }
+            }
+            if (arg < 0) {
+                const V3<T> y = vin[i] * h + s.gravity * (h * h);
+                const T ly = len(y);
+                if (ly > 0) vb[i] += y * (msb[i] * h / ly);
+                continue;
+            }
+            const int o = s.cols[i][arg];
+            const V3<T> b0 = x[o] - a0, b1 = x[o + 1] - a0;
+            T u, v;
+            seg_closest(V3<T>(), a1, b0, b1, u, v);
+            const V3<T> nn = a1 * u - lerp(b0, b1, v);
+            const T l = len(nn);
+            if (!(l > 0)) continue;
+            const V3<T> nnb = nn * (fac * msb[i] / l);
+            V3<T> Ab = nnb * u, B0b = nnb * (-(T(1) - v)), B1b = nnb * (-v);
+            seg_closest_bwd(a1, b0, b1, dot(nnb, a1), -dot(nnb, b1 - b0), Ab, B0b, B1b);
+            xb[i + 1] += Ab;
+            xb[o] += B0b;
+            xb[o + 1] += B1b;
+            xb[i] -= Ab + B0b + B1b;
+        }
+    }
     // Position step k reversed: db holds d̄^{k+1} on entry and d̄^k on return.
     void position_reverse(const std::vector<V3<T>>& x, const std::vector<V3<T>>& y, const std::vector<V3<T>>& dk,
                           const std::vector<V3<T>>& dn, const std::vector<Q4<T>>& qo, T damp, T accel,
@@ -384,6 +587,9 @@ private:
         const T h = s.h;
         std::vector<V3<T>> Fb(n), dnew(n), sc(n);
         std::vector<T> trH(n, T(0));
+        std::vector<V3<T>> ev(n), lv(n);  // e = H⁻¹ z̄ and δ = z - d^k per vertex (H̄ = -e δᵀ)
+        std::vector<S3<T>> HcA, HcB;
+        if (s.ropeContact) collision_hessians(dk, damp, HcA, HcB);
         for (int i = 0; i < n; i++) {
             dnew[i] = db[i];
             const T w = s.invMass[i];
@@ -398,8 +604,30 @@ private:
             }
             if (has(i, F_NEXT)) H.add_diag(s.kStretch[i] / s.lRest[i] / s.lRest[i] * (T(1) + damp));
             if (has(i, F_PREV)) H.add_diag(s.kStretch[i - 1] / s.lRest[i - 1] / s.lRest[i - 1] * (T(1) + damp));
-            const V3<T> e = sym_solve(H, db[i]);
+            if (s.ropeContact) {
+                H += HcA[i];
+                if (has(i, F_PREV)) H += HcB[i - 1];
+            }
+            // step limit d' = z lim / |z| when |z| > lim (cosserat.cu:204-208): z̄ = (lim/|z|)(I - ẑẑᵀ) d̄',
+            // and the limit's adjoint ẑ.d̄' goes to the maxStep entry that set it
+            V3<T> gb = db[i];
+            if (s.useStepLimit) {
+                T lim = s.maxStep[i];
+                int arg = i;
+                if (has(i, F_PREV) && s.maxStep[i - 1] < lim) { lim = s.maxStep[i - 1]; arg = i - 1; }
+                const T l = len(dn[i]);
+                if (l > lim && l > 0) {
+                    const V3<T> zh = dn[i] * (T(1) / l);
+                    const T zg = dot(zh, gb);
+                    msb[arg] += zg;
+                    gb = (gb - zh * zg) * (lim / l);
+                }
+            }
+            dnew[i] = gb;
+            const V3<T> e = sym_solve(H, gb);
             const V3<T> delta = dn[i] - dk[i];
+            ev[i] = e;
+            lv[i] = delta;
             Fb[i] = e * accel;
             trH[i] = -dot(e, delta);
             yb[i] += Fb[i] * a;
@@ -420,6 +648,13 @@ private:
                 if (!s.grids.empty()) wb += mesh_contact_bwd(i, x[i], dk[i], kc, Fb[i], e, delta, dnew[i], xb[i]) * (-kc / w);
             }
             g.w[i] += wb;
+        }
+        if (s.ropeContact) {
+            for (int j = 0; j < n; j++) {
+                if (!has(j, F_NEXT)) continue;
+                for (int c = 0; c < s.numCols[j]; c++)
+                    collision_bwd(j, s.cols[j][c], x, dk, damp, Fb[j], ev[j], lv[j], Fb[j + 1], ev[j + 1], lv[j + 1], dnew, xb);
+            }
         }
         for (int j = 0; j < n; j++) {
             if (!has(j, F_NEXT)) continue;

@@ -181,6 +181,8 @@ public:
     std::vector<int> ropeOf;       // per-vertex rope index
     int numEnvs = 1;
     std::vector<V3<T>> pos, vel, lastVel, dx, dxNext, lastPos;
+    std::vector<V3<T>> dxRaw;      // each iterate before the step limit (read by the adjoint)
+    mutable long long nCollisionTerms = 0, nLimitedSteps = 0;  // forward counters (tests assert coverage)
     std::vector<Q4<T>> q, qPrev, qRest;
     std::vector<T> invMass, lRest, kStretch, padding, maxStep;
     std::vector<uint32_t> flags;
@@ -276,7 +278,7 @@ public:
     void resize_all() {
         ropeOf.assign(n, 0); env.assign(n, 0);
         pos.assign(n, V3<T>()); vel.assign(n, V3<T>()); lastVel.assign(n, V3<T>());
-        dx.assign(n, V3<T>()); dxNext.assign(n, V3<T>()); lastPos.assign(n, V3<T>());
+        dx.assign(n, V3<T>()); dxNext.assign(n, V3<T>()); dxRaw.assign(n, V3<T>()); lastPos.assign(n, V3<T>());
         q.assign(n, Q4<T>()); qPrev.assign(n, Q4<T>()); qRest.assign(n, Q4<T>());
         invMass.assign(n, T(1)); lRest.assign(n, T(1)); kStretch.assign(n, T(100));
         padding.assign(n, T(0)); maxStep.assign(n, std::numeric_limits<T>::infinity());
@@ -744,9 +746,13 @@ public:
             }
             if (invMass[i] != 0) {
                 d += sym_solve(H, f) * accel;
+                dxRaw[i] = d;
                 if (useStepLimit) {
                     const T l = len(d);
-                    if (l > lim && l > 0) d *= lim / l;
+                    if (l > lim && l > 0) {
+                        d *= lim / l;
+                        nLimitedSteps++;
+                    }
                 }
             }
             dxNext[i] = d;
@@ -769,6 +775,7 @@ public:
         dist = (dist - rad2) * invb;
         if (dist > 1) return;
         dist = std::max(dist, T(1e-3));
+        nCollisionTerms++;
         const T invd = T(1) / dist, logd = m_log(dist);
         T dH = (T(-3) + (T(2) + invd) * invd - T(2) * logd) * kCol * invb;
         const T ff = -(T(1) - dist) * (dist - T(1) + T(2) * dist * logd) * invd * kCol;

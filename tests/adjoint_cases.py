@@ -133,3 +133,39 @@ def rel(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=0.1, precision="f64", backend="oracle"):
+    """Two ropes of the "c1" material in one rope-rope contact group, crossing at right angles:
+    rope 0 along x at z = 0 with both ends pinned (every vertex pinned when `static_bar`), rope 1
+    along y, `gap` above it (centre to centre), pinned at its root. Contact radius 2 mm, barrier
+    2 mm: the barrier acts while the centre lines are 4 to 6 mm apart. `backend` "cuda" builds
+    the same scene on the GPU batch."""
+    seg, density, ea, ei = MATERIALS["c1"]
+    rng = np.random.default_rng(seed)
+    r0 = np.zeros((V, 3))
+    r0[:, 0] = seg * (np.arange(V) - (V - 1) / 2)
+    r1 = np.zeros((V, 3))
+    r1[:, 0] = 0.004
+    r1[:, 1] = seg * (np.arange(V) - 3.0)
+    r1[:, 2] = gap
+    r1[1:] += rng.normal(0, 3e-4, (V - 1, 3))
+    pin0 = np.zeros(V, bool)
+    pin0[0] = pin0[-1] = True
+    if static_bar:
+        pin0[:] = True
+    pin1 = np.zeros(V, bool)
+    pin1[0] = True
+    pos = np.stack([r0, r1]).astype(np.float32)
+    if backend == "cuda":
+        import ropesim
+
+        b = ropesim.RopeBatch.from_ropes([pos[0], pos[1]], density, ea, ei, 1 / 6000, num_itr, pinned=[pin0, pin1])
+    else:
+        b = ro.RopeBatch.from_ropes([pos[0], pos[1]], density, ea, ei, 1 / 6000, num_itr, pinned=[pin0, pin1],
+                                    precision=precision)
+    b.set_gravity(np.array([0.0, 0.0, -9.81], np.float32))
+    b.damping = damping
+    b.drag = 0.2
+    b.set_rope_contact(True, radius=0.002, barrier=0.002, k_collision=0.025, mu=0.1, k_friction=1e7, group_ropes=2)
+    return b, pos

@@ -221,3 +221,78 @@ def test_oracle_adjoint_with_mesh_contact_matches_finite_differences():
         ad = float((gr[name] * u.reshape(gr[name].shape)).sum())
         scale = np.linalg.norm(gr[name]) * np.linalg.norm(u)
         assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-7 * scale + 1e-14, (name, ad, fd, scale)
+
+
+@pytest.mark.parametrize("case", ["resting_crossing", "falling_onto_bar"])
+def test_oracle_adjoint_with_rope_contact_matches_finite_differences(case):
+    """Rope-rope contact differentiated: the barrier, its damping and friction, the closest-point
+    parameters (u, v) of each candidate pair and the step limit with the limit's own dependence on
+    the substep-start state (padding and candidate distances). "resting_crossing": rope 1 rests on
+    rope 0 inside the barrier band (stretch damping 0.1); "falling_onto_bar": rope 1 drops 2 cm
+    onto a fully pinned rope at h = 1/60, so the step limit clips steps, by both of its bounds."""
+    R, V = 2, 10
+    # difference steps: the resting scene's small orientation gradient needs larger steps to rise
+    # above rounding; the falling scene's clipped steps need smaller ones to stay off their kinks
+    if case == "resting_crossing":
+        b, pos = ac.rope_crossing(V=V)
+        dt, S, F, es = 1 / 300, 20, 3, 1.0
+    else:
+        b, pos = ac.rope_crossing(V=V, gap=0.02, static_bar=True, damping=0.0)
+        dt, S, F, es = 1 / 30, 2, 3, 0.01
+    s = b._s
+    progs = ac.programs(pos, F + 1, v_std=0.3 if case != "resting_crossing" else 0.05,
+                        p_std=0.01 if case != "resting_crossing" else 0.001)
+    s.step_program_rows(np.concatenate([a[0].ravel() for a in progs]).astype(np.float64), dt, S)
+    progs = [a[1:] for a in progs]
+    tgt = ac.targets(pos, F)
+    st0, par0 = s.get_state(), s.get_params()
+    wr = np.random.default_rng(7)
+    w_end = (1e-2 * wr.standard_normal((R * V, 3)), 1e-3 * wr.standard_normal((R * V, 3)))
+    L0, gr = ac.oracle_loss_and_grad(b, progs, tgt, dt, S, V, w_end=w_end)
+
+    def loss(progs_, st_, par_):
+        s.set_state(*st_)
+        s.set_params(*par_)
+        P0, V0, P1 = progs_
+        val = 0.0
+        for f in range(F):
+            s.step_program_rows(np.concatenate([P0[f].ravel(), V0[f].ravel(), P1[f].ravel()]).astype(np.float64), dt, S)
+            x = s.get_state()[0].reshape(R, V, 3)
+            val += ((x[:, -1] - tgt[f]) ** 2).sum(-1).mean()
+        xF, vF = s.get_state()[:2]
+        return val + float((w_end[0] * xF).sum() + (w_end[1] * vF).sum())
+
+    s.rope_contact_counts()
+    loss(progs, st0, par0)
+    terms, limited = s.rope_contact_counts()
+    assert terms > 0  # barrier terms act during the differentiated frames
+    if case == "falling_onto_bar":
+        assert limited > 0  # and the step limit clips steps
+    rng = np.random.default_rng(11)
+    l = s.rest_lengths()
+    w = par0[2]
+    free = w != 0
+    ea0 = par0[0] / l
+    m0 = np.where(free, 1 / np.where(free, w, 1), 0)
+    seg = np.ones(R * V, bool)
+    seg[V - 1::V] = False
+    cases = []
+    for k, name in enumerate(("g_p0", "g_v0", "g_p1")):
+        u = rng.standard_normal(progs[k].shape)
+        cases.append((name, u, lambda e, u=u, k=k: loss([p + (e * u if j == k else 0) for j, p in enumerate(progs)], st0, par0), 1e-6 * es))
+    for k, name, eps in ((0, "g_pos", 1e-6 * es), (1, "g_vel", 1e-4 * es), (3, "g_q", 1e-4 * es)):
+        u = rng.standard_normal(st0[k].shape)
+        if name == "g_pos":
+            u[::V] = 0
+        cases.append((name, u, lambda e, u=u, k=k: loss(progs, [a + e * u if j == k else a for j, a in enumerate(st0)], par0), eps))
+    u = rng.standard_normal(R * V) * seg * ea0
+    cases.append(("g_ea", u, lambda e, u=u: loss(progs, st0, [(ea0 + e * u) * l, par0[1], w]), 1e-5 * es))
+    u = rng.standard_normal(R * V) * free * m0
+    cases.append(("g_mass", u, lambda e, u=u: loss(progs, st0, [par0[0], par0[1], np.where(free, 1 / np.where(free, m0 + e * u, 1), 0)]), 1e-3 * es))
+    for name, u, fn, eps in cases:
+        d1 = (fn(eps) - fn(-eps)) / (2 * eps)
+        d2 = (fn(eps / 2) - fn(-eps / 2)) / eps
+        fd = (4 * d2 - d1) / 3
+        ad = float((gr[name] * u.reshape(gr[name].shape)).sum())
+        scale = np.linalg.norm(gr[name]) * np.linalg.norm(u)
+        assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-7 * scale + 1e-14, (name, ad, fd, scale)

@@ -195,21 +195,87 @@ def test_differentiable_frame_forward_is_the_step():
         assert float((xa - st[0]).abs().max()) <= 1e-5
 
 
-def test_adjoint_refuses_contact_it_does_not_differentiate():
+def test_adjoint_refuses_contact_groups_larger_than_a_cta():
+    """The adjoint runs each rope-rope contact group inside one CTA; a group of 20 x 64 = 1280
+    vertices runs the plain engine forward and is refused, by the taped step or the backward."""
     import torch
 
     import ropesim.grad as rg
 
-    _, pos = ac.scene(R=R, V=V, plane=True, material="c1")
+    Rg, Vg = 20, 64
+    _, pos = ac.scene(R=Rg, V=Vg, plane=False, material="c1")
     progs = ac.programs(pos, 1)
-    b = _gpu_batch(pos)
-    b.set_rope_contact(True, 2e-3, 1e-3, 1e-5, 0.1, 5.0, 1.2, 1)
+    b = _gpu_batch(pos, plane=False)
+    b.set_rope_contact(True, 2e-3, 1e-3, 1e-5, 0.1, 5.0, 1.2, Rg)
     st = [t.requires_grad_() for t in rg.state(b)]
     par = rg.parameters(b)
     p0, v0, p1 = (torch.tensor(x[0], device="cuda") for x in progs)
-    with pytest.raises(ValueError, match="rope-rope"):  # refused by the taped step or the backward
+    with pytest.raises(ValueError, match="fit one CTA"):
         out = rg.frame(b, st, par, p0, v0, p1, DT, 10)
         out[0].sum().backward()
-    with pytest.raises(ValueError, match="rope-rope"):
+    with pytest.raises(ValueError, match="fit one CTA"):
         out = rg.frame(b, st, par, p0, v0, p1, DT, 10, tape=False)
         out[0].sum().backward()
+
+
+# Rope-rope contact scenes (tests/adjoint_cases.rope_crossing; the oracle adjoint is pinned on
+# them by FP64 finite differences in test_adjoint_oracle.py): (scene, dt, substeps, frames,
+# program spread). "resting_crossing": rope 1 settles on rope 0 inside the barrier band (192
+# active pair terms); "clipped_crossing": rope 1 starts 7 mm above rope 0 and steps of h = 1/60
+# are clipped by the step limit (51 of them, at the padding bound) while 40 pair terms act. The
+# limit's other bound (a candidate's distance) binds only in scenes whose FP64 gradient itself
+# moves by 0.3% .. 100% when the start state moves by 1e-8 m (e.g. a rope dropped onto a pinned
+# one), where FP32 cannot be compared; it is pinned by FP64 finite differences on the CPU. The
+# loss adds a seeded linear term of the final state to the tip loss (rope 0's tip is pinned).
+# The pair shares of the other segment are summed with shared-memory atomics, so these
+# gradients are reproducible to rounding, not bitwise.
+ROPE_SCENES = {
+    "resting_crossing": (dict(damping=0.0), 1 / 300, 20, 3, dict(v_std=0.05, p_std=0.001)),
+    "clipped_crossing": (dict(gap=0.007, damping=0.0), 1 / 60, 1, 4, dict(v_std=0.3, p_std=0.01)),
+}
+
+
+@pytest.mark.parametrize("kind", list(ROPE_SCENES))
+def test_rope_contact_adjoint_matches_fp64_oracle(kind):
+    import torch
+
+    import ropesim.grad as rg
+
+    kw, dt, S_, F_, pk = ROPE_SCENES[kind]
+    Rr, Vr = 2, 10
+    ob, pos = ac.rope_crossing(V=Vr, **kw)
+    progs = ac.programs(pos, F_, **pk)
+    tgt = ac.targets(pos, F_)
+    wr = np.random.default_rng(7)
+    w_end = (1e-2 * wr.standard_normal((Rr * Vr, 3)), 1e-3 * wr.standard_normal((Rr * Vr, 3)))
+    L64, g64 = ac.oracle_loss_and_grad(ob, progs, tgt, dt, S_, Vr, w_end=w_end)
+    ob32, _ = ac.rope_crossing(V=Vr, precision="f32", **kw)
+    L32, g32 = ac.oracle_loss_and_grad(ob32, progs, tgt, dt, S_, Vr, w_end=w_end)
+    b, _ = ac.rope_crossing(V=Vr, backend="cuda", **kw)
+    st = [t.clone().requires_grad_() for t in rg.state(b)]
+    par = [t.clone().requires_grad_() for t in rg.parameters(b)]
+    P = [torch.tensor(a, device="cuda", requires_grad=True) for a in progs]
+    tg = torch.tensor(tgt, device="cuda", dtype=torch.float32)
+    cur, loss = st, 0.0
+    for f in range(F_):
+        cur = rg.frame(b, cur, par, P[0][f], P[1][f], P[2][f], dt, S_)
+        tip = cur[0].view(Rr, Vr, 3)[:, -1]
+        loss = loss + ((tip - tg[f]) ** 2).sum(-1).mean()
+    Wx, Wv = (torch.tensor(w, device="cuda", dtype=torch.float32) for w in w_end)
+    loss = loss + (Wx * cur[0]).sum() + (Wv * cur[1]).sum()
+    loss.backward()
+    g = {"g_p0": P[0].grad, "g_v0": P[1].grad, "g_p1": P[2].grad, "g_ea": par[0].grad, "g_ei": par[1].grad,
+         "g_mass": par[2].grad, "g_pos": st[0].grad, "g_vel": st[1].grad, "g_lvel": st[2].grad, "g_q": st[3].grad}
+    g = {k: v.detach().cpu().numpy().astype(np.float64) for k, v in g.items()}
+    L = float(loss.detach())
+    print(f"\n  [{kind}] loss gpu {L:.8e} fp64 {L64:.8e} fp32-oracle {L32:.8e}")
+    assert abs(L - L64) <= max(1e-4 * abs(L64), 4 * abs(L32 - L64))
+    for k in GROUPS:
+        if np.linalg.norm(g64[k]) == 0.0:  # one substep: v0 cancels from the root's velocity exactly
+            assert np.abs(g[k]).max() <= 1e-6 * np.linalg.norm(g64["g_p1"]), k
+            continue
+        e_gpu = ac.rel(g[k], g64[k])
+        e_32 = ac.rel(g32[k], g64[k])
+        print(f"  {k:7s} |g| {np.linalg.norm(g64[k]):.3e}  gpu-vs-fp64 {e_gpu:.2e}  fp32-oracle-vs-fp64 {e_32:.2e}")
+        assert np.isfinite(g[k]).all()
+        assert e_gpu <= max(1e-4, 4 * e_32), k
