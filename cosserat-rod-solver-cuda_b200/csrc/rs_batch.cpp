@@ -14,12 +14,6 @@
 namespace rs {
 
 namespace {
-// The adjoint runs whole rope-rope contact groups inside one CTA (the persistent engine's layout).
-constexpr const char* kOversizeGroup =
-    "the adjoint differentiates rope-rope contact groups that fit one CTA (bin); this group needs the plain engine";
-}  // namespace
-
-namespace {
 
 // Single-precision rotor helpers for the host setup. The setup follows YarnBall.cu:112-259
 // operation by operation (same order, IEEE float, no contraction) so that initial frames and
@@ -124,10 +118,12 @@ Batch::~Batch() {
         if (p) cudaFree(p);
     if (pl_graph_) cudaGraphExecDestroy(pl_graph_);
     void* pbufs[] = {pl_.dx, pl_.dxn, pl_.y, pl_.qprev, pl_.lpos, pl_.facc, pl_.cand, pl_.spose, d_pl_args_,
-                     d_grp_, d_cols_, d_ncols_, d_maxstep_, d_pad_, gs_pos_, gs_vel_, gs_lvel_, gs_q_, gs_buf_, d_tape_};
+                     d_grp_, d_cols_, d_ncols_, d_maxstep_, d_pad_, gs_pos_, gs_vel_, gs_lvel_, gs_q_, gs_buf_, d_tape_,
+                     d_padj_, d_adj_args_};
     for (void* p : pbufs)
         if (p) cudaFree(p);
     if (h_pl_args_) cudaFreeHost(h_pl_args_);
+    if (h_adj_args_) cudaFreeHost(h_adj_args_);
     if (h_prog_) cudaFreeHost(h_prog_);
     if (h_status_) cudaFreeHost(h_status_);
     if (ev0_) cudaEventDestroy(ev0_);
@@ -1194,8 +1190,6 @@ void Batch::get_parameters(float* ea, float* ei, float* mass, bool on_device) {
 void Batch::step_program_taped(const float* p0, const float* v0, const float* p1, const float* q0, const float* q1,
                                float dt, int substeps, float* tape) {
     if (!tape) throw std::invalid_argument("null tape");
-    if (engine_ != 0) throw std::invalid_argument("a taped step runs the persistent engine only");
-    if (rope_contact_ && oversize_) throw std::invalid_argument(kOversizeGroup);
     if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     pending_tape_ = reinterpret_cast<float4*>(tape);
     try {
@@ -1215,7 +1209,6 @@ float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synch
     if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the end-state outputs are required");
     if (!roots_pinned()) throw std::invalid_argument("the program frame drives every rope's root");
     if (io.tape) {
-        if (rope_contact_ && oversize_) throw std::invalid_argument(kOversizeGroup);
         if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     }
     tune_before_frame();
@@ -1231,8 +1224,6 @@ float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synch
     sdf_begin();
     const float last = h_;
     pending_tape_ = reinterpret_cast<float4*>(io.tape);
-    const bool plain = engine_ == 1 || (rope_contact_ && oversize_);
-    if (io.tape && plain) { pending_tape_ = nullptr; throw std::invalid_argument("a taped frame runs the persistent engine only"); }
     run_frame(ROOT_PROGRAM, false, false, dt, substeps, dt / (float)substeps);
     pending_tape_ = nullptr;
     time_ += dt;
@@ -1262,12 +1253,14 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
     if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the state adjoint outputs are required");
     if (io.p0 && (!io.v0 || !io.p1)) throw std::invalid_argument("a program frame needs p0, v0 and p1");
     if (io.q1 && !io.q0) throw std::invalid_argument("root_q_end requires root_q");
-    if (rope_contact_ && oversize_) throw std::invalid_argument(kOversizeGroup);
     if (!grids_.empty() && (pending_set_ || sdf_moving_)) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     ensure_device();
-    if (block_ > 512)
+    // contact groups larger than one CTA (and the plain engine) take the per-launch adjoint
+    const bool plain = engine_ == 1 || (rope_contact_ && oversize_);
+    if (!plain && block_ > 512)
         throw std::invalid_argument("the adjoint runs bins of at most 512 vertices (ropes of at most 512 vertices)");
-    if (adjoint_smem_bytes(block_, num_itr, rope_contact_) + (size_t)pose_cache_entries() * 5 * sizeof(float4) > 227 * 1024)
+    if (!plain &&
+        adjoint_smem_bytes(block_, num_itr, rope_contact_) + (size_t)pose_cache_entries() * 5 * sizeof(float4) > 227 * 1024)
         throw std::invalid_argument("num_itr too large for the adjoint's shared memory at this bin size");
     grad_alloc(io.tape ? 0 : substeps);
     if (io.ea || io.ei || io.mass) {
@@ -1288,7 +1281,8 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
         r.out_pos = gs_buf_; r.out_vel = gs_buf_ + 3 * (size_t)n_; r.out_q = gs_buf_ + 6 * (size_t)n_;
         r.forces_on = 0; r.out_force = nullptr; r.wrench = nullptr;
         r.tape = d_tape_;
-        check(launch_frame(r, block_, (int)bins_.size(), stream_), "frame replay");
+        if (plain) run_frame_plain(r);
+        else check(launch_frame(r, block_, (int)bins_.size(), stream_), "frame replay");
         tape = d_tape_;
     }
     AdjArgs g{};
@@ -1302,7 +1296,29 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
         if (io.o_v0) check(cudaMemsetAsync(io.o_v0, 0, sizeof(float) * 3 * R_, stream_), "zero");
         if (io.o_p1) check(cudaMemsetAsync(io.o_p1, 0, sizeof(float) * 3 * R_, stream_), "zero");
     }
-    check(launch_adjoint(a, g, block_, (int)bins_.size(), stream_), "adjoint");
+    if (plain) {
+        const size_t words = adjoint_plain_words(n_, num_itr);
+        if (words > padj_words_) {
+            if (d_padj_) check(cudaStreamSynchronize(stream_), "adjoint buffer reuse");
+            if (d_padj_) cudaFree(d_padj_);
+            d_padj_ = nullptr;
+            check(cudaMalloc(&d_padj_, sizeof(float4) * words), "cudaMalloc(adjoint arrays)");
+            padj_words_ = words;
+        }
+        if (!d_adj_args_) {
+            check(cudaMalloc(&d_adj_args_, sizeof(FrameArgs)), "cudaMalloc(adjoint args)");
+            check(cudaMallocHost(&h_adj_args_, sizeof(FrameArgs)), "cudaMallocHost(adjoint args)");
+        }
+        check(cudaStreamSynchronize(stream_), "adjoint args reuse");  // the previous backward read h_adj_args_
+        *h_adj_args_ = a;
+        check(cudaMemcpyAsync(d_adj_args_, h_adj_args_, sizeof(FrameArgs), cudaMemcpyHostToDevice, stream_), "upload(args)");
+        const int surf = a.num_sdf > 0 ? 2 : (a.num_planes > 0 ? 1 : 0);
+        check(launch_adjoint_plain(d_adj_args_, g, adjoint_plain_carve(d_padj_, n_, num_itr), n_, num_itr, substeps, surf,
+                                   rope_contact_, stream_),
+              "adjoint (per launch)");
+    } else {
+        check(launch_adjoint(a, g, block_, (int)bins_.size(), stream_), "adjoint");
+    }
     if (synchronize) check(cudaStreamSynchronize(stream_), "backward");
 }
 

@@ -303,6 +303,11 @@ private:
     int tape_steps_ = 0;
     float4* pending_tape_ = nullptr;  // tape of the frame being launched (step_program_taped)
     void grad_alloc(int substeps);
+    // the per-launch adjoint (contact groups larger than one CTA, plain engine)
+    float4* d_padj_ = nullptr;      // adjoint_plain_words(n, iters) float4
+    size_t padj_words_ = 0;
+    FrameArgs* d_adj_args_ = nullptr;
+    FrameArgs* h_adj_args_ = nullptr;  // pinned staging of the backward's frame parameters
 };
 
 }  // namespace rs

@@ -34,6 +34,13 @@ cudaError_t static_scratch_cols(int** ptr, int* max_verts);
 // launch with a.tape set wrote; shared memory it needs per CTA.
 cudaError_t launch_adjoint(const FrameArgs& a, const AdjArgs& g, int block, int num_bins, cudaStream_t s);
 size_t adjoint_smem_bytes(int block, int iters, bool rope);
+// The same reverse sweep as per-vertex launches over HBM arrays (rs_adjoint_plain.cu), for
+// contact groups larger than one CTA and the plain engine: `pa` is the frame's FrameArgs in
+// device memory; its arrays are carved from one float4 buffer of adjoint_plain_words(n, iters).
+size_t adjoint_plain_words(int n, int iters);
+PlainAdjBufs adjoint_plain_carve(float4* base, int n, int iters);
+cudaError_t launch_adjoint_plain(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs& b, int n, int iters,
+                                 int substeps, int surf, bool rope, cudaStream_t st);
 // Caller-order state <-> device order (the .w constants of cst_* are kept).
 cudaError_t launch_state_in(const int4* topo, const float* pos, const float* vel, const float* lvel, const float* q,
                             const float4* cst_pos, const float4* cst_vel, const float4* cst_lvel, float4* o_pos,

@@ -54,12 +54,23 @@ __global__ void plain_pose_kernel(const FrameArgs* __restrict__ pa, PlainBufs b,
 }
 
 // Inertial prediction, initial guess, lastPos, iteration.cu:34-68; the first substep of a
-// frame resets the broad phase to "every mesh".
-__global__ void plain_init_kernel(const FrameArgs* __restrict__ pa, PlainBufs b, int n, int first) {
+// frame resets the broad phase to "every mesh". Differentiable frames tape the substep's start
+// state here (after its root program; caller order, broad-phase mask in the .w lanes).
+__global__ void plain_init_kernel(const FrameArgs* __restrict__ pa, PlainBufs b, int n, int s) {
     const FrameArgs& a = *pa;
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
+    const int first = s == 0;
     const float4 P = a.pos[d], Vv = a.vel[d], L = a.lvel[d];
+    if (first) b.cand[d] = all_meshes(a.num_sdf);
+    if (a.tape) {
+        const uint64_t cm = b.cand[d];
+        float4* tp = a.tape + (size_t)s * 4 * n + a.topo[d].z;
+        tp[0] = make_float4(P.x, P.y, P.z, __int_as_float((int)(uint32_t)cm));
+        tp[n] = make_float4(Vv.x, Vv.y, Vv.z, __int_as_float((int)(uint32_t)(cm >> 32)));
+        tp[2 * (size_t)n] = L;
+        tp[3 * (size_t)n] = a.q[d];
+    }
     const f3 g = mk3(a.gx, a.gy, a.gz);
     f3 dx, y;
     init_vertex(xyz(Vv), xyz(L), P.w, a.h, a.last_h, g, dot(g, g), dx, y);
@@ -67,7 +78,6 @@ __global__ void plain_init_kernel(const FrameArgs* __restrict__ pa, PlainBufs b,
     b.dx[d] = f4(dx, 0.f);
     b.y[d] = f4(y, 0.f);
     b.lpos[d] = P;
-    if (first) b.cand[d] = all_meshes(a.num_sdf);
     if (a.rope_contact) a.pad[d] = a.sdet_radius + len(y);
 }
 
@@ -269,7 +279,7 @@ cudaError_t plain_launch_pre(const FrameArgs* pa, const PlainBufs& b, int n, int
     if (root_mode != ROOT_NONE && (root_mode == ROOT_PROGRAM || s == 0))
         plain_root_kernel<<<blocks_of(nropes, 128), 128, 0, st>>>(pa, nropes, s);
     if (num_sdf > 0 && moving) plain_pose_kernel<<<blocks_of(envs * num_sdf, 128), 128, 0, st>>>(pa, b, envs, s);
-    plain_init_kernel<<<blocks_of(n, 256), 256, 0, st>>>(pa, b, n, s == 0 ? 1 : 0);
+    plain_init_kernel<<<blocks_of(n, 256), 256, 0, st>>>(pa, b, n, s);
     if (rope) plain_detect_kernel<<<blocks_of(n, 128), 128, 0, st>>>(pa, b, n);
     return cudaGetLastError();
 }

@@ -158,6 +158,26 @@ struct AdjArgs {
 };
 
 // Global-memory working set of the per-substep-launch (plain) engine.
+// HBM arrays of the per-launch adjoint (contact groups larger than one CTA, or the plain engine),
+// one float4 (or word) per device vertex unless noted.
+struct PlainAdjBufs {
+    float4* ld;           // [(iters + 1) n] displacement iterates d^k (.w: the step limit's scale)
+    float4* lq;           // [(iters + 1) n] frame iterates q^k
+    float4* x;            // substep-start positions (+ invMass)
+    float4* y;            // inertial targets
+    uint64_t* cand;       // broad-phase mesh mask of the substep (from the tape)
+    float4 *gx, *gv, *gl, *gq;  // (x̄, k̄s), (v̄, ρ̄), (l̄v, ρ̄ of the previous segment), q̄
+    float4 *gp0, *gv0, *gp1;    // program adjoints of driven roots (.w of gv0: w̄, the invMass adjoint)
+    float4 *td, *tn, *ty;       // per substep: d̄, v̄ at the substep start, ȳ
+    float2* ms;                 // per substep: step-limit adjoints (own segment, previous segment)
+    float4 *ea, *eb, *ec;       // frame reverse: shares to the previous / next rotor, segment share
+    float4 *ha0, *ha1, *hb0, *hb1;  // collision Hessians at d^k: own share, next vertex's share
+    float4 *ef, *ee;            // (F̄, tr H̄) and e = H⁻¹ z̄ of the position reverse
+    float4* cd;                 // [2 n] pair shares of d̄ by iteration parity (atomics)
+    float4* cx;                 // pair shares of x̄ over the substep (atomics)
+    float4* qp;                 // quadratic-drag share on the previous vertex's frame
+};
+
 struct PlainBufs {
     float4* dx;       // displacement iterate
     float4* dxn;      // next iterate (Jacobi output)

@@ -135,12 +135,14 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=0.1, precision="f64", backend="oracle"):
+def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=0.1, precision="f64", backend="oracle",
+                  pairs=1):
     """Two ropes of the "c1" material in one rope-rope contact group, crossing at right angles:
     rope 0 along x at z = 0 with both ends pinned (every vertex pinned when `static_bar`), rope 1
     along y, `gap` above it (centre to centre), pinned at its root. Contact radius 2 mm, barrier
     2 mm: the barrier acts while the centre lines are 4 to 6 mm apart. `backend` "cuda" builds
-    the same scene on the GPU batch."""
+    the same scene on the GPU batch. `pairs` > 1 repeats the crossing along x (pair p shifted by
+    p x (V + 4) x 3 cm, clear of the others), all ropes in one contact group."""
     seg, density, ea, ei = MATERIALS["c1"]
     rng = np.random.default_rng(seed)
     r0 = np.zeros((V, 3))
@@ -156,16 +158,21 @@ def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=
         pin0[:] = True
     pin1 = np.zeros(V, bool)
     pin1[0] = True
-    pos = np.stack([r0, r1]).astype(np.float32)
+    ropes, pins = [], []
+    for k in range(pairs):
+        shift = np.array([k * (V + 4) * seg, 0.0, 0.0])
+        ropes += [r0 + shift, r1 + shift]
+        pins += [pin0, pin1]
+    pos = np.stack(ropes).astype(np.float32)
     if backend == "cuda":
         import ropesim
 
-        b = ropesim.RopeBatch.from_ropes([pos[0], pos[1]], density, ea, ei, 1 / 6000, num_itr, pinned=[pin0, pin1])
+        b = ropesim.RopeBatch.from_ropes(list(pos), density, ea, ei, 1 / 6000, num_itr, pinned=pins)
     else:
-        b = ro.RopeBatch.from_ropes([pos[0], pos[1]], density, ea, ei, 1 / 6000, num_itr, pinned=[pin0, pin1],
-                                    precision=precision)
+        b = ro.RopeBatch.from_ropes(list(pos), density, ea, ei, 1 / 6000, num_itr, pinned=pins, precision=precision)
     b.set_gravity(np.array([0.0, 0.0, -9.81], np.float32))
     b.damping = damping
     b.drag = 0.2
-    b.set_rope_contact(True, radius=0.002, barrier=0.002, k_collision=0.025, mu=0.1, k_friction=1e7, group_ropes=2)
+    b.set_rope_contact(True, radius=0.002, barrier=0.002, k_collision=0.025, mu=0.1, k_friction=1e7,
+                       group_ropes=2 * pairs)
     return b, pos

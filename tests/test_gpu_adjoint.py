@@ -42,7 +42,7 @@ SCENES = {
 }
 
 
-def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clearance=None, mesh=False):
+def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clearance=None, mesh=False, engine=None):
     import ropesim
 
     _, density, ea, ei = ac.MATERIALS[material]
@@ -58,6 +58,8 @@ def _gpu_batch(pos, plane=True, damping=0.0, drag_quad=0.0, material="c1", clear
         args, mp, quat = ac.mesh_setup(pos)
         b.set_contact(0.005, mu_s=0.0, mu_k=0.0)
         b.add_mesh(*args, pos=mp, quat=quat, mu_s=0.0, mu_k=0.0)
+    if engine:
+        b.set_engine(engine)
     return b
 
 
@@ -83,8 +85,11 @@ def _gpu_loss_and_grad(pos, progs, tgt, tape=True, **kw):
     return float(loss.detach()), {k: v.detach().cpu().numpy().astype(np.float64) for k, v in g.items()}, b
 
 
+@pytest.mark.parametrize("engine", ["persistent", "plain"])
 @pytest.mark.parametrize("kind", list(SCENES))
-def test_adjoint_matches_fp64_oracle(kind):
+def test_adjoint_matches_fp64_oracle(kind, engine):
+    """Both engines: the CTA-resident adjoint kernel after persistent frames, the per-launch
+    adjoint (rs_adjoint_plain.cu) after plain-engine frames."""
     kw, pk = SCENES[kind]
     kw = dict(material="c1", **kw)
     ob, pos = ac.scene(R=R, V=V, **kw)
@@ -93,8 +98,8 @@ def test_adjoint_matches_fp64_oracle(kind):
     L64, g64 = ac.oracle_loss_and_grad(ob, progs, tgt, DT, S, V)
     ob32, _ = ac.scene(R=R, V=V, precision="f32", **kw)
     _, g32 = ac.oracle_loss_and_grad(ob32, progs, tgt, DT, S, V)
-    L, g, _ = _gpu_loss_and_grad(pos, progs, tgt, **kw)
-    print(f"\n  [{kind}] loss gpu {L:.8e} fp64 {L64:.8e}")
+    L, g, _ = _gpu_loss_and_grad(pos, progs, tgt, engine=engine, **kw)
+    print(f"\n  [{kind}, {engine}] loss gpu {L:.8e} fp64 {L64:.8e}")
     assert abs(L - L64) <= 1e-4 * abs(L64)
     for k in GROUPS:
         e_gpu = ac.rel(g[k], g64[k])
@@ -195,26 +200,23 @@ def test_differentiable_frame_forward_is_the_step():
         assert float((xa - st[0]).abs().max()) <= 1e-5
 
 
-def test_adjoint_refuses_contact_groups_larger_than_a_cta():
-    """The adjoint runs each rope-rope contact group inside one CTA; a group of 20 x 64 = 1280
-    vertices runs the plain engine forward and is refused, by the taped step or the backward."""
+def test_adjoint_refuses_moving_meshes():
+    """Mesh poses are differentiated as constants: a frame with pending mesh targets (a mesh
+    that moves during it) is refused, by the taped step or the backward."""
     import torch
 
     import ropesim.grad as rg
 
-    Rg, Vg = 20, 64
-    _, pos = ac.scene(R=Rg, V=Vg, plane=False, material="c1")
+    _, pos = ac.scene(R=R, V=V, plane=False, material="c1")
     progs = ac.programs(pos, 1)
-    b = _gpu_batch(pos, plane=False)
-    b.set_rope_contact(True, 2e-3, 1e-3, 1e-5, 0.1, 5.0, 1.2, Rg)
+    b = _gpu_batch(pos, plane=False, mesh=True)
+    _, mp, quat = ac.mesh_setup(pos)
+    b.set_mesh_poses(0, mp + np.float32(0.01), quat)
     st = [t.requires_grad_() for t in rg.state(b)]
     par = rg.parameters(b)
     p0, v0, p1 = (torch.tensor(x[0], device="cuda") for x in progs)
-    with pytest.raises(ValueError, match="fit one CTA"):
+    with pytest.raises(ValueError, match="static meshes"):
         out = rg.frame(b, st, par, p0, v0, p1, DT, 10)
-        out[0].sum().backward()
-    with pytest.raises(ValueError, match="fit one CTA"):
-        out = rg.frame(b, st, par, p0, v0, p1, DT, 10, tape=False)
         out[0].sum().backward()
 
 
@@ -235,14 +237,23 @@ ROPE_SCENES = {
 }
 
 
+@pytest.mark.parametrize("engine", ["persistent", "plain", "oversize_group"])
 @pytest.mark.parametrize("kind", list(ROPE_SCENES))
-def test_rope_contact_adjoint_matches_fp64_oracle(kind):
+def test_rope_contact_adjoint_matches_fp64_oracle(kind, engine):
+    """Rope-rope contact through the CTA-resident adjoint (persistent), the per-launch adjoint
+    after plain frames (plain), and the per-launch adjoint that a contact group larger than one
+    CTA takes by itself (oversize_group: ten crossings of 52-vertex ropes in one group of
+    20 ropes, 1040 vertices)."""
     import torch
 
     import ropesim.grad as rg
 
     kw, dt, S_, F_, pk = ROPE_SCENES[kind]
     Rr, Vr = 2, 10
+    if engine == "oversize_group":
+        Vr = 52
+        kw = dict(kw, pairs=10)
+        Rr = 20
     ob, pos = ac.rope_crossing(V=Vr, **kw)
     progs = ac.programs(pos, F_, **pk)
     tgt = ac.targets(pos, F_)
@@ -252,6 +263,8 @@ def test_rope_contact_adjoint_matches_fp64_oracle(kind):
     ob32, _ = ac.rope_crossing(V=Vr, precision="f32", **kw)
     L32, g32 = ac.oracle_loss_and_grad(ob32, progs, tgt, dt, S_, Vr, w_end=w_end)
     b, _ = ac.rope_crossing(V=Vr, backend="cuda", **kw)
+    if engine == "plain":
+        b.set_engine("plain")
     st = [t.clone().requires_grad_() for t in rg.state(b)]
     par = [t.clone().requires_grad_() for t in rg.parameters(b)]
     P = [torch.tensor(a, device="cuda", requires_grad=True) for a in progs]
@@ -268,7 +281,7 @@ def test_rope_contact_adjoint_matches_fp64_oracle(kind):
          "g_mass": par[2].grad, "g_pos": st[0].grad, "g_vel": st[1].grad, "g_lvel": st[2].grad, "g_q": st[3].grad}
     g = {k: v.detach().cpu().numpy().astype(np.float64) for k, v in g.items()}
     L = float(loss.detach())
-    print(f"\n  [{kind}] loss gpu {L:.8e} fp64 {L64:.8e} fp32-oracle {L32:.8e}")
+    print(f"\n  [{kind}, {engine}] loss gpu {L:.8e} fp64 {L64:.8e} fp32-oracle {L32:.8e}")
     assert abs(L - L64) <= max(1e-4 * abs(L64), 4 * abs(L32 - L64))
     for k in GROUPS:
         if np.linalg.norm(g64[k]) == 0.0:  # one substep: v0 cancels from the root's velocity exactly
