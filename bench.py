@@ -635,6 +635,162 @@ def run_config4(args):
     print(json.dumps(line), flush=True)
 
 
+def config5_scene(R=256, V=128, seed=5):
+    """Config 5 stand-in (seeded): R free ropes of V vertices, 1 cm segments (density 0.117 kg/m),
+    per-rope EA log-uniform [1e2, 1e3] N and EI log-uniform [1e-5, 1e-3] N m^2 (at 8 sweeps the
+    adjoint of stiffer stretch, k / (m / h^2) above ~7 or EA above ~3e3 N here, grows without bound:
+    the Jacobi map's linearisation is unstable there, in FP64 as well), dropped in layers of
+    8 parallel straight ropes 15 mm apart in z (each layer a random rotation about z and a random
+    offset within a 0.3 m footprint; ropes 4 cm apart within a layer, so no pair starts closer than
+    the 10 mm contact distance; the lowest layer 5 cm up), onto the plane z = 0 inside a shallow
+    spherical bowl (radius 6 m, its lowest point 5 cm below the plane, rising to 8 cm above it at
+    the lattice edge) baked to a 128^3 lattice. Returns (positions [R, V, 3],
+    EA [R], EI [R], lattice args)."""
+    sys.path.insert(0, PKG)
+    from ropesim import sdf
+
+    rng = np.random.default_rng(seed)
+    seg, per_layer = 0.01, 8
+    layers = (R + per_layer - 1) // per_layer
+    pos = np.zeros((R, V, 3), np.float32)
+    t = (np.arange(V) - (V - 1) / 2) * seg
+    for r in range(R):
+        L, k = r // per_layer, r % per_layer
+        if k == 0:
+            th = rng.uniform(0, np.pi)
+            off = rng.uniform(-0.05, 0.05, 2)
+            d, nrm = np.array([np.cos(th), np.sin(th)]), np.array([-np.sin(th), np.cos(th)])
+        c = off + nrm * (k - (per_layer - 1) / 2) * 0.04
+        pos[r, :, 0] = c[0] + d[0] * t
+        pos[r, :, 1] = c[1] + d[1] * t
+        pos[r, :, 2] = 0.05 + 0.015 * L
+    ea = np.exp(rng.uniform(np.log(1e2), np.log(1e3), R)).astype(np.float32)
+    ei = np.exp(rng.uniform(np.log(1e-5), np.log(1e-3), R)).astype(np.float32)
+    sp = 0.0165  # 128 nodes per axis: 2.0955 m
+    lo = np.array([-1.05, -1.05, -0.25])
+    g = sdf.from_function(sdf.sdf_bowl(6.0, centre=(0.0, 0.0, 5.95)), lo, lo + 126.5 * sp, sp)
+    assert g.values.shape == (128, 128, 128)
+    phi = sdf.sdf_bowl(6.0, centre=(0.0, 0.0, 5.95))(pos.reshape(-1, 3))
+    assert phi.min() > 0.02, "a rope starts outside the bowl"
+    return pos, ea, ei, g.as_args()
+
+
+def run_config5(args):
+    """Config 5: contact-heavy forward + backward. 256 x 128 free ropes (config5_scene) with one
+    rope-rope contact group of all ropes (radius 0.9 R, barrier 0.2 R for R = 5 mm, k_collision
+    0.025, mu 0.4, k_friction 1e7), the plane z = 0 and the bowl (R = 5 mm, mu_s 0.5, mu_k 0.4);
+    dt 1/60, 100 substeps, 8 iterations. The group (32,768 vertices) is larger than a CTA, so frames
+    run the per-substep-launch path and the backward the per-launch adjoint. Stiffness fitting:
+    targets are the rollout with the seeded per-rope EA / EI; one step = one --frames rollout from
+    the perturbed estimate (forward with tapes, trajectory loss, backward) and one Adam step on
+    per-rope log EA / log EI. Reported: fitting steps/s and forward + backward vertex-substeps/s,
+    the forward-only rollout, and with --fit-steps N the parameter errors after N steps."""
+    import torch
+
+    import ropesim
+    import ropesim.grad as rg
+
+    torch.cuda.set_device(0)
+    R = args.ropes if args.ropes != 4096 else 256
+    V, F, S5 = 128, args.frames, 100
+    pos, ea_true, ei_true, lattice = config5_scene(R, V)
+    Rc = 0.005
+    b = ropesim.RopeBatch.from_positions(pos, 0.117, 1000.0, 1e-3, 1 / 6000, ITERS, pinned=np.zeros(V, bool))
+    b.set_gravity(np.array([0, 0, -9.81], np.float32))
+    b.damping = 0.0
+    b.drag = 0.2
+    b.set_planes(np.array([[0.0, 0.0, 1.0, 0.0]], np.float32), radius=Rc, mu_s=0.5, mu_k=0.4)
+    b.set_contact(Rc, mu_s=0.5, mu_k=0.4)
+    b.add_mesh(*lattice, pos=np.zeros((R, 3), np.float32), quat=np.tile(np.float32([0, 0, 0, 1]), (R, 1)), mu_s=0.5, mu_k=0.4)
+    b.set_rope_contact(True, radius=0.9 * Rc, barrier=0.2 * Rc, k_collision=0.025, mu=0.4, k_friction=1e7, group_ropes=R)
+    st0 = rg.state(b)
+    _, _, mass = rg.parameters(b)
+    n = R * V
+    seg_mask = torch.ones(R, V, device="cuda")
+    seg_mask[:, -1] = 0.0
+
+    def per_vertex(x):  # per-rope values onto the vertices that own a segment
+        return (x[:, None] * seg_mask).reshape(n)
+
+    true_ea = torch.tensor(ea_true, device="cuda")
+    true_ei = torch.tensor(ei_true, device="cuda")
+    with torch.no_grad():  # the trajectories the method itself generates, with the seeded parameters
+        cur, traj = st0, []
+        for f in range(F):
+            cur = rg.frame(b, cur, (per_vertex(true_ea), per_vertex(true_ei), mass), None, None, None, DT, S5)
+            traj.append(cur[0].clone())
+    drop = float((st0[0][:, 2] - traj[-1][:, 2]).mean())
+    rng = np.random.default_rng(6)
+    log_ea = torch.tensor(np.log(ea_true) + rng.normal(0, 0.3, R), device="cuda", dtype=torch.float32, requires_grad=True)
+    log_ei = torch.tensor(np.log(ei_true) + rng.normal(0, 0.3, R), device="cuda", dtype=torch.float32, requires_grad=True)
+    opt = torch.optim.Adam([log_ea, log_ei], lr=0.05, eps=1e-12)
+
+    def errors():
+        with torch.no_grad():
+            e_ea = (log_ea.exp() / true_ea).log().abs().median()
+            e_ei = (log_ei.exp() / true_ei).log().abs().median()
+        return float(e_ea), float(e_ei)
+
+    info = {}
+
+    def fit_step():
+        opt.zero_grad(set_to_none=True)
+        cur, loss = st0, 0.0
+        par = (per_vertex(log_ea.exp()), per_vertex(log_ei.exp()), mass)
+        for f in range(F):
+            cur = rg.frame(b, cur, par, None, None, None, DT, S5)
+            loss = loss + ((cur[0] - traj[f]) ** 2).sum(-1).mean() * 1e6  # mm^2
+        loss.backward()
+        info["loss"] = float(loss.detach())
+        info["finite"] = bool(torch.isfinite(log_ea.grad).all() and torch.isfinite(log_ei.grad).all())
+        opt.step()
+
+    def fwd_only():
+        b.set_state(*st0)
+        for f in range(F):
+            b.step_free(DT, S5)
+
+    def timed(fn, k):
+        ms = []
+        for _ in range(k):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    err0 = errors()
+    timed(fit_step, args.warmup)
+    loss_first = info["loss"]
+    msb = timed(fit_step, args.steps)
+    fit = {"steps_done": args.warmup + args.steps}
+    if args.fit_steps > fit["steps_done"]:
+        timed(fit_step, args.fit_steps - fit["steps_done"])
+        fit["steps_done"] = args.fit_steps
+    err1 = errors()
+    fit.update({"loss_first_step": loss_first, "loss_last_step": info["loss"], "grads_finite": info["finite"],
+                "median_abs_log_error_ea": [err0[0], err1[0]], "median_abs_log_error_ei": [err0[1], err1[1]]})
+    timed(fwd_only, 1)
+    msf = timed(fwd_only, max(1, min(args.steps, 3)))
+    ms_step = float(np.mean(msb))
+    line = {"metric": "stiffness-fitting steps/s (forward + backward)", "value": 1e3 / ms_step, "unit": "steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config-5 pile: layered drop into a baked bowl)",
+            "config": {"workload": f"config5-contact-{R}x{V}", "ropes": R, "verts_per_rope": V, "frames": F,
+                       "substeps": S5, "num_itr": ITERS, "contact_group_vertices": n,
+                       "step": f"one fitting step: {F}-frame rollout with tapes, trajectory loss, backward, Adam on "
+                               "per-rope log EA / log EI", "engine": "per-substep launches (group larger than a CTA)",
+                       "mean_drop_m": drop},
+            "fwd_bwd_vertex_substeps_per_s": n * S5 * F / (ms_step * 1e-3),
+            "forward_only": {"ms_per_rollout": float(np.mean(msf)), "value": n * S5 * F / (float(np.mean(msf)) * 1e-3)},
+            "fwd_bwd_over_fwd": ms_step / float(np.mean(msf)), "fit": fit}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_ROPES
     ap = argparse.ArgumentParser()
@@ -649,7 +805,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
     ap.add_argument("--frames", type=int, default=30, help="config4: control frames per rollout")
     ap.add_argument("--no-tape", action="store_true", help="config4: backward replays frames instead of keeping tapes")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
+    ap.add_argument("--fit-steps", type=int, default=0, help="config5: total fitting steps to run (e.g. 50)")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
                     help="config2 (the headline line), config3 (uneven ropes, planes and meshes vs the plain path) "
                          "or config4 (differentiable rollouts: forward and forward + backward)")
     args = ap.parse_args()
@@ -662,6 +819,8 @@ def main():
         run_config3(args)
     elif args.workload == "config4":
         run_config4(args)
+    elif args.workload == "config5":
+        run_config5(args)
     else:
         run_ours(args)
 

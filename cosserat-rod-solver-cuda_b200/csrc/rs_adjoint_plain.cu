@@ -590,12 +590,13 @@ inline int blocks_of(int n, int t) { return (n + t - 1) / t; }
 
 template <int SURF, bool ROPE>
 void run_adjoint_plain(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs& b, int n, int iters, int substeps,
-                       cudaStream_t st) {
+                       const RopeGrid* grid, cudaStream_t st) {
     const int nb = blocks_of(n, kBlock);
     padj_load_kernel<<<nb, kBlock, 0, st>>>(pa, g, b, n);
     for (int s = substeps - 1; s >= 0; s--) {
         padj_init_kernel<<<nb, kBlock, 0, st>>>(pa, g, b, n, s);
-        if (ROPE) padj_detect_kernel<<<nb, kBlock, 0, st>>>(pa, b, n);
+        if (ROPE && grid) rope_grid_detect(pa, b.x, *grid, n, false, st);
+        else if (ROPE) padj_detect_kernel<<<nb, kBlock, 0, st>>>(pa, b, n);
         for (int k = 0; k < iters; k++) {
             padj_position_kernel<SURF, ROPE><<<blocks_of(n, kOwned), kPosBlock, 0, st>>>(pa, b, n, k);
             padj_frame_kernel<<<nb, kBlock, 0, st>>>(pa, b, n, k);
@@ -614,10 +615,10 @@ void run_adjoint_plain(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs
 
 template <bool ROPE>
 void run_adjoint_plain_s(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs& b, int n, int iters, int substeps,
-                         int surf, cudaStream_t st) {
-    if (surf == SURF_MESHES) run_adjoint_plain<SURF_MESHES, ROPE>(pa, g, b, n, iters, substeps, st);
-    else if (surf == SURF_PLANES) run_adjoint_plain<SURF_PLANES, ROPE>(pa, g, b, n, iters, substeps, st);
-    else run_adjoint_plain<SURF_NONE, ROPE>(pa, g, b, n, iters, substeps, st);
+                         int surf, const RopeGrid* grid, cudaStream_t st) {
+    if (surf == SURF_MESHES) run_adjoint_plain<SURF_MESHES, ROPE>(pa, g, b, n, iters, substeps, grid, st);
+    else if (surf == SURF_PLANES) run_adjoint_plain<SURF_PLANES, ROPE>(pa, g, b, n, iters, substeps, grid, st);
+    else run_adjoint_plain<SURF_NONE, ROPE>(pa, g, b, n, iters, substeps, grid, st);
 }
 
 }  // namespace
@@ -647,9 +648,9 @@ PlainAdjBufs adjoint_plain_carve(float4* base, int n, int iters) {
 }
 
 cudaError_t launch_adjoint_plain(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs& b, int n, int iters,
-                                 int substeps, int surf, bool rope, cudaStream_t st) {
-    if (rope) run_adjoint_plain_s<true>(pa, g, b, n, iters, substeps, surf, st);
-    else run_adjoint_plain_s<false>(pa, g, b, n, iters, substeps, surf, st);
+                                 int substeps, int surf, bool rope, const RopeGrid* grid, cudaStream_t st) {
+    if (rope) run_adjoint_plain_s<true>(pa, g, b, n, iters, substeps, surf, grid, st);
+    else run_adjoint_plain_s<false>(pa, g, b, n, iters, substeps, surf, grid, st);
     return cudaGetLastError();
 }
 

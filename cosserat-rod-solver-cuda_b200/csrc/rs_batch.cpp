@@ -119,7 +119,7 @@ Batch::~Batch() {
     if (pl_graph_) cudaGraphExecDestroy(pl_graph_);
     void* pbufs[] = {pl_.dx, pl_.dxn, pl_.y, pl_.qprev, pl_.lpos, pl_.facc, pl_.cand, pl_.spose, d_pl_args_,
                      d_grp_, d_cols_, d_ncols_, d_maxstep_, d_pad_, gs_pos_, gs_vel_, gs_lvel_, gs_q_, gs_buf_, d_tape_,
-                     d_padj_, d_adj_args_};
+                     d_padj_, d_adj_args_, grid_mem_};
     for (void* p : pbufs)
         if (p) cudaFree(p);
     if (h_pl_args_) cudaFreeHost(h_pl_args_);
@@ -575,6 +575,32 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     host_dyn_valid_ = false;
 }
 
+// The grid broad phase serves contact groups larger than one CTA (the brute force's O(V²) pairs
+// per substep dominate there); groups that fit a CTA keep the brute force, as the reference.
+const RopeGrid* Batch::rope_grid() {
+    if (!oversize_) return nullptr;
+    if (!grid_mem_) {
+        RopeGrid g{};
+        g.T = rope_grid_buckets(n_);
+        g.scan_bytes = rope_grid_scan_bytes(g.T);
+        const size_t N = (size_t)n_, T = (size_t)g.T;
+        // seven sub-buffers, each rounded up to 256 bytes
+        const size_t bytes = sizeof(float4) * N + sizeof(int) * (2 * N + 2 * (T + 1)) + sizeof(unsigned) + g.scan_bytes + 8 * 256;
+        check(cudaMalloc(&grid_mem_, bytes), "cudaMalloc(rope grid)");
+        char* p = static_cast<char*>(grid_mem_);
+        auto take = [&](size_t sz) { char* r = p; p += (sz + 255) & ~size_t(255); return r; };
+        g.ms = reinterpret_cast<float4*>(take(sizeof(float4) * N));
+        g.bucket = reinterpret_cast<int*>(take(sizeof(int) * N));
+        g.sorted = reinterpret_cast<int*>(take(sizeof(int) * N));
+        g.count = reinterpret_cast<int*>(take(sizeof(int) * (T + 1)));
+        g.start = reinterpret_cast<int*>(take(sizeof(int) * (T + 1)));
+        g.smax = reinterpret_cast<unsigned*>(take(sizeof(unsigned)));
+        g.scan_tmp = take(g.scan_bytes);
+        grid_ = g;
+    }
+    return &grid_;
+}
+
 // ------------------------------------------------------------------ plain engine
 void Batch::set_engine(int e) {
     if (e != 0 && e != 1) throw std::invalid_argument("engine must be 0 (persistent) or 1 (plain)");
@@ -621,7 +647,7 @@ void Batch::run_frame_plain(const FrameArgs& a) {
     }
     for (int s = 0; s < a.substeps; s++) {
         check(plain_launch_pre(d_pl_args_, pl_, n_, R_, R_, a.num_sdf, a.sdf_moving != 0, a.root_mode, a.rope_contact != 0, s,
-                               stream_),
+                               a.rope_contact ? rope_grid() : nullptr, stream_),
               "plain substep prologue");
         check(cudaGraphLaunch(pl_graph_, stream_), "plain graph launch");
     }
@@ -1204,10 +1230,11 @@ void Batch::step_program_taped(const float* p0, const float* v0, const float* p1
 float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synchronize) {
     if (!(dt > 0.f)) throw std::invalid_argument("dt must be > 0");
     if (substeps < 1) throw std::invalid_argument("substeps must be >= 1");
-    if (!io.pos || !io.vel || !io.lvel || !io.q || !io.p0 || !io.v0 || !io.p1)
-        throw std::invalid_argument("the frame-start state and the program rows are required");
+    if (!io.pos || !io.vel || !io.lvel || !io.q) throw std::invalid_argument("the frame-start state is required");
+    if ((io.p0 != nullptr) != (io.v0 != nullptr) || (io.p0 != nullptr) != (io.p1 != nullptr))
+        throw std::invalid_argument("a program frame needs p0, v0 and p1 (all NULL: a free frame)");
     if (!io.o_pos || !io.o_vel || !io.o_lvel || !io.o_q) throw std::invalid_argument("the end-state outputs are required");
-    if (!roots_pinned()) throw std::invalid_argument("the program frame drives every rope's root");
+    if (io.p0 && !roots_pinned()) throw std::invalid_argument("the program frame drives every rope's root");
     if (io.tape) {
         if (!grids_.empty() && pending_set_) throw std::invalid_argument("the adjoint differentiates static meshes only: no mesh pose targets may be pending in a differentiated frame");
     }
@@ -1220,11 +1247,11 @@ float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synch
               "frame parameters");
         host_const_stale_ = true;
     }
-    stage_rows(io.p0, io.v0, io.p1, nullptr, nullptr, false);
+    if (io.p0) stage_rows(io.p0, io.v0, io.p1, nullptr, nullptr, false);
     sdf_begin();
     const float last = h_;
     pending_tape_ = reinterpret_cast<float4*>(io.tape);
-    run_frame(ROOT_PROGRAM, false, false, dt, substeps, dt / (float)substeps);
+    run_frame(io.p0 ? ROOT_PROGRAM : ROOT_NONE, false, false, dt, substeps, dt / (float)substeps);
     pending_tape_ = nullptr;
     time_ += dt;
     sdf_end(substeps);
@@ -1314,7 +1341,7 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
         check(cudaMemcpyAsync(d_adj_args_, h_adj_args_, sizeof(FrameArgs), cudaMemcpyHostToDevice, stream_), "upload(args)");
         const int surf = a.num_sdf > 0 ? 2 : (a.num_planes > 0 ? 1 : 0);
         check(launch_adjoint_plain(d_adj_args_, g, adjoint_plain_carve(d_padj_, n_, num_itr), n_, num_itr, substeps, surf,
-                                   rope_contact_, stream_),
+                                   rope_contact_, rope_contact_ ? rope_grid() : nullptr, stream_),
               "adjoint (per launch)");
     } else {
         check(launch_adjoint(a, g, block_, (int)bins_.size(), stream_), "adjoint");

@@ -308,6 +308,10 @@ private:
     size_t padj_words_ = 0;
     FrameArgs* d_adj_args_ = nullptr;
     FrameArgs* h_adj_args_ = nullptr;  // pinned staging of the backward's frame parameters
+    // grid broad phase of contact groups larger than one CTA (null until first needed)
+    RopeGrid grid_{};
+    void* grid_mem_ = nullptr;
+    const RopeGrid* rope_grid();
 };
 
 }  // namespace rs

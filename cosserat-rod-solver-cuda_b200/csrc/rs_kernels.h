@@ -25,7 +25,12 @@ cudaError_t launch_scale(float* x, int n, float k, cudaStream_t s);
 cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, int iters, int surf, bool rope,
                                cudaStream_t s);
 cudaError_t plain_launch_pre(const FrameArgs* pa, const PlainBufs& b, int n, int nropes, int envs, int num_sdf, bool moving,
-                             int root_mode, bool rope, int s, cudaStream_t st);
+                             int root_mode, bool rope, int s, const RopeGrid* grid, cudaStream_t st);
+// Rope-rope detection through a uniform grid (rs_ropegrid.cu), the brute force's candidate lists,
+// for contact groups larger than one CTA: `pos` the substep-start positions (device order).
+int rope_grid_buckets(int n);
+size_t rope_grid_scan_bytes(int T);
+cudaError_t rope_grid_detect(const FrameArgs* pa, const float4* pos, const RopeGrid& g, int n, bool flag, cudaStream_t st);
 cudaError_t plain_launch_finish(const FrameArgs* pa, const PlainBufs& b, int n, cudaStream_t st);
 // Device address of the library's static rope-rope candidate array on the current device and
 // its capacity in vertices (looked up once per device, then cached; no allocation).
@@ -40,7 +45,7 @@ size_t adjoint_smem_bytes(int block, int iters, bool rope);
 size_t adjoint_plain_words(int n, int iters);
 PlainAdjBufs adjoint_plain_carve(float4* base, int n, int iters);
 cudaError_t launch_adjoint_plain(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs& b, int n, int iters,
-                                 int substeps, int surf, bool rope, cudaStream_t st);
+                                 int substeps, int surf, bool rope, const RopeGrid* grid, cudaStream_t st);
 // Caller-order state <-> device order (the .w constants of cst_* are kept).
 cudaError_t launch_state_in(const int4* topo, const float* pos, const float* vel, const float* lvel, const float* q,
                             const float4* cst_pos, const float4* cst_vel, const float4* cst_lvel, float4* o_pos,

@@ -94,22 +94,10 @@ __global__ void plain_detect_kernel(const FrameArgs* __restrict__ pa, PlainBufs 
         return;
     }
     const int4 gr = a.grp[d];
-    const f3 p = xyz(b.lpos[d]), a1 = xyz(b.lpos[d + 1]) - p;
-    const float ri = fmaxf(a.pad[d], a.pad[d + 1]);
-    float lim = a.pad[d] - a.det_radius;
-    int cnt = 0;
-    for (int j = gr.x; j < gr.y; j++) {
-        if (!(a.topo[j].x & F_NEXT)) continue;
-        if (j >= gr.z && j < gr.w && abs(j - d) <= 2) continue;
-        const f3 pj0 = xyz(b.lpos[j]), pj1 = xyz(b.lpos[j + 1]);
-        if (rope_pair_candidate(p, a1, ri, pj0, pj1, fmaxf(a.pad[j], a.pad[j + 1]))) {
-            if (cnt < kMaxCols) {
-                a.cols[(size_t)cnt * n + d] = j;
-                lim = fminf(lim, step_limit_of(p, a1, pj0, pj1));
-            }
-            cnt++;
-        }
-    }
+    float lim;
+    const int cnt = detect_group(
+        a, d, d, gr.x, gr.y, gr.z, gr.w, xyz(b.lpos[d]), xyz(b.lpos[d + 1]), [&](int j) { return a.pad[j]; },
+        [&](int j) { return a.topo[j].x; }, [&](int j) { return xyz(b.lpos[j]); }, lim);
     if (cnt > kMaxCols) atomicMax(a.status, ERR_MAX_COLLISIONS);
     a.ncols[d] = cnt < kMaxCols ? cnt : kMaxCols;
     a.maxstep[d] = lim;
@@ -275,12 +263,17 @@ cudaError_t plain_record_inner(const FrameArgs* pa, const PlainBufs& b, int n, i
 }
 
 cudaError_t plain_launch_pre(const FrameArgs* pa, const PlainBufs& b, int n, int nropes, int envs, int num_sdf, bool moving,
-                             int root_mode, bool rope, int s, cudaStream_t st) {
+                             int root_mode, bool rope, int s, const RopeGrid* grid, cudaStream_t st) {
     if (root_mode != ROOT_NONE && (root_mode == ROOT_PROGRAM || s == 0))
         plain_root_kernel<<<blocks_of(nropes, 128), 128, 0, st>>>(pa, nropes, s);
     if (num_sdf > 0 && moving) plain_pose_kernel<<<blocks_of(envs * num_sdf, 128), 128, 0, st>>>(pa, b, envs, s);
     plain_init_kernel<<<blocks_of(n, 256), 256, 0, st>>>(pa, b, n, s);
-    if (rope) plain_detect_kernel<<<blocks_of(n, 128), 128, 0, st>>>(pa, b, n);
+    if (rope && grid) {
+        const cudaError_t e = rope_grid_detect(pa, b.lpos, *grid, n, true, st);
+        if (e != cudaSuccess) return e;
+    } else if (rope) {
+        plain_detect_kernel<<<blocks_of(n, 128), 128, 0, st>>>(pa, b, n);
+    }
     return cudaGetLastError();
 }
 

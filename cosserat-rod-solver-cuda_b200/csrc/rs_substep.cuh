@@ -307,18 +307,36 @@ __device__ __forceinline__ float position_solve_limited(f3& dx, f3 f, const sym3
 // (padding - detection radius, and 0.45 x each listed candidate's distance), batch.cu:19-49 and
 // collision.cu:103-136. pad(j), flg(j) and pos(j) read the group's padded radii, flags and
 // substep-start positions. Returns the number of candidates found (the list keeps kMaxCols).
+//
+// Before the closest-point test each pair passes a conservative early out: the centre lines of
+// segments with midpoints m_t, m_j and half-lengths h_t, h_j are at least |m_t - m_j| - h_t - h_j
+// apart, so a pair with |m_t - m_j| > (h_t + h_j + r) (1 + 1e-4) + 1e-6 m (r the sum of the padded
+// radii) cannot pass the test, whose FP32 distance errs by far less than that margin at these
+// separations. The candidate lists are those of the plain brute force, pair for pair.
+// The pair test of detect_group (segment (p, p + a1) with midpoint mt, half-length ht and padded
+// radius ri against segment (pj0, pj1) with radius rj), shared with the grid broad phase.
+__device__ __forceinline__ bool pair_accepts(f3 p, f3 a1, f3 mt, float ht, float ri, f3 pj0, f3 pj1, float rj) {
+    const f3 dm = (pj0 + pj1) * 0.5f - mt;
+    const float reach = (ht + 0.5f * len(pj1 - pj0) + ri + rj) * 1.0001f + 1e-6f;
+    if (dot(dm, dm) > reach * reach) return false;
+    return rope_pair_candidate(p, a1, ri, pj0, pj1, rj);
+}
+
 template <class Pad, class Flg, class Pos>
 __device__ __forceinline__ int detect_group(const FrameArgs& a, int t, int dv, int g0, int g1, int r0, int r1, f3 p, f3 p1,
                                            Pad pad, Flg flg, Pos pos, float& lim) {
     const f3 a1 = p1 - p;
     const float ri = fmaxf(pad(t), pad(t + 1));
+    const f3 mt = p + a1 * 0.5f;
+    const float ht = 0.5f * len(a1);
     lim = pad(t) - a.det_radius;
     int cnt = 0;
     for (int j = g0; j < g1; j++) {
         if (!(flg(j) & F_NEXT)) continue;
         if (j >= r0 && j < r1 && abs(j - t) <= 2) continue;
         const f3 pj0 = pos(j), pj1 = pos(j + 1);
-        if (rope_pair_candidate(p, a1, ri, pj0, pj1, fmaxf(pad(j), pad(j + 1)))) {
+        const float rj = fmaxf(pad(j), pad(j + 1));
+        if (pair_accepts(p, a1, mt, ht, ri, pj0, pj1, rj)) {
             if (cnt < kMaxCols) {
                 a.cols[(size_t)cnt * a.n + dv] = j;
                 lim = fminf(lim, step_limit_of(p, a1, pj0, pj1));

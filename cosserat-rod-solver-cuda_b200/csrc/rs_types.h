@@ -178,6 +178,20 @@ struct PlainAdjBufs {
     float4* qp;                 // quadratic-drag share on the previous vertex's frame
 };
 
+// Uniform-grid broad phase of rope-rope detection for contact groups larger than one CTA:
+// segment midpoints hashed into cells of twice the largest reach, counting-sorted by bucket.
+struct RopeGrid {
+    float4* ms;        // [n] segment midpoint and reach (half length + padded radius); w < 0: no segment
+    int* bucket;       // [n] hash bucket of the segment's cell (-1: no segment)
+    int* count;        // [T + 1] bucket counts, then fill cursors
+    int* start;        // [T + 1] exclusive scan of the counts
+    int* sorted;       // [n] segments by bucket
+    unsigned* smax;    // the largest reach (float bits)
+    void* scan_tmp;    // CUB scan scratch
+    size_t scan_bytes;
+    int T;             // buckets, a power of two
+};
+
 struct PlainBufs {
     float4* dx;       // displacement iterate
     float4* dxn;      // next iterate (Jacobi output)

@@ -78,11 +78,15 @@ class Frame(torch.autograd.Function):
     @staticmethod
     def forward(ctx, batch, dt, substeps, tape, pos, vel, lvel, q, ea, ei, mass, p0, v0, p1):
         n, R = _n(batch), int(batch.num_envs)
-        ctx.shapes = [tuple(t.shape) for t in (pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)]
+        ctx.shapes = [None if t is None else tuple(t.shape) for t in (pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)]
+        ctx.free = p0 is None
         pos, vel, lvel = (_check(t, (n, 3), k) for t, k in ((pos, "pos"), (vel, "vel"), (lvel, "lvel")))
         q = _check(q, (n, 4), "q")
         ea, ei, mass = (_check(t, (n,), k) for t, k in ((ea, "ea"), (ei, "ei"), (mass, "mass")))
-        p0, v0, p1 = (_check(t, (R, 3), k) for t, k in ((p0, "p0"), (v0, "v0"), (p1, "p1")))
+        if (p0 is None) != (v0 is None) or (p0 is None) != (p1 is None):
+            raise ValueError("a program frame needs p0, v0 and p1 (all None: a free frame)")
+        if p0 is not None:
+            p0, v0, p1 = (_check(t, (R, 3), k) for t, k in ((p0, "p0"), (v0, "v0"), (p1, "p1")))
         out = [torch.empty(n, k, device="cuda", dtype=torch.float32) for k in (3, 3, 3, 4)]
         # the frame's substep tape (64 B per vertex-substep) lets the backward skip the replay
         ctx.tape = torch.empty(16 * int(substeps) * n, device="cuda", dtype=torch.float32) if tape else None
@@ -100,12 +104,12 @@ class Frame(torch.autograd.Function):
     def backward(ctx, g_pos, g_vel, g_lvel, g_q):
         pos, vel, lvel, q, ea, ei, mass, p0, v0, p1 = ctx.saved_tensors
         b = ctx.batch
-        n, R = pos.shape[0], p0.shape[0]
+        n, R = pos.shape[0], int(b.num_envs)
         g_in = [None if g is None else g.detach().contiguous().to(torch.float32) for g in (g_pos, g_vel, g_lvel, g_q)]
         o = [torch.empty(n, 3, device="cuda", dtype=torch.float32) for _ in range(3)]
         o.append(torch.empty(n, 4, device="cuda", dtype=torch.float32))
         op = [torch.empty(n, device="cuda", dtype=torch.float32) for _ in range(3)]
-        og = [torch.empty(R, 3, device="cuda", dtype=torch.float32) for _ in range(3)]
+        og = [None] * 3 if ctx.free else [torch.empty(R, 3, device="cuda", dtype=torch.float32) for _ in range(3)]
         ptrs = [_ptr(t) for t in (pos, vel, lvel, q, p0, v0, p1, None, None)]
         ptrs += [_ptr(t) for t in g_in] + [_ptr(t) for t in o] + [_ptr(t) for t in op] + [_ptr(t) for t in og]
         ptrs += [_ptr(ctx.tape), _ptr(ea), _ptr(ei), _ptr(mass)]
@@ -114,7 +118,7 @@ class Frame(torch.autograd.Function):
         b._backward(ptrs, ctx.dt, ctx.substeps, ctx.last_h)
         cur.wait_stream(ext)
         ctx.tape = None
-        grads = [t.reshape(sh) for t, sh in zip(o + op + og, ctx.shapes)]
+        grads = [None if t is None else t.reshape(sh) for t, sh in zip(o + op + og, ctx.shapes)]
         return (None, None, None, None, *grads)
 
 
@@ -131,7 +135,8 @@ def _streams(batch):
 
 
 def frame(batch, st, params, p0, v0, p1, dt, substeps, tape=True):
-    """One differentiable control frame: returns the frame-end (pos, vel, lvel, q).
+    """One differentiable control frame: returns the frame-end (pos, vel, lvel, q). p0, v0, p1
+    ([R, 3] root program rows) all None make a free frame (no root driving, as step_free).
 
     tape=True keeps the frame's substep tape in device memory until the backward (64 B per
     vertex-substep: 420 MB for 65,536 vertices x 100 substeps), so the backward does not replay

@@ -237,11 +237,12 @@ typedef struct rs_backward_io {
 RS_API int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
 /* The same, returning with the work queued on the handle's stream (no host synchronization). */
 RS_API int rs_batch_backward_async(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
-/* One differentiable program frame in one call (device pointers, caller order): loads the
- * frame-start state and the parameters (NULL = keep), steps with the program rows p0 / v0 / p1
- * [R,3], writes the end state to out_* and, when tape != NULL (16 * substeps * n floats), the
- * substep tape for rs_batch_backward. *last_h receives the frame's lastH (RS_P_H before the
- * frame). Queued on the handle's stream without host synchronization. */
+/* One differentiable frame in one call (device pointers, caller order): loads the frame-start
+ * state and the parameters (NULL = keep), steps with the program rows p0 / v0 / p1 [R,3] (all
+ * three NULL: a free frame, as rs_batch_step_free), writes the end state to out_* and, when
+ * tape != NULL (16 * substeps * n floats), the substep tape for rs_batch_backward. *last_h
+ * receives the frame's lastH (RS_P_H before the frame). Queued on the handle's stream without
+ * host synchronization. */
 typedef struct rs_frame_io {
     const float *pos, *vel, *lvel, *q;
     const float *ea, *ei, *mass;

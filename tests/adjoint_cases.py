@@ -33,9 +33,9 @@ def mesh_setup(pos):
 
 
 def scene(R=8, V=16, seed=0, plane=True, damping=0.0, drag_quad=0.0, num_itr=8, precision="f64", material="c2",
-          clearance=0.004, mesh=False):
+          clearance=0.004, mesh=False, free=False):
     """R hanging ropes of V vertices, tips `clearance` above a plane at z = 0 (when `plane`), or
-    resting on a static mesh (when `mesh`, see mesh_setup)."""
+    resting on a static mesh (when `mesh`, see mesh_setup). `free`: no vertex pinned."""
     seg, density, ea, ei = MATERIALS[material]
     rng = np.random.default_rng(seed)
     pos = np.zeros((R, V, 3), np.float32)
@@ -44,7 +44,8 @@ def scene(R=8, V=16, seed=0, plane=True, damping=0.0, drag_quad=0.0, num_itr=8, 
         pos[r, :, 1] = 0.15 * (r // 4)
         pos[r, :, 2] = seg * (V - 1) + clearance - seg * np.arange(V)
         pos[r, 1:, :2] += rng.normal(0, 1e-3, (V - 1, 2)).astype(np.float32)
-    b = ro.RopeBatch.from_positions(pos, density, ea, ei, 1 / 6000, num_itr, precision=precision)
+    pins = np.zeros(V, bool) if free else None
+    b = ro.RopeBatch.from_positions(pos, density, ea, ei, 1 / 6000, num_itr, pinned=pins, precision=precision)
     b.set_gravity((0.0, 0.0, -9.81))
     b.damping = damping
     b.drag = 0.2
@@ -89,15 +90,22 @@ def oracle_loss_and_grad(b, progs, tgt, dt, S, V, w_end=None):
     Returns (loss, dict) with g_pos/g_vel/g_lvel/g_q of the initial state, g_ea/g_ei/g_mass per
     vertex and g_p0/g_v0/g_p1 [F, R, 3]."""
     s = b._s
-    P0, V0, P1 = progs
-    F, R = P0.shape[:2]
+    free = progs is None or (not isinstance(progs[0], np.ndarray) and progs[0] is None)
+    if free:  # free frames: progs = (None, None, None) or None, with F = len(tgt)
+        F, R = len(tgt), tgt.shape[1]
+    else:
+        P0, V0, P1 = progs
+        F, R = P0.shape[:2]
     n = s.n
     starts = []
     loss = 0.0
     tips = []
     for f in range(F):
         starts.append(s.get_state())
-        s.step_program_rows(np.concatenate([P0[f].ravel(), V0[f].ravel(), P1[f].ravel()]).astype(np.float64), dt, S)
+        if free:
+            s.step_free(dt, S)
+        else:
+            s.step_program_rows(np.concatenate([P0[f].ravel(), V0[f].ravel(), P1[f].ravel()]).astype(np.float64), dt, S)
         x = s.get_state()[0].reshape(R, V, 3)
         tips.append(x[:, -1])
         loss += ((x[:, -1] - tgt[f]) ** 2).sum(-1).mean()
@@ -115,11 +123,12 @@ def oracle_loss_and_grad(b, progs, tgt, dt, S, V, w_end=None):
     for f in range(F - 1, -1, -1):
         gx.reshape(R, V, 3)[:, -1] += 2.0 * (tips[f] - tgt[f]) / R
         s.set_state(*starts[f])
-        prog = np.concatenate([P0[f].ravel(), V0[f].ravel(), P1[f].ravel()]).astype(np.float64)
+        prog = None if free else np.concatenate([P0[f].ravel(), V0[f].ravel(), P1[f].ravel()]).astype(np.float64)
         g = s.frame_backward(prog, dt, S, gx, gv, glv, gq)
         gx, gv, glv, gq = g["x"], g["v"], g["lv"], g["q"]
         gks += g["ks"]; grho += g["rho"]; gw += g["w"]
-        gP[0][f], gP[1][f], gP[2][f] = g["P0"], g["V0"], g["P1"]
+        if not free:
+            gP[0][f], gP[1][f], gP[2][f] = g["P0"], g["V0"], g["P1"]
     s.set_state(*end)
     return loss, {
         "g_pos": gx, "g_vel": gv, "g_lvel": glv, "g_q": gq,
@@ -136,13 +145,14 @@ def rel(a, b):
 
 
 def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=0.1, precision="f64", backend="oracle",
-                  pairs=1):
+                  pairs=1, floor=None):
     """Two ropes of the "c1" material in one rope-rope contact group, crossing at right angles:
     rope 0 along x at z = 0 with both ends pinned (every vertex pinned when `static_bar`), rope 1
     along y, `gap` above it (centre to centre), pinned at its root. Contact radius 2 mm, barrier
     2 mm: the barrier acts while the centre lines are 4 to 6 mm apart. `backend` "cuda" builds
     the same scene on the GPU batch. `pairs` > 1 repeats the crossing along x (pair p shifted by
-    p x (V + 4) x 3 cm, clear of the others), all ropes in one contact group."""
+    p x (V + 4) x 3 cm, clear of the others), all ropes in one contact group. `floor` = z makes
+    every vertex free (no pins) and adds the plane z = floor with contact radius 2 mm."""
     seg, density, ea, ei = MATERIALS["c1"]
     rng = np.random.default_rng(seed)
     r0 = np.zeros((V, 3))
@@ -158,6 +168,9 @@ def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=
         pin0[:] = True
     pin1 = np.zeros(V, bool)
     pin1[0] = True
+    if floor is not None:
+        pin0[:] = False
+        pin1[:] = False
     ropes, pins = [], []
     for k in range(pairs):
         shift = np.array([k * (V + 4) * seg, 0.0, 0.0])
@@ -175,4 +188,6 @@ def rope_crossing(V=10, seed=0, num_itr=4, gap=0.005, static_bar=False, damping=
     b.drag = 0.2
     b.set_rope_contact(True, radius=0.002, barrier=0.002, k_collision=0.025, mu=0.1, k_friction=1e7,
                        group_ropes=2 * pairs)
+    if floor is not None:
+        b.set_planes(np.array([[0.0, 0.0, 1.0, floor]], np.float32), radius=0.002, mu_s=0.5, mu_k=0.3)
     return b, pos

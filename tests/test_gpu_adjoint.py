@@ -220,6 +220,57 @@ def test_adjoint_refuses_moving_meshes():
         out[0].sum().backward()
 
 
+@pytest.mark.parametrize("engine", ["persistent", "plain"])
+def test_free_frames_adjoint_matches_fp64_oracle(engine):
+    """Free frames (no root program: p0 = v0 = p1 = None): unpinned ropes thrown with seeded
+    vertex velocities N(0, 0.3) m/s; gradients w.r.t. EA, EI, mass and the initial state."""
+    import torch
+
+    import ropesim
+    import ropesim.grad as rg
+
+    kw = dict(material="c1", plane=False, free=True)
+    ob, pos = ac.scene(R=R, V=V, **kw)
+    vel0 = np.random.default_rng(4).normal(0, 0.3, (R * V, 3))
+    tgt = ac.targets(pos, F)
+    res = {}
+    for prec in ("f64", "f32"):
+        o, _ = ac.scene(R=R, V=V, precision=prec, **kw)
+        st = list(o._s.get_state())
+        st[1] = vel0.copy()
+        o._s.set_state(*st)
+        res[prec] = ac.oracle_loss_and_grad(o, None, tgt, DT, S, V)
+    (L64, g64), (_, g32) = res["f64"], res["f32"]
+    _, density, ea, ei = ac.MATERIALS["c1"]
+    b = ropesim.RopeBatch.from_positions(pos, density, ea, ei, 1 / 6000, 8, pinned=np.zeros(V, bool))
+    b.set_gravity(np.array([0.0, 0.0, -9.81], np.float32))
+    b.damping = 0.0
+    b.drag = 0.2
+    if engine == "plain":
+        b.set_engine("plain")
+    st = [t.clone() for t in rg.state(b)]
+    st[1] = torch.tensor(vel0, device="cuda", dtype=torch.float32)
+    st = [t.requires_grad_() for t in st]
+    par = [t.clone().requires_grad_() for t in rg.parameters(b)]
+    tg = torch.tensor(tgt, device="cuda", dtype=torch.float32)
+    cur, loss = st, 0.0
+    for f in range(F):
+        cur = rg.frame(b, cur, par, None, None, None, DT, S)
+        loss = loss + ((cur[0].view(R, V, 3)[:, -1] - tg[f]) ** 2).sum(-1).mean()
+    loss.backward()
+    g = {"g_ea": par[0].grad, "g_ei": par[1].grad, "g_mass": par[2].grad, "g_pos": st[0].grad, "g_vel": st[1].grad,
+         "g_lvel": st[2].grad, "g_q": st[3].grad}
+    L = float(loss.detach())
+    print(f"\n  [free frames, {engine}] loss gpu {L:.8e} fp64 {L64:.8e}")
+    assert abs(L - L64) <= 1e-4 * abs(L64)
+    for k, v in g.items():
+        gk = v.detach().cpu().numpy().astype(np.float64)
+        e_gpu, e_32 = ac.rel(gk, g64[k]), ac.rel(g32[k], g64[k])
+        print(f"  {k:7s} |g| {np.linalg.norm(g64[k]):.3e}  gpu-vs-fp64 {e_gpu:.2e}  fp32-oracle-vs-fp64 {e_32:.2e}")
+        assert np.isfinite(gk).all()
+        assert e_gpu <= max(1e-4, 4 * e_32), k
+
+
 # Rope-rope contact scenes (tests/adjoint_cases.rope_crossing; the oracle adjoint is pinned on
 # them by FP64 finite differences in test_adjoint_oracle.py): (scene, dt, substeps, frames,
 # program spread). "resting_crossing": rope 1 settles on rope 0 inside the barrier band (192

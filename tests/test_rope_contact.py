@@ -243,3 +243,21 @@ def test_candidate_overflow_raises():
     with pytest.raises(RuntimeError, match="MAX_COLLISIONS"):
         b.step_free(1 / 60, 2)
     assert b.last_error == 1
+
+
+@pytest.mark.gpu
+def test_candidate_overflow_raises_in_grid_broad_phase():
+    """The same error from a contact group larger than one CTA (300 x 4 = 1,200 vertices), whose
+    detection runs through the grid broad phase: a segment with more than 128 candidates falls
+    back to the brute force, which keeps the first 128 and raises."""
+    import ropesim
+
+    n = 300
+    pos = np.zeros((n, 4, 3), np.float32)
+    pos[:, :, 2] = 1.0 - 0.01 * np.arange(4)
+    pos[:, :, 0] = 1e-4 * np.arange(n)[:, None]
+    b = ropesim.RopeBatch.from_positions(pos, RHO, EA, EI, H, 4, pinned=np.ones(4, bool))
+    b.set_rope_contact(True, 0.004, 0.001, 0.025, 0.4, 1e7, 1.2, n)
+    with pytest.raises(RuntimeError, match="MAX_COLLISIONS"):
+        b.step_free(1 / 60, 2)
+    assert b.last_error == 1
