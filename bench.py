@@ -680,11 +680,17 @@ def run_config5(args):
     rope-rope contact group of all ropes (radius 0.9 R, barrier 0.2 R for R = 5 mm, k_collision
     0.025, mu 0.4, k_friction 1e7), the plane z = 0 and the bowl (R = 5 mm, mu_s 0.5, mu_k 0.4);
     dt 1/60, 100 substeps, 8 iterations. The group (32,768 vertices) is larger than a CTA, so frames
-    run the per-substep-launch path and the backward the per-launch adjoint. Stiffness fitting:
-    targets are the rollout with the seeded per-rope EA / EI; one step = one --frames rollout from
-    the perturbed estimate (forward with tapes, trajectory loss, backward) and one Adam step on
-    per-rope log EA / log EI. Reported: fitting steps/s and forward + backward vertex-substeps/s,
-    the forward-only rollout, and with --fit-steps N the parameter errors after N steps."""
+    run the per-substep-launch path (grid broad phase) and the backward the per-launch adjoint.
+
+    Stiffness fitting: targets are the rollout with the seeded per-rope EA / EI (its full state at
+    every frame). Through the pile the exact gradient of the 8-sweep map grows by ~1e4 per frame
+    (the compressed barrier is far stiffer than m / h^2), so the fit is one-step-ahead (teacher
+    forced): every frame starts from the target state, the loss is the predicted frame-end
+    positions' mean squared distance to the target (mm^2) summed over the frames, and each frame
+    is differentiated on its own (a frame whose gradient overflows FP32 is left out and counted).
+    One step = --frames such frames forward (with tapes) and backward, then one Adam step on
+    per-rope log EA / log EI. Reported: fitting steps/s, forward + backward vertex-substeps/s, the
+    forward-only rollout, and with --fit-steps N the parameter errors after N steps."""
     import torch
 
     import ropesim
@@ -693,9 +699,10 @@ def run_config5(args):
     torch.cuda.set_device(0)
     R = args.ropes if args.ropes != 4096 else 256
     V, F, S5 = 128, args.frames, 100
+    iters = args.iters or ITERS
     pos, ea_true, ei_true, lattice = config5_scene(R, V)
     Rc = 0.005
-    b = ropesim.RopeBatch.from_positions(pos, 0.117, 1000.0, 1e-3, 1 / 6000, ITERS, pinned=np.zeros(V, bool))
+    b = ropesim.RopeBatch.from_positions(pos, 0.117, 1000.0, 1e-3, 1 / 6000, iters, pinned=np.zeros(V, bool))
     b.set_gravity(np.array([0, 0, -9.81], np.float32))
     b.damping = 0.0
     b.drag = 0.2
@@ -715,11 +722,11 @@ def run_config5(args):
     true_ea = torch.tensor(ea_true, device="cuda")
     true_ei = torch.tensor(ei_true, device="cuda")
     with torch.no_grad():  # the trajectories the method itself generates, with the seeded parameters
-        cur, traj = st0, []
+        cur, traj = st0, [st0]
         for f in range(F):
             cur = rg.frame(b, cur, (per_vertex(true_ea), per_vertex(true_ei), mass), None, None, None, DT, S5)
-            traj.append(cur[0].clone())
-    drop = float((st0[0][:, 2] - traj[-1][:, 2]).mean())
+            traj.append(tuple(t.clone() for t in cur))
+    drop = float((st0[0][:, 2] - traj[-1][0][:, 2]).mean())
     rng = np.random.default_rng(6)
     log_ea = torch.tensor(np.log(ea_true) + rng.normal(0, 0.3, R), device="cuda", dtype=torch.float32, requires_grad=True)
     log_ei = torch.tensor(np.log(ei_true) + rng.normal(0, 0.3, R), device="cuda", dtype=torch.float32, requires_grad=True)
@@ -731,18 +738,24 @@ def run_config5(args):
             e_ei = (log_ei.exp() / true_ei).log().abs().median()
         return float(e_ea), float(e_ei)
 
-    info = {}
+    info = {"dropped_frames": 0}
 
     def fit_step():
-        opt.zero_grad(set_to_none=True)
-        cur, loss = st0, 0.0
-        par = (per_vertex(log_ea.exp()), per_vertex(log_ei.exp()), mass)
+        g_ea, g_ei = torch.zeros_like(log_ea), torch.zeros_like(log_ei)
+        total = 0.0
         for f in range(F):
-            cur = rg.frame(b, cur, par, None, None, None, DT, S5)
-            loss = loss + ((cur[0] - traj[f]) ** 2).sum(-1).mean() * 1e6  # mm^2
-        loss.backward()
-        info["loss"] = float(loss.detach())
-        info["finite"] = bool(torch.isfinite(log_ea.grad).all() and torch.isfinite(log_ei.grad).all())
+            par = (per_vertex(log_ea.exp()), per_vertex(log_ei.exp()), mass)
+            out = rg.frame(b, traj[f], par, None, None, None, DT, S5)
+            loss = ((out[0] - traj[f + 1][0]) ** 2).sum(-1).mean() * 1e6  # mm^2
+            ga, gi = torch.autograd.grad(loss, (log_ea, log_ei))
+            if bool(torch.isfinite(ga).all() and torch.isfinite(gi).all()):
+                g_ea += ga
+                g_ei += gi
+            else:
+                info["dropped_frames"] += 1
+            total += float(loss.detach())
+        log_ea.grad, log_ei.grad = g_ea, g_ei
+        info["loss"] = total
         opt.step()
 
     def fwd_only():
@@ -763,15 +776,18 @@ def run_config5(args):
         return ms
 
     err0 = errors()
-    timed(fit_step, args.warmup)
+    timed(fit_step, 1)
     loss_first = info["loss"]
+    timed(fit_step, args.warmup - 1)
     msb = timed(fit_step, args.steps)
     fit = {"steps_done": args.warmup + args.steps}
     if args.fit_steps > fit["steps_done"]:
         timed(fit_step, args.fit_steps - fit["steps_done"])
         fit["steps_done"] = args.fit_steps
     err1 = errors()
-    fit.update({"loss_first_step": loss_first, "loss_last_step": info["loss"], "grads_finite": info["finite"],
+    fit.update({"objective": "one-step-ahead (teacher forced) frame-end positions, mm^2 summed over frames",
+                "loss_first_step": loss_first, "loss_last_step": info["loss"],
+                "frames_dropped_for_overflow": info["dropped_frames"],
                 "median_abs_log_error_ea": [err0[0], err1[0]], "median_abs_log_error_ei": [err0[1], err1[1]]})
     timed(fwd_only, 1)
     msf = timed(fwd_only, max(1, min(args.steps, 3)))
@@ -781,10 +797,10 @@ def run_config5(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded config-5 pile: layered drop into a baked bowl)",
             "config": {"workload": f"config5-contact-{R}x{V}", "ropes": R, "verts_per_rope": V, "frames": F,
-                       "substeps": S5, "num_itr": ITERS, "contact_group_vertices": n,
-                       "step": f"one fitting step: {F}-frame rollout with tapes, trajectory loss, backward, Adam on "
-                               "per-rope log EA / log EI", "engine": "per-substep launches (group larger than a CTA)",
-                       "mean_drop_m": drop},
+                       "substeps": S5, "num_itr": iters, "contact_group_vertices": n,
+                       "step": f"one fitting step: {F} teacher-forced frames forward (taped) + backward, Adam on "
+                               "per-rope log EA / log EI", "engine": "per-substep launches, grid broad phase "
+                               "(group larger than a CTA)", "mean_drop_m": drop},
             "fwd_bwd_vertex_substeps_per_s": n * S5 * F / (ms_step * 1e-3),
             "forward_only": {"ms_per_rollout": float(np.mean(msf)), "value": n * S5 * F / (float(np.mean(msf)) * 1e-3)},
             "fwd_bwd_over_fwd": ms_step / float(np.mean(msf)), "fit": fit}
@@ -806,6 +822,7 @@ def main():
     ap.add_argument("--frames", type=int, default=30, help="config4: control frames per rollout")
     ap.add_argument("--no-tape", action="store_true", help="config4: backward replays frames instead of keeping tapes")
     ap.add_argument("--fit-steps", type=int, default=0, help="config5: total fitting steps to run (e.g. 50)")
+    ap.add_argument("--iters", type=int, default=0, help="config5: Jacobi sweeps per substep (0 = the default 8)")
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
                     help="config2 (the headline line), config3 (uneven ropes, planes and meshes vs the plain path) "
                          "or config4 (differentiable rollouts: forward and forward + backward)")

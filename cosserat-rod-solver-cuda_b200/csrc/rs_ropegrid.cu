@@ -39,7 +39,14 @@ __global__ void rg_reach_kernel(const FrameArgs* __restrict__ pa, const float4* 
     }
     const f3 p = xyz(pos[d]), p1 = xyz(pos[d + 1]);
     const float s = 0.5f * len(p1 - p) + fmaxf(a.pad[d], a.pad[d + 1]);
-    g.ms[d] = f4((p + p1) * 0.5f, s);
+    const f3 m = (p + p1) * 0.5f;
+    if (!(isfinite(s) && isfinite(m.x) && isfinite(m.y) && isfinite(m.z))) {
+        // a diverged segment takes no part (the brute force's tests would reject it as well):
+        // it must not widen the cells of every other segment
+        g.ms[d] = make_float4(0.f, 0.f, 0.f, -1.f);
+        return;
+    }
+    g.ms[d] = f4(m, s);
     atomicMax(g.smax, __float_as_uint(s));  // reaches are positive: their bits order as the floats
 }
 
@@ -84,6 +91,11 @@ __global__ void rg_query_kernel(const FrameArgs* __restrict__ pa, const float4* 
     const f3 mt = p + a1 * 0.5f;
     const float ht = 0.5f * len(a1);
     const float4 md = g.ms[d];
+    if (md.w < 0.f) {  // diverged: no candidates
+        a.ncols[d] = 0;
+        a.maxstep[d] = INFINITY;
+        return;
+    }
     const float c = cell_edge(g);
     const int cx = (int)floorf(md.x / c), cy = (int)floorf(md.y / c), cz = (int)floorf(md.z / c);
     int list[kMaxCols];
