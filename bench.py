@@ -609,7 +609,8 @@ def run_config4(args):
                 cur = st
                 loss = 0.0
                 for f in range(F):
-                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4, tape=not args.no_tape)
+                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4,
+                                   tape=False if args.no_tape else ("iterates" if args.iterate_tape else True))
                     loss = loss + ((cur[0].view(R, V, 3)[:, -1] - tgt[f]) ** 2).sum(-1).mean()
                 loss.backward()
                 grads["finite"] = bool(all(torch.isfinite(t.grad).all() for t in st + par + pr))
@@ -626,7 +627,9 @@ def run_config4(args):
             "data": "synthetic (seeded config-4 rollouts)",
             "config": {"workload": f"config4-diff-{R}x{V}", "ropes": R, "verts_per_rope": V, "frames": F,
                        "substeps": S4, "num_itr": ITERS, "step": f"one {F}-frame rollout",
-                       "backward": "replays each frame" if args.no_tape else "from the forward's substep tapes",
+                       "backward": "replays each frame" if args.no_tape else (
+                           "from the forward's substep and iterate tapes" if args.iterate_tape
+                           else "from the forward's substep tapes"),
                        "counted": "forward vertex-substeps of the rollout", "l2": "flushed between rollouts (256 MB write)"},
             "forward": out["persistent"], "fwd_bwd": out["fwd_bwd"], "plain_path_forward": out["plain"],
             "fwd_bwd_over_fwd": out["fwd_bwd"]["ms_per_rollout"] / out["persistent"]["ms_per_rollout"],
@@ -821,6 +824,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
     ap.add_argument("--frames", type=int, default=30, help="config4: control frames per rollout")
     ap.add_argument("--no-tape", action="store_true", help="config4: backward replays frames instead of keeping tapes")
+    ap.add_argument("--no-iterate-tape", dest="iterate_tape", action="store_false",
+                    help="config4: keep only the substep tapes (the backward recomputes the iterates)")
     ap.add_argument("--fit-steps", type=int, default=0, help="config5: total fitting steps to run (e.g. 50)")
     ap.add_argument("--iters", type=int, default=0, help="config5: Jacobi sweeps per substep (0 = the default 8)")
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],

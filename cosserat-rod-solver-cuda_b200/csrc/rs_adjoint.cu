@@ -33,6 +33,14 @@ namespace rs {
 
 namespace {
 
+// 16-byte asynchronous copies global -> shared (cp.async, no L1 allocation) and their completion.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Shared memory of the adjoint kernel, in float4 units (BLOCK = bin size, I = iterations):
 //   X, QR, KC, EA, EB, EC, EF   one slot per vertex each
 //   with rope-rope contact, seven more: RP (padding, step limit, flags, limit adjoint handed to
@@ -131,9 +139,15 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
         float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
         uint64_t cand = 0ull;  // the forward's broad-phase mask of this substep (tape .w lanes)
         if (act) {
-            const float4* tp = g.tape + (size_t)s * 4 * n + uidx;
-            const float4 t0 = tp[0], t1 = tp[n];
-            p = xyz(t0); v = xyz(t1); lvin = xyz(tp[2 * n]); q = tp[3 * n];
+            float4 t0, t1, t2, t3;
+            if (!ROPE && g.itape && s < S - 1) {  // copied into this thread's slots during substep s + 1
+                cp_async_wait_all();
+                t0 = X[t]; t1 = EA[t]; t2 = EB[t]; t3 = EC[t];
+            } else {
+                const float4* tp = g.tape + (size_t)s * 4 * n + uidx;
+                t0 = __ldcs(tp); t1 = __ldcs(tp + n); t2 = __ldcs(tp + 2 * n); t3 = __ldcs(tp + 3 * n);
+            }
+            p = xyz(t0); v = xyz(t1); lvin = xyz(t2); q = t3;
             cand = (uint64_t)(uint32_t)__float_as_int(t0.w) | ((uint64_t)(uint32_t)__float_as_int(t1.w) << 32);
         }
         const float4* mycache = PC + (size_t)lrope * nsdf * kPoseF4;
@@ -159,37 +173,58 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             RP[t].y = lim;
         }
 
-        // ---- recompute the iterates (the frame kernel's arithmetic)
-        for (int k = 0; k < I; k++) {
-            f3 f, f2;
-            sym3 H, H2;
-            const float4* Dk = LD + (size_t)k * BLOCK;
-            const f3 p1dx = hasNext ? xyz(Dk[t + 1]) : zero3();
-            const bool touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
-            if constexpr (ROPE) collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, dx, p1dx, f, f2, H, H2);
-            EA[t] = f4(f2, H2.xx);
-            EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
-            EC[t].x = H2.yz;
-            __syncthreads();
-            if (hasPrev) {
-                const float4 fa = EA[t - 1], fb = EB[t - 1];
-                f += xyz(fa);
-                H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
+        // ---- the iterates: from the forward's iterate tape, or recomputed (the frame kernel's
+        // arithmetic). Levels 1..I of the tape arrive by asynchronous copies: the last substep's
+        // here, every other substep's during the reverse of the substep after it, each level into
+        // its slot as soon as that reverse is done with it.
+        if (!ROPE && g.itape) {
+            if (s == S - 1 && act) {
+                for (int k = 0; k < I; k++) {
+                    cp_async16(LD + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)(s * 2 * I + k) * n + uidx);
+                    cp_async16(LQ + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)(s * 2 * I + I + k) * n + uidx);
+                }
+                cp_async_commit();
             }
-            float sc = 1.f;
-            if constexpr (ROPE) sc = position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, RP[t - 1].y) : lim);
-            else position_solve(dx, f, H, a.accel, im, !touched);
-            LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, sc);
-            __syncthreads();
-            if (upd) {
-                const f3 seg = (p1 - p) + (xyz(LD[(size_t)(k + 1) * BLOCK + t + 1]) - dx);
-                const float4* Lk = LQ + (size_t)k * BLOCK;
-                q = frame_update(q, seg, c.invl, ks, hasPrev, hasPrev ? Lk[t - 1] : q, hasPrev ? QR[t - 1] : q, nextOrient,
-                                 nextOrient ? Lk[t + 1] : q, QR[t]);
+            cp_async_wait_all();
+            dx = xyz(LD[(size_t)I * BLOCK + t]);
+            q = LQ[(size_t)I * BLOCK + t];
+        } else {
+            for (int k = 0; k < I; k++) {
+                f3 f, f2;
+                sym3 H, H2;
+                const float4* Dk = LD + (size_t)k * BLOCK;
+                const f3 p1dx = hasNext ? xyz(Dk[t + 1]) : zero3();
+                const bool touched =
+                    position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+                if constexpr (ROPE)
+                    collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, dx, p1dx, f, f2, H, H2);
+                EA[t] = f4(f2, H2.xx);
+                EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
+                EC[t].x = H2.yz;
+                __syncthreads();
+                if (hasPrev) {
+                    const float4 fa = EA[t - 1], fb = EB[t - 1];
+                    f += xyz(fa);
+                    H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
+                }
+                float sc = 1.f;
+                if constexpr (ROPE)
+                    sc = position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, RP[t - 1].y) : lim);
+                else position_solve(dx, f, H, a.accel, im, !touched);
+                LD[(size_t)(k + 1) * BLOCK + t] = f4(dx, sc);
+                __syncthreads();
+                if (upd) {
+                    const f3 seg = (p1 - p) + (xyz(LD[(size_t)(k + 1) * BLOCK + t + 1]) - dx);
+                    const float4* Lk = LQ + (size_t)k * BLOCK;
+                    q = frame_update(q, seg, c.invl, ks, hasPrev, hasPrev ? Lk[t - 1] : q, hasPrev ? QR[t - 1] : q,
+                                     nextOrient, nextOrient ? Lk[t + 1] : q, QR[t]);
+                }
+                LQ[(size_t)(k + 1) * BLOCK + t] = q;
             }
-            LQ[(size_t)(k + 1) * BLOCK + t] = q;
         }
-        __syncthreads();
+        // prefetched levels were complete before the barrier after the start state (every thread
+        // waited for its copies there); otherwise the levels just written need one
+        if (ROPE || !g.itape || s == S - 1) __syncthreads();
 
         // ---- end of substep reversed: x' = x + d, v' = drag(d / h), lv' = v
         f3 db = xb;
@@ -388,6 +423,21 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             EF[t] = f4(Fb, trH);
             if constexpr (ROPE) EE[t] = f4(e, 0.f);
             __syncthreads();
+            // level k+1 is read by no one any more: fetch the previous substep's into its slot;
+            // after the last reverse iteration the exchange slots X, EA, EB, EC are free as well
+            // and take the previous substep's start state
+            if (!ROPE && g.itape && s > 0 && act) {
+                cp_async16(LD + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)((s - 1) * 2 * I + k) * n + uidx);
+                cp_async16(LQ + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)((s - 1) * 2 * I + I + k) * n + uidx);
+                if (k == 0) {
+                    const float4* tp = g.tape + (size_t)(s - 1) * 4 * n + uidx;
+                    cp_async16(X + t, tp);
+                    cp_async16(EA + t, tp + n);
+                    cp_async16(EB + t, tp + 2 * n);
+                    cp_async16(EC + t, tp + 3 * n);
+                }
+                cp_async_commit();
+            }
             if (hasNext) {
                 const float4 Fn4 = EF[t + 1];
                 const f3 Fn = xyz(Fn4);

@@ -567,6 +567,7 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     h_ = h;
     FrameArgs a = frame_args(root_mode, has_q0, has_q1, dt, steps);
     a.tape = pending_tape_;
+    a.itape = pending_itape_;
     const bool timed = timing_ || tuning();
     if (timed) check(cudaEventRecord(ev0_, stream_), "event");
     if (engine_ == 1 || (rope_contact_ && oversize_)) run_frame_plain(a);
@@ -1251,8 +1252,10 @@ float Batch::frame_forward(const FrameIO& io, float dt, int substeps, bool synch
     sdf_begin();
     const float last = h_;
     pending_tape_ = reinterpret_cast<float4*>(io.tape);
+    pending_itape_ = (io.tape && itape_usable()) ? reinterpret_cast<float4*>(io.itape) : nullptr;
     run_frame(io.p0 ? ROOT_PROGRAM : ROOT_NONE, false, false, dt, substeps, dt / (float)substeps);
     pending_tape_ = nullptr;
+    pending_itape_ = nullptr;
     time_ += dt;
     sdf_end(substeps);
     tune_after_frame();
@@ -1314,15 +1317,13 @@ void Batch::backward(const BackwardIO& io, float dt, int substeps, float last_h,
     }
     AdjArgs g{};
     g.tape = tape;
+    // the iterates recorded with this frame's tape (never with a replayed tape)
+    g.itape = (io.tape && io.itape && itape_usable()) ? reinterpret_cast<const float4*>(io.itape) : nullptr;
     g.g_pos = io.g_pos; g.g_vel = io.g_vel; g.g_lvel = io.g_lvel; g.g_q = io.g_q;
     g.o_pos = io.o_pos; g.o_vel = io.o_vel; g.o_lvel = io.o_lvel; g.o_q = io.o_q;
     g.o_ea = io.o_ea; g.o_ei = io.o_ei; g.o_mass = io.o_mass;
     g.o_p0 = io.o_p0; g.o_v0 = io.o_v0; g.o_p1 = io.o_p1;
-    if (io.p0) {  // ropes whose root the program does not reach keep zero program adjoints
-        if (io.o_p0) check(cudaMemsetAsync(io.o_p0, 0, sizeof(float) * 3 * R_, stream_), "zero");
-        if (io.o_v0) check(cudaMemsetAsync(io.o_v0, 0, sizeof(float) * 3 * R_, stream_), "zero");
-        if (io.o_p1) check(cudaMemsetAsync(io.o_p1, 0, sizeof(float) * 3 * R_, stream_), "zero");
-    }
+    // o_p0 / o_v0 / o_p1: every rope's first vertex (F_ROOT) writes its rope's row in the adjoint
     if (plain) {
         const size_t words = adjoint_plain_words(n_, num_itr);
         if (words > padj_words_) {

@@ -117,6 +117,7 @@ public:
         float *o_ea, *o_ei, *o_mass, *o_p0, *o_v0, *o_p1;
         const float* tape;
         const float *ea, *ei, *mass;
+        const float* itape;  // iterates recorded by frame_forward (or null: recompute)
     };
     void backward(const BackwardIO& io, float dt, int substeps, float last_h, bool synchronize = true);
     // One differentiable program frame in one call: load the state and (optional) parameters,
@@ -127,6 +128,7 @@ public:
         const float *p0, *v0, *p1;
         float *o_pos, *o_vel, *o_lvel, *o_q;
         float* tape;
+        float* itape;  // every iterate of every substep (persistent engine, no rope-rope contact)
     };
     float frame_forward(const FrameIO& io, float dt, int substeps, bool synchronize);
     // step_program that also records the frame's substep tape (device, 16 * substeps * n
@@ -302,6 +304,8 @@ private:
     float4* d_tape_ = nullptr;      // [tape_steps_][4][n]
     int tape_steps_ = 0;
     float4* pending_tape_ = nullptr;  // tape of the frame being launched (step_program_taped)
+    float4* pending_itape_ = nullptr; // iterate tape of the frame being launched (frame_forward)
+    bool itape_usable() const { return engine_ == 0 && !rope_contact_; }
     void grad_alloc(int substeps);
     // the per-launch adjoint (contact groups larger than one CTA, plain engine)
     float4* d_padj_ = nullptr;      // adjoint_plain_words(n, iters) float4

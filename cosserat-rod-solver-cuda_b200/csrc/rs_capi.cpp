@@ -608,7 +608,7 @@ static int backward_impl(rs_batch* b, const rs_backward_io* io, float dt, int su
         rs::Batch::BackwardIO x{io->pos, io->vel, io->lvel, io->q, io->p0, io->v0, io->p1, io->q0, io->q1,
                                 io->g_pos, io->g_vel, io->g_lvel, io->g_q, io->o_pos, io->o_vel, io->o_lvel, io->o_q,
                                 io->o_ea, io->o_ei, io->o_mass, io->o_p0, io->o_v0, io->o_p1, io->tape,
-                                io->ea, io->ei, io->mass};
+                                io->ea, io->ei, io->mass, io->itape};
         std::lock_guard<std::mutex> g(s.mutex());
         s.backward(x, dt, substeps, last_h, sync);
     });
@@ -624,7 +624,7 @@ int rs_batch_frame_forward(rs_batch* b, const rs_frame_io* io, float dt, int sub
         rs::Batch& s = B(b);
         need(io != nullptr, "null argument");
         rs::Batch::FrameIO x{io->pos, io->vel, io->lvel, io->q, io->ea, io->ei, io->mass, io->p0, io->v0, io->p1,
-                             io->out_pos, io->out_vel, io->out_lvel, io->out_q, io->tape};
+                             io->out_pos, io->out_vel, io->out_lvel, io->out_q, io->tape, io->itape};
         std::lock_guard<std::mutex> g(s.mutex());
         const float lh = s.frame_forward(x, dt, substeps, false);
         if (last_h) *last_h = lh;

@@ -151,11 +151,12 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             if (a.has_q0) sm.q[cur][t] = q;
         }
         if (a.tape && act) {  // differentiable frames: this substep's start state, caller order
+            // (streaming stores: read once, by the backward, after the frame)
             float4* tp = a.tape + (size_t)s * 4 * a.n + a.topo[dv].z;
-            tp[0] = f4(p, __int_as_float((int)(uint32_t)cand));  // broad-phase mask of this substep
-            tp[a.n] = f4(v, __int_as_float((int)(uint32_t)(cand >> 32)));
-            tp[2 * (size_t)a.n] = sm.lv[t];
-            tp[3 * (size_t)a.n] = q;
+            __stcs(tp, f4(p, __int_as_float((int)(uint32_t)cand)));  // broad-phase mask of this substep
+            __stcs(tp + a.n, f4(v, __int_as_float((int)(uint32_t)(cand >> 32))));
+            __stcs(tp + 2 * (size_t)a.n, sm.lv[t]);
+            __stcs(tp + 3 * (size_t)a.n, q);
         }
         float4* cache = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
         float4* tbox = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? tbox1 : tbox0) : tbox0;
@@ -219,6 +220,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
             else position_solve(dx, f, H, a.accel, im, !touched);
             if (act) sm.dx[t] = f4(dx, 0.f);
+            if constexpr (!ROPE)
+                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + it) * a.n + a.topo[dv].z, f4(dx, 0.f));
             __syncthreads();  // B2
 
             // ---- frame step over the double-buffered rotors (no barrier needed before it)
@@ -228,6 +231,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
                                  (fl & F_NEXT_ORIENT) != 0, (fl & F_NEXT_ORIENT) ? sm.q[cur][t + 1] : q, sm.qr[t]);
             }
             if (act) sm.q[cur ^ 1][t] = q;
+            if constexpr (!ROPE)
+                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + I + it) * a.n + a.topo[dv].z, q);
             cur ^= 1;
         }
         __syncthreads();  // B3

@@ -15,8 +15,8 @@
 #include "../../include/ropesim_b200.h"
 
 namespace py = pybind11;
-static_assert(sizeof(rs_backward_io) == 27 * sizeof(const float*), "rs_backward_io is 27 pointers");
-static_assert(sizeof(rs_frame_io) == 15 * sizeof(const float*), "rs_frame_io is 15 pointers");
+static_assert(sizeof(rs_backward_io) == 28 * sizeof(const float*), "rs_backward_io is 28 pointers");
+static_assert(sizeof(rs_frame_io) == 16 * sizeof(const float*), "rs_frame_io is 16 pointers");
 using farray = py::array_t<float, py::array::c_style | py::array::forcecast>;
 
 namespace {
@@ -713,26 +713,26 @@ PYBIND11_MODULE(_ropesim, m) {
                                    ok(rs_batch_get_param(b.h, RS_P_H, &v));
                                    return v;
                                })
-        // Low-level reverse of one frame, queued on the handle's stream: 27 device pointers in
+        // Low-level reverse of one frame, queued on the handle's stream: 28 device pointers in
         // rs_backward_io order (0 = NULL); ropesim.grad validates the tensors behind them.
         .def("_backward",
              [](RopeBatch& b, std::vector<uintptr_t> ptrs, float dt, int substeps, float last_h) {
-                 if (ptrs.size() != 27) throw py::value_error("_backward expects 27 pointers");
+                 if (ptrs.size() != 28) throw py::value_error("_backward expects 28 pointers");
                  rs_backward_io io;
                  const float** c = reinterpret_cast<const float**>(&io);
-                 for (int i = 0; i < 27; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
+                 for (int i = 0; i < 28; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
                  py::gil_scoped_release rel;
                  ok(rs_batch_backward_async(b.h, &io, dt, substeps, last_h));
              },
              py::arg("ptrs"), py::arg("dt"), py::arg("substeps"), py::arg("last_h"))
-        // One differentiable frame in one call, queued on the handle's stream: 15 device pointers in
+        // One differentiable frame in one call, queued on the handle's stream: 16 device pointers in
         // rs_frame_io order; returns the frame's lastH.
         .def("_frame_forward",
              [](RopeBatch& b, std::vector<uintptr_t> ptrs, float dt, int substeps) {
-                 if (ptrs.size() != 15) throw py::value_error("_frame_forward expects 15 pointers");
+                 if (ptrs.size() != 16) throw py::value_error("_frame_forward expects 16 pointers");
                  rs_frame_io io;
                  const float** c = reinterpret_cast<const float**>(&io);
-                 for (int i = 0; i < 15; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
+                 for (int i = 0; i < 16; i++) c[i] = reinterpret_cast<const float*>(ptrs[i]);
                  float lh = 0.f;
                  b.stepped = true;
                  {

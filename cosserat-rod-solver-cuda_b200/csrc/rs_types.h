@@ -145,19 +145,22 @@ struct FrameArgs {
     // tape[(s * 4 + f) * n + u] for f = x, v, lv (previous substep's start velocity), q and the
     // caller-order index u
     float4* tape;
+    // and, when set (no rope-rope contact), every iterate: d^{k+1} at itape[(s * 2I + k) * n + u]
+    // and q^{k+1} at itape[(s * 2I + I + k) * n + u], k = 0 .. I-1
+    float4* itape;
 };
 
 // One frame's backward (rs_adjoint.cu). Arrays are caller order; null outputs are skipped and
 // null upstream adjoints read as zero.
 struct AdjArgs {
     const float4* tape;                          // [S][4][n] caller order, written by a frame launch
+    const float4* itape;                         // [S][2I][n] caller order iterates, or null (recompute)
     const float *g_pos, *g_vel, *g_lvel, *g_q;   // adjoints of the frame-end state [n,3] x3, [n,4]
     float *o_pos, *o_vel, *o_lvel, *o_q;         // adjoints of the frame-start state
     float *o_ea, *o_ei, *o_mass;                 // [n] adjoints of EA, EI (segment i -> i+1), mass
     float *o_p0, *o_v0, *o_p1;                   // [R,3] adjoints of the root program rows
 };
 
-// Global-memory working set of the per-substep-launch (plain) engine.
 // HBM arrays of the per-launch adjoint (contact groups larger than one CTA, or the plain engine),
 // one float4 (or word) per device vertex unless noted.
 struct PlainAdjBufs {
@@ -192,6 +195,7 @@ struct RopeGrid {
     int T;             // buckets, a power of two
 };
 
+// Global-memory working set of the per-substep-launch (plain) engine.
 struct PlainBufs {
     float4* dx;       // displacement iterate
     float4* dxn;      // next iterate (Jacobi output)

@@ -88,12 +88,16 @@ class Frame(torch.autograd.Function):
         if p0 is not None:
             p0, v0, p1 = (_check(t, (R, 3), k) for t, k in ((p0, "p0"), (v0, "v0"), (p1, "p1")))
         out = [torch.empty(n, k, device="cuda", dtype=torch.float32) for k in (3, 3, 3, 4)]
-        # the frame's substep tape (64 B per vertex-substep) lets the backward skip the replay
+        # the frame's substep tape (64 B per vertex-substep) lets the backward skip the replay;
+        # the iterate tape (32 B per vertex-substep-iteration) also skips the recomputation
         ctx.tape = torch.empty(16 * int(substeps) * n, device="cuda", dtype=torch.float32) if tape else None
+        ctx.itape = None
+        if tape == "iterates":
+            ctx.itape = torch.empty(8 * int(batch.num_itr) * int(substeps) * n, device="cuda", dtype=torch.float32)
         cur, ext = _streams(batch)
         ext.wait_stream(cur)
         ptrs = [_ptr(t) for t in (pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)] + [_ptr(t) for t in out]
-        ptrs.append(_ptr(ctx.tape))
+        ptrs += [_ptr(ctx.tape), _ptr(ctx.itape)]
         last_h = batch._frame_forward(ptrs, float(dt), int(substeps))
         cur.wait_stream(ext)
         ctx.batch, ctx.dt, ctx.substeps, ctx.last_h = batch, float(dt), int(substeps), float(last_h)
@@ -112,12 +116,12 @@ class Frame(torch.autograd.Function):
         og = [None] * 3 if ctx.free else [torch.empty(R, 3, device="cuda", dtype=torch.float32) for _ in range(3)]
         ptrs = [_ptr(t) for t in (pos, vel, lvel, q, p0, v0, p1, None, None)]
         ptrs += [_ptr(t) for t in g_in] + [_ptr(t) for t in o] + [_ptr(t) for t in op] + [_ptr(t) for t in og]
-        ptrs += [_ptr(ctx.tape), _ptr(ea), _ptr(ei), _ptr(mass)]
+        ptrs += [_ptr(ctx.tape), _ptr(ea), _ptr(ei), _ptr(mass), _ptr(ctx.itape)]
         cur, ext = _streams(b)
         ext.wait_stream(cur)
         b._backward(ptrs, ctx.dt, ctx.substeps, ctx.last_h)
         cur.wait_stream(ext)
-        ctx.tape = None
+        ctx.tape = ctx.itape = None
         grads = [None if t is None else t.reshape(sh) for t, sh in zip(o + op + og, ctx.shapes)]
         return (None, None, None, None, *grads)
 
@@ -140,9 +144,15 @@ def frame(batch, st, params, p0, v0, p1, dt, substeps, tape=True):
 
     tape=True keeps the frame's substep tape in device memory until the backward (64 B per
     vertex-substep: 420 MB for 65,536 vertices x 100 substeps), so the backward does not replay
-    the frame; tape=False keeps only the frame-start state and replays the frame in the backward."""
+    the frame; tape="iterates" also keeps every iterate (32 B per vertex-substep-iteration: 1.7 GB
+    more at that size and 8 iterations), so the backward does not recompute them either (used on
+    the persistent engine without rope-rope contact; elsewhere the backward recomputes);
+    tape=False keeps only the frame-start state and replays the frame in the backward."""
     pos, vel, lvel, q = st
     ea, ei, mass = params
     ins = (pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)
-    keep = bool(tape) and torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad for t in ins)
+    if tape not in (True, False, "iterates"):
+        raise ValueError("tape must be True, False or 'iterates'")
+    grad = torch.is_grad_enabled() and any(isinstance(t, torch.Tensor) and t.requires_grad for t in ins)
+    keep = (tape if tape else False) if grad else False
     return Frame.apply(batch, dt, substeps, keep, *ins)

@@ -233,6 +233,7 @@ typedef struct rs_backward_io {
     float *o_p0, *o_v0, *o_p1;
     const float* tape;  /* NULL = replay the frame; else this frame's recorded tape */
     const float *ea, *ei, *mass;  /* the frame's parameters (NULL = the handle's current ones) */
+    const float* itape; /* the frame's iterate tape (rs_frame_io.itape) or NULL (recompute) */
 } rs_backward_io;
 RS_API int rs_batch_backward(rs_batch* b, const rs_backward_io* io, float dt, int substeps, float last_h);
 /* The same, returning with the work queued on the handle's stream (no host synchronization). */
@@ -240,7 +241,10 @@ RS_API int rs_batch_backward_async(rs_batch* b, const rs_backward_io* io, float 
 /* One differentiable frame in one call (device pointers, caller order): loads the frame-start
  * state and the parameters (NULL = keep), steps with the program rows p0 / v0 / p1 [R,3] (all
  * three NULL: a free frame, as rs_batch_step_free), writes the end state to out_* and, when
- * tape != NULL (16 * substeps * n floats), the substep tape for rs_batch_backward. *last_h
+ * tape != NULL (16 * substeps * n floats), the substep tape for rs_batch_backward. With itape
+ * != NULL as well (8 * num_itr * substeps * n floats: every iterate d^k, q^k of every substep)
+ * the backward reads the iterates instead of recomputing them; without rope-rope contact and on
+ * the persistent engine only (elsewhere it is ignored and the backward recomputes). *last_h
  * receives the frame's lastH (RS_P_H before the frame). Queued on the handle's stream without
  * host synchronization. */
 typedef struct rs_frame_io {
@@ -249,6 +253,7 @@ typedef struct rs_frame_io {
     const float *p0, *v0, *p1;
     float *out_pos, *out_vel, *out_lvel, *out_q;
     float* tape;
+    float* itape;
 } rs_frame_io;
 RS_API int rs_batch_frame_forward(rs_batch* b, const rs_frame_io* io, float dt, int substeps, float* last_h);
 /* rs_batch_step_program that also records the frame's substep tape for rs_batch_backward:
