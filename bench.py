@@ -328,7 +328,7 @@ def run_config3(args):
         cur = p1
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     out = {}
-    for engine in ("persistent", "plain"):
+    for engine in ("persistent",) if args.no_plain else ("persistent", "plain"):
         b = build_config3(ropesim, scene, engine)
         st = torch.cuda.ExternalStream(b.stream_ptr())
         ms = []
@@ -348,15 +348,74 @@ def run_config3(args):
         out[engine] = {"ms_per_step": float(np.mean(ms)), "value": nv * S * len(ms) / (sum(ms) * 1e-3),
                        "finite": bool(np.isfinite(pos).all()), "layout": list(b.layout())}
         del b
+    if not args.no_plain:
+        out["plain_per_length"] = plain_per_length(ropesim, scene, prog, poses, args, flush)
     line = {"metric": METRIC, "value": out["persistent"]["value"], "unit": METRIC, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": out["persistent"]["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-3 scene)",
             "config": {"workload": f"config3-uneven-{R}", "ropes": R, "verts": nv, "verts_per_rope": "U{16..256}",
                        "substeps": S, "num_itr": ITERS, "planes": 2, "meshes": M, "lattice": "64^3",
                        "l2": "flushed between frames (256 MB write)"},
-            "persistent": out["persistent"], "plain_path": out["plain"],
-            "speedup_vs_plain": out["persistent"]["value"] / out["plain"]["value"]}
+            "persistent": out["persistent"]}
+    if not args.no_plain:
+        line.update({"plain_path": out["plain"], "speedup_vs_plain": out["persistent"]["value"] / out["plain"]["value"],
+                     "plain_per_length": out["plain_per_length"],
+                     "speedup_vs_plain_per_length": out["persistent"]["value"] / out["plain_per_length"]["value"]})
     print(json.dumps(line), flush=True)
+
+
+def plain_per_length(ropesim, scene, prog, poses, args, flush):
+    """The plain path as the reference's API can run uneven ropes: RopeBatch holds num_envs ropes
+    of one length, so the scene becomes one plain-engine batch per distinct vertex count (each
+    with its own copy of the lattices), stepped in sequence on one stream every frame. Same
+    ropes, stiffnesses, masses, planes, mesh poses and root programs as the single packed batch;
+    a frame is timed with CUDA events on the legacy default stream, which every batch's blocking
+    stream is ordered with."""
+    import torch
+
+    ropes, verts, ea_v, ei_v, m_v, grids = scene
+    starts = np.concatenate([[0], np.cumsum(verts)[:-1]])
+    batches = []
+    for V in np.unique(verts):
+        idx = np.nonzero(verts == V)[0]
+        b = ropesim.RopeBatch.from_positions(np.stack([ropes[r] for r in idx]), 0.117, 1000.0, 1e-3, H, ITERS)
+        sel = np.stack([starts[r] + np.arange(V) for r in idx])  # [n_V, V] flat vertex indices
+        b.set_stretch_stiffnesses(ea_v[sel[:, :-1]])
+        b.set_bend_stiffnesses(ei_v[sel[:, :-1]])
+        b.set_masses(m_v[sel])
+        b.set_engine("plain")
+        b.set_gravity(np.array([0, 0, -9.81], np.float32))
+        b.damping = 0.0
+        b.drag = 0.2
+        b.set_planes(np.array([[0, 0, 1, 0], [0.05, 0.0, 1.0, -0.02]], np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
+        for gd in grids:
+            b.add_mesh(*gd.as_args())
+        batches.append((b, torch.as_tensor(idx, device="cuda")))
+    nv = int(np.sum(verts))
+    ms = []
+    nwarm, nsteps = min(args.warmup, 3), min(args.steps, 3)
+    for f in range(nwarm + nsteps):
+        sub = [(b, poses[f][0][i].contiguous(), poses[f][1][i].contiguous(),
+                [prog[f][k][i].contiguous() for k in range(3)]) for b, i in batches]
+        if f >= nwarm:
+            flush.fill_(float(f))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        for b, pp, pq, pr in sub:
+            b.set_mesh_poses_all(pp, pq, teleport=(f == 0))
+            b.step(pr[0], pr[1], DT, S, root_pos_end=pr[2])
+        if f >= nwarm:
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    finite = all(bool(torch.isfinite(torch.as_tensor(b.positions())).all()) for b, _ in batches)
+    res = {"ms_per_step": float(np.mean(ms)), "value": nv * S * len(ms) / (sum(ms) * 1e-3), "batches": len(batches),
+           "steps": nsteps, "finite": finite,
+           "note": "one plain-engine RopeBatch per distinct vertex count (the reference's RopeBatch takes ropes of "
+                   "one length), stepped in sequence"}
+    del batches
+    return res
 
 
 def max_over_ranks(x, dist, device):
@@ -392,7 +451,9 @@ def run_ours(args):
 
     lib = ctypes.CDLL(os.path.join(PKG, "ropesim", "libropesim_b200.so"))
     frames = args.warmup + args.steps
-    pos, p0, v0, p1 = c2_inputs(N_ROPES, frames, 1234 + rank)
+    # frames [0, W+K) drive the device-timed leg; the end-to-end leg continues the same root
+    # programs over frames [W+K, 2(W+K)) (its own W warm-up frames, then K timed)
+    pos, p0, v0, p1 = c2_inputs(N_ROPES, 2 * frames, 1234 + rank)
     b = ropesim.RopeBatch.from_positions(pos, 0.117, 11473.0, 4.48e-3, H, ITERS, deterministic=True)
     configure(b)
     if args.block:
@@ -437,7 +498,7 @@ def run_ours(args):
 
     # ---- end-to-end leg: host inputs in, host positions out, through the public API
     if args.no_e2e:
-        frames = args.warmup  # no e2e frames
+        frames = args.warmup  # no timed e2e frames
     hp0 = torch.as_tensor(p0).pin_memory()
     hv0 = torch.as_tensor(v0).pin_memory()
     hp1 = torch.as_tensor(p1).pin_memory()
@@ -446,13 +507,23 @@ def run_ours(args):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t0 = time.perf_counter()
-    for f in range(args.warmup, frames):
+
+    def e2e_frame(f):
         a0 = hp0[f].to(dev, non_blocking=True)
         a1 = hv0[f].to(dev, non_blocking=True)
         a2 = hp1[f].to(dev, non_blocking=True)
         b.step(a0, a1, DT, S, root_pos_end=a2)
         out.copy_(view)
+
+    e2e_first = args.warmup + args.steps
+    for f in range(e2e_first, e2e_first + args.warmup):
+        e2e_frame(f)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for f in range(e2e_first + args.warmup, e2e_first + frames):
+        e2e_frame(f)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if world > 1:

@@ -48,9 +48,13 @@ struct FrameSmem {
 static_assert(sizeof(FrameSmem<64>) == 144 * 64 && sizeof(FrameSmem<1024>) == 144 * 1024, "FrameSmem layout");
 
 // Resident CTAs per SM the register allocation targets: 28 warps per SM (<= 72 registers;
-// 24 warps for 256-thread CTAs) without meshes, 16 warps per SM (<= 128 registers) with meshes.
+// 24 warps for 256-thread CTAs) without meshes; 24 warps per SM (<= 80 registers) with meshes,
+// where the rarely taken lattice-sampling path spills a few values to L1 (176 B per thread) and
+// the extra resident CTA hides the barrier waits of the vertices that do sample (config 3:
+// 34.3 -> 31.1 ms per frame); 16 warps per SM (<= 128 registers) with rope-rope contact.
 #ifndef RS_MIN_BLOCKS
-#define RS_MIN_BLOCKS(B, SURF, ROPE) ((B) <= 256 ? (((SURF) == SURF_MESHES || (ROPE) ? 512 : 896) / (B)) : 1)
+#define RS_MIN_BLOCKS(B, SURF, ROPE) \
+    ((B) <= 256 ? (((ROPE) ? 512 : (SURF) == SURF_MESHES ? 768 : 896) / (B)) : 1)
 #endif
 
 template <int BLOCK, int SURF, bool ROPE>
