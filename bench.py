@@ -881,6 +881,201 @@ def run_config5(args):
     print(json.dumps(line), flush=True)
 
 
+def run_exchange(args):
+    """The rigid-body exchange loop at scale (the reference's Isaac bridge, ropesim/isaac_bridge.py:236-271):
+    per exchange, mesh poses from CUDA tensors (set_mesh_poses_all), one rope step, and the
+    frame-averaged wrenches read back through mesh_wrenches_view (a device copy, as the bridge's
+    wrenches()). Config-3 scene (uneven ropes, 2 planes, 8 meshes per env) with the contact-force
+    readout on, exchanged once per control frame (K = 1, 100 substeps) and sub-cycled (K = 10
+    steps of 10 substeps, the bridge's --exchange 10), next to the same frames with the readout
+    off. One step = one control frame; CUDA events on the solver stream around the whole loop."""
+    import torch
+
+    import ropesim
+    import scenarios as Sc
+
+    torch.cuda.set_device(0)
+    R = args.ropes if args.ropes != 4096 else 8192
+    scene = config3_scene(R)
+    ropes, verts = scene[0], scene[1]
+    nv = int(np.sum(verts))
+    M = 8
+    rng = np.random.default_rng(23)
+    frames = args.warmup + args.steps
+    pos0 = np.zeros((R, M, 3), np.float32)
+    for r, rope in enumerate(ropes):
+        L = 0.02 * (len(rope) - 1)
+        for m in range(M):
+            pos0[r, m] = rope[0] + np.array([0.25 * np.cos(0.8 * m), 0.25 * np.sin(0.8 * m), -(0.15 + 0.1 * m) * L])
+    q0 = np.zeros((R, M, 4), np.float32)
+    q0[..., 3] = 1.0
+    roots = np.stack([r[0] for r in ropes]).astype(np.float32)
+
+    def leg(K, forces):
+        b = build_config3(ropesim, scene, "persistent")
+        b.enable_contact_forces(forces)
+        st = torch.cuda.ExternalStream(b.stream_ptr())
+        wview = torch.as_tensor(b.mesh_wrenches_view()) if forces else None
+        prng = np.random.default_rng(29)
+        p, q, cur = pos0, q0, roots.copy()
+        poses, progs = [], []
+        for f in range(frames * K):  # per exchange: poses and a root program over dt / K
+            poses.append((torch.as_tensor(p, device="cuda"), torch.as_tensor(q, device="cuda")))
+            p, q = Sc.walk_poses(prng, p, q, step=0.003 / K, ang=0.02 / K)
+            v0 = prng.normal(0, 0.1, (R, 3)).astype(np.float32)
+            p1 = (cur + prng.normal(0, 0.01 / K, (R, 3))).astype(np.float32)
+            progs.append(tuple(torch.as_tensor(x, device="cuda") for x in (cur, v0, p1)))
+            cur = p1
+        out = []
+        ms, wall = [], []
+        for f in range(frames):
+            if f >= args.warmup:
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                t0 = time.perf_counter()
+            for k in range(K):
+                x = f * K + k
+                b.set_mesh_poses_all(poses[x][0], poses[x][1], teleport=(x == 0))
+                b.step(progs[x][0], progs[x][1], DT / K, S // K, root_pos_end=progs[x][2])
+                if forces:
+                    out.append(wview[:, :M].clone())
+            if f >= args.warmup:
+                e1.record(st)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                wall.append(time.perf_counter() - t0)
+        torch.cuda.synchronize()
+        res = {"K": K, "readout": forces, "ms_per_frame": float(np.mean(ms)), "wall_ms_per_frame": 1e3 * float(np.mean(wall)),
+               "value": nv * S * len(ms) / (sum(ms) * 1e-3)}
+        if forces:
+            w = torch.stack(out[-K:]).float()
+            res["wrench_max_abs"] = float(w.abs().max())
+            res["finite"] = bool(torch.isfinite(w).all())
+        del b
+        return res
+
+    legs = [leg(1, False), leg(1, True), leg(10, True)]
+    line = {"metric": "vertex-substeps/s (exchange loop)", "value": legs[2]["value"], "unit": METRIC, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": legs[2]["ms_per_frame"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-3 scene)",
+            "config": {"workload": f"exchange-config3-{R}", "ropes": R, "verts": nv, "meshes": M, "substeps": S,
+                       "step": "one control frame of K exchanges: poses in (CUDA), rope step, wrenches out (device copy)"},
+            "legs": legs,
+            "readout_cost": legs[1]["ms_per_frame"] / legs[0]["ms_per_frame"],
+            "subcycle_cost_k10": legs[2]["ms_per_frame"] / legs[1]["ms_per_frame"]}
+    print(json.dumps(line), flush=True)
+
+
+# Operations of one evaluation, counted from the kernel source (add/sub/mul/div/sqrt = 1): a
+# point-triangle distance on its longest path (the face interior, FP32), a line-triangle crossing
+# test (three edge predicates, FP64) and one solid angle (FP32, atan2 counted as 1).
+BAKE_FLOP_DIST, BAKE_FLOP_CROSS, BAKE_FLOP_SOLID = 80, 15, 66
+
+
+def run_bake(args):
+    """Mesh baking (the reference's sdf.bake_mesh, on Warp there): an icosphere of `--bake-subdiv`
+    subdivisions (default 5: 20,480 triangles, r 0.15 m) baked with 2.5 mm cells and a 5 cm margin
+    (162^3 = 4.25 M nodes). value: lattice nodes per second of the whole call (CUDA events on the
+    bake's stream around it; the host's triangle sort and upload are inside); kernel_ms_per_bake:
+    the kernels alone; e2e: sdf.bake_mesh from host arrays to a host lattice (wall clock);
+    cpu_baseline: the FP64 brute-force oracle on all host cores over one slab of the lattice."""
+    import ctypes
+
+    import torch
+
+    import meshes
+    from ropesim import sdf
+
+    torch.cuda.set_device(0)
+    lib = ctypes.CDLL(os.path.join(PKG, "ropesim", "libropesim_b200.so"))
+    v, f = meshes.icosphere(args.bake_subdiv, 0.15)
+    spacing, margin = 0.0025, 0.05
+    origin, dims = sdf._lattice(v.min(0) - margin, v.max(0) + margin, spacing)
+    nodes = int(np.prod(dims))
+    out = torch.empty(dims, dtype=torch.float32, device="cuda")
+    st = torch.cuda.Stream()
+    cnt = (ctypes.c_ulonglong * 4)()
+    vp, fp = np.ascontiguousarray(v, np.float32), np.ascontiguousarray(f, np.int32)
+    org = np.ascontiguousarray(origin, np.float32)
+
+    def bake(counters=None):
+        rc = lib.rs_sdf_bake(vp.ctypes.data_as(ctypes.c_void_p), len(v), fp.ctypes.data_as(ctypes.c_void_p), len(f),
+                             org.ctypes.data_as(ctypes.c_void_p), ctypes.c_double(spacing), dims[0], dims[1], dims[2],
+                             ctypes.c_float(0.0), ctypes.c_float(0.0), ctypes.c_void_p(out.data_ptr()), 1,
+                             ctypes.c_void_p(st.cuda_stream), counters)
+        if rc != 0:
+            raise RuntimeError("rs_sdf_bake failed")
+
+    bake(cnt)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        bake()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ms, kms = [], []
+    sampler = ClockSampler(0)
+    with sampler:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            bake(cnt)
+            e1.record(st)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            kms.append(cnt[3] * 1e-6)
+    dev_ms = float(np.mean(ms))
+    kernel_ms = float(np.mean(kms))
+    # end to end: host mesh in, host lattice out, through the public Python API
+    sdf.bake_mesh(v, f, spacing, margin)
+    t0 = time.perf_counter()
+    ke = max(1, min(args.steps, 5))
+    for _ in range(ke):
+        g = sdf.bake_mesh(v, f, spacing, margin)
+    e2e_s = (time.perf_counter() - t0) / ke
+    assert g.values.shape == tuple(dims) and np.isfinite(g.values).all()
+    assert np.array_equal(out.cpu().numpy(), g.values)
+    ev_d, ev_x, ev_w = int(cnt[0]), int(cnt[1]), int(cnt[2])
+    flops = ev_d * BAKE_FLOP_DIST + ev_w * BAKE_FLOP_SOLID  # FP32 work (the FP64 crossing tests are few)
+    tf = ctypes.c_double(0)
+    lib.rs_probe_fp32_peak(ctypes.byref(tf), None)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+    line = {"metric": "lattice nodes/s (mesh bake)", "value": nodes / (dev_ms * 1e-3), "unit": "nodes/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (icosphere mesh)",
+            "config": {"workload": f"bake-icosphere{args.bake_subdiv}", "triangles": len(f), "lattice": list(dims),
+                       "nodes": nodes, "spacing_m": spacing, "margin_m": margin, "signed": True,
+                       "l2": "flushed between bakes (256 MB write)"},
+            "e2e": {"value": nodes / e2e_s, "unit": "nodes/s", "h2d_bytes_per_step": int(vp.nbytes + fp.nbytes),
+                    "d2h_bytes_per_step": nodes * 4},
+            "kernel_ms_per_bake": kernel_ms,
+            "timing": "value: CUDA events around the whole rs_sdf_bake call on its stream (host triangle sort and "
+                      "upload included); kernel_ms_per_bake and roofline: the two kernels alone",
+            "gpu_launches": 2 * args.steps,
+            "evaluations": {"point_triangle_distances": ev_d, "crossing_tests": ev_x, "solid_angles": ev_w,
+                            "brute_force_pairs": nodes * len(f), "distance_fraction_of_brute_force": ev_d / (nodes * len(f))},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": tf.value, "unit": "TFLOP/s",
+                         "frac": achieved / tf.value, "traffic": None,
+                         "flops_per_eval": {"distance": BAKE_FLOP_DIST, "crossing_fp64": BAKE_FLOP_CROSS,
+                                            "solid_angle": BAKE_FLOP_SOLID},
+                         "peak_source": "measured FP32 FMA probe (rs_probe_fp32_peak) on this GPU"},
+            "clocks": sampler.summary()}
+    if not args.no_cpu:
+        import _oracle
+
+        i1 = 1
+        t0 = time.perf_counter()
+        _oracle.bake_sdf(vp, fp, org, spacing, [i1, dims[1], dims[2]], 0.0, 0.0, 0)
+        t = time.perf_counter() - t0
+        thr = _oracle.hardware_threads()
+        line["cpu_baseline"] = {"value": i1 * dims[1] * dims[2] / t, "unit": "nodes/s", "cores": thr, "kind": "port",
+                                "sample": f"{i1} of {dims[0]} x-slabs of the lattice (FP64 brute-force oracle, "
+                                          f"{thr} threads, {t:.1f} s)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     global N_ROPES
     ap = argparse.ArgumentParser()
@@ -899,7 +1094,9 @@ def main():
                     help="config4: keep only the substep tapes (the backward recomputes the iterates)")
     ap.add_argument("--fit-steps", type=int, default=0, help="config5: total fitting steps to run (e.g. 50)")
     ap.add_argument("--iters", type=int, default=0, help="config5: Jacobi sweeps per substep (0 = the default 8)")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
+    ap.add_argument("--bake-subdiv", type=int, default=5, help="bake: icosphere subdivisions of the baked mesh")
+    ap.add_argument("--workload", default="config2",
+                    choices=["config2", "config3", "config4", "config5", "bake", "exchange"],
                     help="config2 (the headline line), config3 (uneven ropes, planes and meshes vs the plain path) "
                          "or config4 (differentiable rollouts: forward and forward + backward)")
     args = ap.parse_args()
@@ -914,6 +1111,11 @@ def main():
         run_config4(args)
     elif args.workload == "config5":
         run_config5(args)
+    elif args.workload == "exchange":
+        run_exchange(args)
+    elif args.workload == "bake":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        run_bake(args)
     else:
         run_ours(args)
 

@@ -22,7 +22,7 @@ PKG = os.path.join(HERE, "ropesim")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["rs_frame.cu", "rs_plain.cu", "rs_adjoint.cu", "rs_adjoint_plain.cu", "rs_ropegrid.cu"]
+CU_SOURCES = ["rs_frame.cu", "rs_plain.cu", "rs_adjoint.cu", "rs_adjoint_plain.cu", "rs_ropegrid.cu", "rs_sdfbake.cu"]
 CPP_SOURCES = ["rs_batch.cpp", "rs_capi.cpp"]
 HEADERS = ["rs_types.h", "rs_device.cuh", "rs_substep.cuh", "rs_adjoint.cuh", "rs_kernels.h", "rs_batch.h"]
 

@@ -643,6 +643,20 @@ int rs_batch_step_program_taped(rs_batch* b, const float* p0, const float* v0, c
     });
 }
 
+int rs_sdf_bake(const float* vertices, int num_vertices, const int* triangles, int num_triangles, const float* origin3,
+                double spacing, int nx, int ny, int nz, float thickness, float round, float* out, int out_on_device,
+                void* stream, unsigned long long* counters) {
+    return guarded([&] {
+        need(vertices && triangles && origin3 && out, "null argument");
+        std::string err;
+        const cudaError_t e = rs::sdf_bake(vertices, num_vertices, triangles, num_triangles, origin3, spacing, nx, ny, nz,
+                                           thickness, round, out, out_on_device != 0, counters,
+                                           static_cast<cudaStream_t>(stream), &err);
+        if (e == cudaErrorInvalidValue && !err.empty() && err.rfind("sdf bake:", 0) != 0) throw std::invalid_argument(err);
+        if (e != cudaSuccess) throw rs::cuda_error(err.empty() ? cudaGetErrorString(e) : err);
+    });
+}
+
 int rs_probe_fp32_peak(double* tflops, double* ms) {
     return guarded([&] {
         need(tflops != nullptr, "null argument");

@@ -57,6 +57,63 @@ static_assert(sizeof(FrameSmem<64>) == 144 * 64 && sizeof(FrameSmem<1024>) == 14
     ((B) <= 256 ? (((ROPE) ? 512 : (SURF) == SURF_MESHES ? 768 : 896) / (B)) : 1)
 #endif
 
+// Mesh part of the contact readout (contact.cuh:172-204) for one warp: every lane calls it
+// (cand = 0 for lanes without a vertex or with a pinned one). The contact force of each
+// candidate mesh goes to the lane's `fv` in ascending mesh order, as in surfaces(); the wrench
+// BY the rope ON the mesh is summed over the warp with shuffles and added by one lane with six
+// atomics when all lanes with candidates belong to one env (the common case: a warp holds 32
+// consecutive vertices of a rope), else lane by lane. The reference adds six atomics per
+// contact.
+__device__ __forceinline__ void mesh_readout_warp(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos, f3 d,
+                                                  float k, float h, int env, f3& fv, const float* btab,
+                                                  const float4* tbox) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const unsigned lo = __reduce_or_sync(FULL, (unsigned)cand), hi = __reduce_or_sync(FULL, (unsigned)(cand >> 32));
+    uint64_t um = ((uint64_t)hi << 32) | lo;
+    if (!um) return;
+    const unsigned withc = __ballot_sync(FULL, cand != 0ull);
+    const int env0 = __shfl_sync(FULL, env, __ffs(withc) - 1);
+    const bool one_env = __ballot_sync(FULL, cand != 0ull && env != env0) == 0u;
+    for (; um; um &= um - 1ull) {
+        const int m = __ffsll((long long)um) - 1;
+        f3 fm = zero3(), tq = zero3();
+        bool hit = false;
+        if ((cand >> m) & 1ull) {
+            const float4 lo4 = tbox[2 * m], hi4 = tbox[2 * m + 1];
+            const f3 pr = pos + d;
+            if (pr.x >= lo4.x && pr.x <= hi4.x && pr.y >= lo4.y && pr.y <= hi4.y && pr.z >= lo4.z && pr.z <= hi4.z) {
+                const PoseV P = load_pose(cache + m * kPoseF4);
+                f3 n, dRel;
+                float gap;
+                if (sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, a.sdf_skip != 0, btab, n, gap,
+                                   dRel)) {
+                    sym3 Hs = sym_zero();
+                    surface_contact(n, gap, dRel, k, h, a.grids[m].muS, a.grids[m].muK, a.c_vslip, fm, Hs);
+                    fv += fm;
+                    tq = cross((pos - P.pos) + d - n * a.c_radius, -fm);
+                    hit = true;
+                }
+            }
+        }
+        if (one_env) {
+            float w[6] = {-fm.x, -fm.y, -fm.z, tq.x, tq.y, tq.z};
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) w[c] += __shfl_xor_sync(FULL, w[c], o);
+            if (__ballot_sync(FULL, hit) && (threadIdx.x & 31) == 0) {
+                float* wr = a.wrench + ((size_t)env0 * kMaxSdf + m) * 6;
+#pragma unroll
+                for (int c = 0; c < 6; c++) atomicAdd(wr + c, w[c]);
+            }
+        } else if (hit) {
+            float* wr = a.wrench + ((size_t)env * kMaxSdf + m) * 6;
+            atomicAdd(wr + 0, -fm.x); atomicAdd(wr + 1, -fm.y); atomicAdd(wr + 2, -fm.z);
+            atomicAdd(wr + 3, tq.x); atomicAdd(wr + 4, tq.y); atomicAdd(wr + 5, tq.z);
+        }
+    }
+}
+
 template <int BLOCK, int SURF, bool ROPE>
 __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame_kernel(const FrameArgs a) {
     // FrameSmem<BLOCK>, the pose cache [2][pose_cache][kPoseF4], then the lattice block bounds
@@ -144,7 +201,6 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
     }
     uint64_t cand = all_meshes(nsdf);  // the first substep of a frame visits every mesh
     f3 facc = zero3();
-    float* wrow = (SURF == SURF_MESHES && a.forces_on && nsdf > 0) ? a.wrench + (size_t)env * kMaxSdf * 6 : nullptr;
 
     int cur = 0;
     if (act) sm.q[0][t] = q;
@@ -241,17 +297,20 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         }
         __syncthreads();  // B3
 
-        // ---- velocity, drag, readout, advection, broad phase
+        // ---- velocity, drag, readout (planes, then meshes warp-cooperatively), advection, broad phase
+        f3 fv = zero3();
         if (im != 0.f) {
             const f3 tg = (a.drag_quad > 0.f) ? (hasNext ? qtangent(q) : qtangent(sm.q[cur][t - 1])) : zero3();
             v = end_velocity(a, dx, invH, tg);
             if (SURF != SURF_NONE && a.forces_on) {
-                f3 fv = zero3();
                 sym3 Hs = sym_zero();
-                surfaces<SURF>(a, mycache, cand, p, dx, c.kc, h, fv, Hs, wrow, &fv, btab, mytbox);
-                facc += fv;
+                surfaces<SURF_PLANES>(a, mycache, 0ull, p, dx, c.kc, h, fv, Hs, nullptr, nullptr);
             }
         }
+        if constexpr (SURF == SURF_MESHES)
+            if (a.forces_on && nsdf > 0)
+                mesh_readout_warp(a, mycache, (act && im != 0.f) ? cand : 0ull, p, dx, c.kc, h, env, fv, btab, mytbox);
+        if (SURF != SURF_NONE && a.forces_on) facc += fv;
         p += dx;
         if (SURF == SURF_MESHES && nsdf > 0) cand = (im != 0.f) ? build_candidates(a, mycache, nsdf, p, dx) : 0ull;
     }

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "rs_types.h"
 
 namespace rs {
@@ -59,5 +61,12 @@ cudaError_t launch_params_out(const int4* topo, const float4* pos, const float4*
                               const float4* qrest, float* ea, float* ei, float* mass, int n, cudaStream_t s);
 // FP32 FMA throughput probe (16 * 8 FMAs per thread per iteration).
 cudaError_t launch_fp32_probe(float* out, int blocks, int threads, int iters, cudaStream_t s);
+// Signed-distance lattice of a triangle mesh (rs_sdfbake.cu): host vertices [nv,3] and
+// triangles [nt,3]; `out` [nx,ny,nz] host (synchronous) or device (queued on s); counters NULL
+// or [4] host (distance evaluations, crossing tests, solid angles, kernel nanoseconds). On a validation failure
+// *err is set and cudaErrorInvalidValue returned.
+cudaError_t sdf_bake(const float* verts, int nv, const int* tris, int nt, const float* origin, double spacing, int nx, int ny,
+                     int nz, float thickness, float round, float* out, bool out_on_device, unsigned long long* counters,
+                     cudaStream_t s, std::string* err);
 
 }  // namespace rs

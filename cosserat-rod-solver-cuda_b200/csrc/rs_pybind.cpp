@@ -398,6 +398,33 @@ PYBIND11_MODULE(_ropesim, m) {
     m.doc() = "B200 Stable Cosserat Rods engine (persistent sm_100a frame kernel) behind the ropesim API";
     m.attr("__version__") = rs_version();
 
+    // the GPU half of ropesim.sdf.bake_mesh (lattice box and closedness checks are in Python)
+    m.def("bake_sdf",
+          [](farray vertices, py::array_t<int, py::array::c_style | py::array::forcecast> triangles, farray origin,
+             double spacing, std::vector<int> dims, float thickness, float round, bool counters) {
+              if (vertices.ndim() != 2 || vertices.shape(1) != 3) throw py::value_error("vertices must be [V, 3]");
+              if (triangles.ndim() != 2 || triangles.shape(1) != 3) throw py::value_error("triangles must be [T, 3]");
+              if (dims.size() != 3) throw py::value_error("dims must be (nx, ny, nz)");
+              const auto o = vec3(origin, "origin");
+              py::array_t<float> out({(py::ssize_t)dims[0], (py::ssize_t)dims[1], (py::ssize_t)dims[2]});
+              unsigned long long cnt[4] = {0, 0, 0, 0};
+              const float* vp = vertices.data();
+              const int* tp = triangles.data();
+              float* op = out.mutable_data();
+              const int nv = (int)vertices.shape(0), nt = (int)triangles.shape(0);
+              int rc;
+              {
+                  py::gil_scoped_release nogil;
+                  rc = rs_sdf_bake(vp, nv, tp, nt, o.data(), spacing, dims[0], dims[1], dims[2], thickness, round, op, 0,
+                                   nullptr, counters ? cnt : nullptr);
+              }
+              ok(rc);
+              if (!counters) return py::object(out);
+              return py::object(py::make_tuple(out, cnt[0], cnt[1], cnt[2]));
+          },
+          py::arg("vertices"), py::arg("triangles"), py::arg("origin"), py::arg("spacing"), py::arg("dims"),
+          py::arg("thickness") = 0.f, py::arg("round") = 0.f, py::arg("counters") = false);
+
     py::class_<CudaView>(m, "CudaView")
         .def_property_readonly("__cuda_array_interface__", [](const CudaView& v) {
             py::dict d;

@@ -17,7 +17,7 @@ from dataclasses import dataclass
 import numpy as np
 
 __all__ = ["SdfGrid", "from_function", "sdf_box", "sdf_sphere", "sdf_cylinder", "sdf_bowl", "sdf_capsule",
-           "bake_mesh"]
+           "bake_mesh", "is_closed"]
 
 
 @dataclass
@@ -147,15 +147,55 @@ def sdf_capsule(radius, half_length, axis=2, centre=(0.0, 0.0, 0.0)):
     return phi
 
 
+def is_closed(triangles):
+    """True when every undirected edge belongs to exactly two triangles (closed, manifold)."""
+    t = np.asarray(triangles, np.int64).reshape(-1, 3)
+    if t.size == 0:
+        return False
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    e.sort(axis=1)
+    _, counts = np.unique(e, axis=0, return_counts=True)
+    return bool(np.all(counts == 2))
+
+
 def bake_mesh(vertices, triangles, spacing, margin, thickness=0.0, round=0.0, device=None):
-    """Triangle-mesh baking needs NVIDIA Warp in the reference (ropesim/sdf.py:96-156); it is
-    not on the substep path and Warp is not part of this build. Closed forms and
-    from_function() cover the benchmark scenes."""
-    try:
-        import warp  # noqa: F401
-    except ImportError as e:
-        raise ImportError("bake_mesh needs warp-lang; use from_function() with a closed form instead") from e
-    raise NotImplementedError("bake_mesh is not part of this build; use from_function()")
+    """Distance lattice of a triangle mesh on its padded bounding box, baked on the GPU
+    (the reference's bake_mesh, ropesim/sdf.py:96-156, which needs Warp; here the library's own
+    sm_100a kernels, no Warp).
+
+    vertices [V, 3], triangles [T, 3], any winding. thickness == 0: the SIGNED distance, negative
+    inside (generalized winding number of magnitude > 1/2); the mesh must be closed (every edge
+    shared by exactly two triangles; weld unwelded exports first). thickness > 0: a two-sided
+    shell, |distance| - thickness / 2, for open meshes (sheets, heightfields); thickness must be
+    >= 2 * spacing so that both faces keep a gradient. round > 0 offsets the surface outward
+    (phi - round), rounding convex edges by that radius. margin pads the box beyond the shell and
+    rounding on every side (use >= rope radius + a few cells). `device` is accepted for the
+    reference's signature; the current CUDA device bakes.
+    """
+    from ._ropesim import bake_sdf
+
+    vertices = np.asarray(vertices, np.float32).reshape(-1, 3)
+    triangles = np.asarray(triangles, np.int32).reshape(-1, 3)
+    if len(vertices) < 3 or len(triangles) < 1:
+        raise ValueError("bake_mesh needs a triangle mesh")
+    if triangles.min() < 0 or triangles.max() >= len(vertices):
+        raise ValueError("triangle indices out of range")
+    if thickness > 0:
+        if thickness < 2 * spacing:
+            raise ValueError("thickness must be >= 2 * spacing (one cell on each side of the mid-surface)")
+    elif not is_closed(triangles):
+        raise ValueError("open mesh (an edge is not shared by exactly two triangles): a signed distance has no "
+                         "inside. Weld a watertight but unwelded export first, or pass thickness >= 2 * spacing "
+                         "to bake a two-sided shell")
+    if round < 0:
+        raise ValueError("round must be >= 0")
+    pad = margin + 0.5 * thickness + round
+    lo, hi = vertices.min(0) - pad, vertices.max(0) + pad
+    origin, dims = _lattice(lo, hi, spacing)
+    values = bake_sdf(vertices, triangles, origin, float(spacing), list(dims), float(thickness), float(round))
+    if not np.isfinite(values).all():
+        raise ValueError("bake_mesh produced non-finite distances")
+    return SdfGrid(values, origin, float(spacing))
 
 
 def _roundtrip_check():  # pragma: no cover - developer aid

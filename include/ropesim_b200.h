@@ -202,8 +202,10 @@ RS_API int rs_batch_contact_views(rs_batch* b, float** forces, float** wrenches)
  * No counterpart in the reference, which has no gradients. What is differentiated is the
  * deterministic substep (root program, inertial prediction, num_itr x (position step with
  * inertia, plane contact and friction, stretch, damping; frame step), velocity with linear and
- * quadratic drag); branches (contact active, friction regime, frame-step signs) are held where
- * the forward pass took them. Rope-rope and mesh contact are refused (RS_EINVAL).
+ * quadratic drag), with plane, static SDF-mesh and rope-rope contact (barrier, damping,
+ * friction, closest points, step limit); branches (contact active, friction regime, frame-step
+ * signs, step-limit clips) are held where the forward pass took them. A frame during which a
+ * mesh moves is refused (RS_EINVAL).
  *
  * State: pos / vel / lvel [n,3], q [n,4], caller order; lvel is the velocity at the last
  * substep's start (the next substep's initial guess extrapolates from it). Parameters: ea / ei
@@ -261,6 +263,24 @@ RS_API int rs_batch_frame_forward(rs_batch* b, const rs_frame_io* io, float dt, 
  * program, caller order), so that the backward need not replay the frame. */
 RS_API int rs_batch_step_program_taped(rs_batch* b, const float* p0, const float* v0, const float* p1,
                                        const float* q0, const float* q1, float dt, int substeps, float* tape);
+
+/* ---------------------------------------------------------------- mesh baking
+ * Replaces ropesim.sdf.bake_mesh's Warp kernel (ropesim/sdf.py:96-167): the signed distance of
+ * every node origin + (i, j, k) * spacing (float32 of the float64 sum, C order [nx, ny, nz]) to
+ * a triangle mesh (host vertices [num_vertices, 3], host triangles [num_triangles, 3], any
+ * winding): exact closest-point distance, negative where the generalized winding number's
+ * magnitude exceeds 1/2 (inside a closed mesh). thickness > 0 bakes the two-sided shell
+ * |distance| - thickness / 2 instead (open meshes); round > 0 subtracts round. The lattice box
+ * and the closedness check are the caller's (the Python bake_mesh does both as the reference).
+ * out: host memory (out_on_device = 0; the call returns when it is filled) or device memory
+ * (out_on_device = 1; queued on `stream`, NULL = the legacy default stream). counters: NULL or
+ * host [4] receiving the point-triangle distances, line-triangle crossing tests and solid
+ * angles evaluated and the kernels' device time in nanoseconds, the host preparation (triangle
+ * sort and upload) excluded; the call then synchronizes. Zero-area triangles are dropped. RS_EINVAL on
+ * bad sizes or indices, or more than 7000 nodes along z. */
+RS_API int rs_sdf_bake(const float* vertices, int num_vertices, const int* triangles, int num_triangles,
+                       const float* origin3, double spacing, int nx, int ny, int nz, float thickness, float round,
+                       float* out, int out_on_device, void* stream, unsigned long long* counters);
 
 /* ---------------------------------------------------------------- measurement
  * Measured FP32 FMA throughput of the current device in TFLOP/s (2 FLOP per FMA), from a

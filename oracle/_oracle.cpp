@@ -11,6 +11,7 @@
 #include "rs_adjoint.hpp"
 #include "rs_opcount.hpp"
 #include "rs_oracle.hpp"
+#include "rs_sdfbake_oracle.hpp"
 
 namespace py = pybind11;
 using f32a = py::array_t<float, py::array::c_style | py::array::forcecast>;
@@ -237,4 +238,22 @@ PYBIND11_MODULE(_oracle, m) {
     m.def("count_program_ops", &count_program_ops, py::arg("positions"), py::arg("density"), py::arg("k_stretch"),
           py::arg("k_bend"), py::arg("h"), py::arg("num_itr"), py::arg("p0"), py::arg("v0"), py::arg("p1"), py::arg("dt"),
           py::arg("substeps"), py::arg("planes") = py::none(), py::arg("radius") = 0.f);
+    // FP64 brute-force mesh bake: (phi, distance, winding number), each [nx, ny, nz] float64
+    m.def("bake_sdf", [](f32a verts, i32a tris, f32a origin, double spacing, std::vector<int> dims, double thickness,
+                         double round, int threads) {
+        rso::BakeOut o;
+        {
+            py::gil_scoped_release nogil;
+            o = rso::bake_sdf(verts.data(), (int)verts.shape(0), tris.data(), (int)tris.shape(0), origin.data(), spacing,
+                              dims[0], dims[1], dims[2], thickness, round,
+                              threads > 0 ? threads : (int)std::thread::hardware_concurrency());
+        }
+        auto arr = [&](const std::vector<double>& v) {
+            py::array_t<double> a({(py::ssize_t)dims[0], (py::ssize_t)dims[1], (py::ssize_t)dims[2]});
+            std::copy(v.begin(), v.end(), a.mutable_data());
+            return a;
+        };
+        return py::make_tuple(arr(o.phi), arr(o.dist), arr(o.wind));
+    }, py::arg("vertices"), py::arg("triangles"), py::arg("origin"), py::arg("spacing"), py::arg("dims"),
+       py::arg("thickness") = 0.0, py::arg("round") = 0.0, py::arg("threads") = 0);
 }

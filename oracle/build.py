@@ -1,6 +1,7 @@
 """Build recipe for the CPU test oracle (TEST INFRASTRUCTURE ONLY).
 
-Compiles oracle/_oracle.cpp (pybind11 binding of rs_oracle.hpp) into an in-tree
+Compiles oracle/_oracle.cpp (pybind11 binding of rs_oracle.hpp, rs_adjoint.hpp and
+rs_sdfbake_oracle.hpp) into an in-tree
 extension module with the host compiler. No fast-math: the restatement keeps IEEE
 float/double arithmetic. The reference itself is not built here: it needs GLM, which
 is not present in this image.
@@ -25,7 +26,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     out = ext_path()
     srcs = [os.path.join(HERE, "_oracle.cpp"), os.path.join(HERE, "rs_oracle.hpp"), os.path.join(HERE, "rs_opcount.hpp"),
-            os.path.join(HERE, "rs_adjoint.hpp")]
+            os.path.join(HERE, "rs_adjoint.hpp"), os.path.join(HERE, "rs_sdfbake_oracle.hpp")]
     if not force and os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(s) for s in srcs):
         return out
     cmd = [
