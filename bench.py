@@ -684,11 +684,13 @@ def run_config4(args):
                                    tape=False if args.no_tape else ("iterates" if args.iterate_tape else True))
                     loss = loss + ((cur[0].view(R, V, 3)[:, -1] - tgt[f]) ** 2).sum(-1).mean()
                 loss.backward()
-                grads["finite"] = bool(all(torch.isfinite(t.grad).all() for t in st + par + pr))
-                grads["loss"] = float(loss.detach())
+                grads["tensors"] = [t.grad for t in st + par + pr]  # checked after the timed rollouts
+                grads["loss_t"] = loss.detach()
 
             timed(fwd_bwd, args.warmup)
             msb = timed(fwd_bwd, args.steps)
+            grads["finite"] = bool(all(torch.isfinite(t).all() for t in grads["tensors"]))
+            grads["loss"] = float(grads["loss_t"])
             out["fwd_bwd"] = {"ms_per_rollout": float(np.mean(msb)), "value": nv * S4 * F * len(msb) / (sum(msb) * 1e-3),
                               "grads_finite": grads["finite"], "loss": grads["loss"]}
         del b

@@ -98,6 +98,9 @@ __device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, 
     f3 lo, hi;
     world_box(lo_o, hi_o, Pp, Pq, lo, hi);
     store_pose(out, Pp, Pq, Pv, Pw, lo, hi);
+    // the broad phase's padding for the mesh's own travel over one substep (contact.cuh:121-136),
+    // once per pose instead of once per vertex; static poses keep 0 in this slot
+    out[4].w = a.sdf_moving ? a.h * (len(Pv) + len(Pw) * 0.5f * len(hi - lo)) : 0.f;
 }
 
 // Surfaces (planes, then candidate meshes in ascending index) at one probe point,
@@ -410,10 +413,10 @@ __device__ __forceinline__ uint64_t build_candidates(const FrameArgs& a, const f
     uint64_t mask = 0ull;
     int cnt = 0;
     for (int m = 0; m < nsdf; m++) {
-        const PoseV P = load_pose(cache + m * kPoseF4);
-        const float pm = pad + (a.sdf_moving ? a.h * (len(P.vel) + len(P.om) * 0.5f * len(P.hi - P.lo)) : 0.f);
-        if (p.x >= P.lo.x - pm && p.x <= P.hi.x + pm && p.y >= P.lo.y - pm && p.y <= P.hi.y + pm && p.z >= P.lo.z - pm &&
-            p.z <= P.hi.z + pm) {
+        const float4 e3 = cache[m * kPoseF4 + 3], e4 = cache[m * kPoseF4 + 4];  // (.., lo), (hi, travel pad)
+        const float pm = pad + e4.w;
+        if (p.x >= e3.y - pm && p.x <= e4.x + pm && p.y >= e3.z - pm && p.y <= e4.y + pm && p.z >= e3.w - pm &&
+            p.z <= e4.z + pm) {
             mask |= 1ull << m;
             cnt++;
         }
