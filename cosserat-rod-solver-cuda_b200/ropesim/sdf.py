@@ -154,7 +154,10 @@ def is_closed(triangles):
         return False
     e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
     e.sort(axis=1)
-    _, counts = np.unique(e, axis=0, return_counts=True)
+    if e.min() < 0:
+        raise ValueError("triangle indices must be >= 0")
+    key = e[:, 0] * (int(e[:, 1].max()) + 1) + e[:, 1]  # one integer per undirected edge
+    _, counts = np.unique(key, return_counts=True)
     return bool(np.all(counts == 2))
 
 
