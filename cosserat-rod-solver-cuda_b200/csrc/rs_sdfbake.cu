@@ -10,10 +10,10 @@
 //  * Triangles are sorted along a Morton curve of their centroids on the host and grouped in
 //    tiles of 32 with one AABB per tile.
 //  * bake_distance_kernel: one CTA per brick of 4 x 8 x 8 nodes (z fastest, as the lattice's C
-//    order). It first evaluates the tile nearest the brick, then visits every tile but skips
-//    those whose AABB is farther from the brick's box than the brick's current largest
-//    per-node distance (a block max, refreshed every 16 tiles): such a tile cannot lower any
-//    node's minimum. The test keeps a 1e-4 relative margin for the rounding of the box gap.
+//    order), culling per warp (a 1 x 4 x 8 slab): it first evaluates the tile nearest the slab,
+//    then visits every tile but skips those whose AABB is farther from the slab than the slab's
+//    current largest per-node distance (a warp max): such a tile cannot lower any node's
+//    minimum. The test keeps a 1e-4 relative margin for the rounding of the box gap.
 //  * bake_sign_rows_kernel: one warp per lattice row along z counts the signed crossings of the
 //    row's line with the mesh (one pass over the triangles, tiles skipped by their x-y box); the
 //    crossings above a node are its winding number. Crossing predicates are evaluated in double,
@@ -44,7 +44,6 @@ namespace {
 
 constexpr int kBX = 4, kBY = 8, kBZ = 8;  // nodes per CTA brick (256 threads)
 constexpr int kTile = 32;                 // triangles per culling tile
-constexpr int kRefresh = 16;              // tiles evaluated between block-max refreshes
 
 struct BakeArgs {
     const float4* tri;   // [3 T] vertices a, b, c of each triangle (Morton order)
@@ -115,35 +114,35 @@ __device__ __forceinline__ float box_gap2(f3 lo0, f3 hi0, float4 lo1, float4 hi1
     return gx * gx + gy * gy + gz * gz;
 }
 
-__device__ __forceinline__ float block_max_nonneg(float v, unsigned* red) {
-    // non-negative floats order like their bit patterns
-    unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(v));
-    __syncthreads();  // the previous reduction's readers are done with red[]
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = u;
-    __syncthreads();
-    unsigned m = red[0];
+__device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
-    for (int w = 1; w < 8; w++) m = max(m, red[w]);
-    return __uint_as_float(m);
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
+// One CTA per brick of 4 x 8 x 8 nodes (z fastest, coalesced stores); each warp culls for its own
+// 1 x 4 x 8 slab of the brick: it evaluates the tile nearest its slab first, then skips every
+// tile whose AABB is farther from the slab than the slab's largest current minimum (a warp max,
+// refreshed after every 4 evaluated tiles), which cannot lower any of its nodes' minima. No CTA
+// barriers: warps proceed independently.
 __global__ void __launch_bounds__(256) bake_distance_kernel(const BakeArgs A) {
-    __shared__ unsigned red[8];
-    __shared__ float2 amin[8];
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31;
     const int i0 = blockIdx.x * kBX, j0 = blockIdx.y * kBY, k0 = blockIdx.z * kBZ;
     const int i = i0 + (t >> 6), j = j0 + ((t >> 3) & 7), k = k0 + (t & 7);
     const bool valid = i < A.nx && j < A.ny && k < A.nz;
+    if (__ballot_sync(0xffffffffu, valid) == 0u) return;  // a whole warp outside the lattice
     const f3 p = mk3(node_coord(A.ox, A.sp, min(i, A.nx - 1)), node_coord(A.oy, A.sp, min(j, A.ny - 1)),
                      node_coord(A.oz, A.sp, min(k, A.nz - 1)));
-    const f3 blo = mk3(node_coord(A.ox, A.sp, i0), node_coord(A.oy, A.sp, j0), node_coord(A.oz, A.sp, k0));
-    const f3 bhi = mk3(node_coord(A.ox, A.sp, min(i0 + kBX - 1, A.nx - 1)), node_coord(A.oy, A.sp, min(j0 + kBY - 1, A.ny - 1)),
+    // the warp's slab: node i, rows jw .. jw + 3, columns k0 .. k0 + 7 (clamped to the lattice)
+    const int jw = j0 + (((t >> 5) & 1) << 2);
+    const f3 blo = mk3(node_coord(A.ox, A.sp, i), node_coord(A.oy, A.sp, jw), node_coord(A.oz, A.sp, k0));
+    const f3 bhi = mk3(node_coord(A.ox, A.sp, i), node_coord(A.oy, A.sp, min(jw + 3, A.ny - 1)),
                        node_coord(A.oz, A.sp, min(k0 + kBZ - 1, A.nz - 1)));
 
-    // the tile nearest the brick (smallest box gap, lowest index on ties) seeds the bound
+    // the tile nearest the slab (smallest box gap, lowest index on ties) seeds the bound
     float lb = INFINITY;
     int tb = 0;
-    for (int e = t; e < A.tiles; e += 256) {
+    for (int e = lane; e < A.tiles; e += 32) {
         const float g = box_gap2(blo, bhi, __ldg(A.tbox + 2 * e), __ldg(A.tbox + 2 * e + 1));
         if (g < lb) { lb = g; tb = e; }
     }
@@ -153,14 +152,7 @@ __global__ void __launch_bounds__(256) bake_distance_kernel(const BakeArgs A) {
         const int e = __shfl_xor_sync(0xffffffffu, tb, o);
         if (g < lb || (g == lb && e < tb)) { lb = g; tb = e; }
     }
-    if ((t & 31) == 0) amin[t >> 5] = make_float2(lb, __int_as_float(tb));
-    __syncthreads();
-    int seed = __float_as_int(amin[0].y);
-    float sl = amin[0].x;
-    for (int w = 1; w < 8; w++) {
-        const int e = __float_as_int(amin[w].y);
-        if (amin[w].x < sl || (amin[w].x == sl && e < seed)) { sl = amin[w].x; seed = e; }
-    }
+    const int seed = tb;
 
     float best = INFINITY;
     long long evals = 0;
@@ -173,22 +165,22 @@ __global__ void __launch_bounds__(256) bake_distance_kernel(const BakeArgs A) {
         evals += q1 - e * kTile;
     };
     eval_tile(seed);
-    float U2 = block_max_nonneg(valid ? best : 0.f, red);
+    float U2 = warp_max(valid ? best : 0.f);
     int since = 0;
     for (int e = 0; e < A.tiles; e++) {
         if (e == seed) continue;
         const float g = box_gap2(blo, bhi, __ldg(A.tbox + 2 * e), __ldg(A.tbox + 2 * e + 1));
-        if (g > U2 * (1.f + 1e-4f)) continue;  // uniform: every thread sees the same g and U2
+        if (g > U2 * (1.f + 1e-4f)) continue;  // uniform over the warp: same g and U2 in every lane
         eval_tile(e);
-        if (++since == kRefresh) {
+        if (++since == 4) {
             since = 0;
-            U2 = block_max_nonneg(valid ? best : 0.f, red);
+            U2 = warp_max(valid ? best : 0.f);
         }
     }
     if (valid) A.out[((size_t)i * A.ny + j) * A.nz + k] = sqrtf(best);
     if (A.counters) {
-        const int nvalid = __syncthreads_count(valid);
-        if (t == 0) atomicAdd(A.counters, (unsigned long long)(evals * nvalid));
+        const int nvalid = __popc(__ballot_sync(0xffffffffu, valid));
+        if (lane == 0) atomicAdd(A.counters, (unsigned long long)(evals * nvalid));
     }
 }
 

@@ -5,7 +5,7 @@
  * handles, host or device float pointers with explicit sizes, `int` status codes and a
  * thread-local error string. No torch or pybind11 types cross it. The pybind11 module
  * `ropesim._ropesim` of this repository is one client; ctypes / cffi clients work the same way
- * (see INTEGRATION.md).
+ * (load libropesim_b200.so, declare these signatures, pass device addresses as integers).
  *
  * Layout conventions: "caller order" is the reference's flat order (rope r owns its vertices
  * consecutively, ropes in index order). Rotors are (x, y, z, w). All device pointers are

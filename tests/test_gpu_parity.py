@@ -1,9 +1,9 @@
 """Parity of the CUDA product against the FP64 oracle (and its FP32 instantiation).
 
-Bounds, stated per scene (the north-star tolerance is 1e-5 m over 60 control frames):
-  * well-posed scenes (config 1 hanging rope, gentle program driving, clamped legacy roots):
+Bounds, stated per scene (the target tolerance is 1e-5 m of vertex deviation over 60 control frames):
+  * well-posed scenes (the 33-vertex hanging rope, gentle program driving, clamped legacy roots):
     max |x_gpu - x_f64| <= 1e-5 m over every frame;
-  * chaotic scenes (config 2's random whipping, config 3's uneven ropes in mesh/plane
+  * chaotic scenes (the 4096 x 64 whipping workload, uneven ropes in mesh/plane
     contact): rounding is amplified by the dynamics itself (the FP32 and FP64 oracles part by
     mm), so the bound is the FP32 noise floor: the GPU may deviate from FP64 by at most
     4x the FP32 oracle's own deviation + 1e-6 m, and by <= 1e-5 m after the first frame.
