@@ -613,7 +613,7 @@ def run_config4(args):
 
     torch.cuda.set_device(0)
     R = args.ropes if args.ropes != 4096 else 1024
-    V, F, S4 = 64, args.frames, 100
+    V, F, S4 = 64, args.frames or 30, 100
     seg, density, ea, ei = 0.03, 0.1, 500.0, 1e-4
     rng = np.random.default_rng(4)
     roots = np.stack([rng.uniform(-0.5, 0.5, R), rng.uniform(-0.5, 0.5, R), rng.uniform(2.5, 3.5, R)], 1).astype(np.float32)
@@ -774,7 +774,7 @@ def run_config5(args):
 
     torch.cuda.set_device(0)
     R = args.ropes if args.ropes != 4096 else 256
-    V, F, S5 = 128, args.frames, 100
+    V, F, S5 = 128, args.frames or 60, 100
     iters = args.iters or ITERS
     pos, ea_true, ei_true, lattice = config5_scene(R, V)
     Rc = 0.005
@@ -1090,7 +1090,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
     ap.add_argument("--block", type=int, default=0, help="bin size (CTA threads); 0 = the library's choice")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
-    ap.add_argument("--frames", type=int, default=30, help="config4: control frames per rollout")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="control frames per rollout (0 = the workload's own: 30 for config4, 60 for config5)")
     ap.add_argument("--no-tape", action="store_true", help="config4: backward replays frames instead of keeping tapes")
     ap.add_argument("--no-iterate-tape", dest="iterate_tape", action="store_false",
                     help="config4: keep only the substep tapes (the backward recomputes the iterates)")

@@ -631,7 +631,9 @@ void Batch::run_frame_plain(const FrameArgs& a) {
     plain_alloc();
     check(cudaStreamSynchronize(stream_), "plain args reuse");  // the previous frame read h_pl_args_
     *h_pl_args_ = a;
-    h_pl_args_->sdf_skip = 0;  // the plain path samples every candidate lattice, as the reference does
+    // as the in-repo baseline the plain path samples every candidate lattice, as the reference does;
+    // as the product path of contact groups larger than a CTA it keeps the exact block skip
+    h_pl_args_->sdf_skip = engine_ == 1 ? 0 : 1;
     check(cudaMemcpyAsync(d_pl_args_, h_pl_args_, sizeof(FrameArgs), cudaMemcpyHostToDevice, stream_), "upload(args)");
     const int surf = a.num_sdf > 0 ? 2 : (a.num_planes > 0 ? 1 : 0);
     const std::string key = std::to_string(a.iters) + ":" + std::to_string(surf) + ":" + std::to_string(a.rope_contact);
