@@ -110,6 +110,14 @@ __global__ void rg_query_kernel(const FrameArgs* __restrict__ pa, const float4* 
                     const int j = g.sorted[k];
                     if (j < gr.x || j >= gr.y) continue;
                     if (j >= gr.z && j < gr.w && abs(j - d) <= 2) continue;
+                    // conservative pre-test on the cached midpoints and reaches (one load instead of
+                    // four): its bound exceeds pair_accepts' own by 1e-4 relative + 1e-6 m, far more
+                    // than the rounding between the two forms, so it rejects only pairs that
+                    // pair_accepts rejects as well
+                    const float4 mj = g.ms[j];
+                    const f3 dq = xyz(mj) - xyz(md);
+                    const float rq = (md.w + mj.w) * 1.0002f + 2e-6f;
+                    if (dot(dq, dq) > rq * rq) continue;
                     const f3 pj0 = xyz(pos[j]), pj1 = xyz(pos[j + 1]);
                     if (!pair_accepts(p, a1, mt, ht, ri, pj0, pj1, fmaxf(a.pad[j], a.pad[j + 1]))) continue;
                     // insert into the sorted unique list
