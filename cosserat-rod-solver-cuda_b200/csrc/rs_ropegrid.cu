@@ -5,11 +5,13 @@
 // of 32,768 segments). Here each substep: (1) every segment's midpoint m and reach s (half length
 // + padded radius) and the largest reach; (2) the midpoint's cell (edge c = 2 s_max + margin)
 // hashed into T buckets, counted; (3) an exclusive scan (CUB) and a scatter sort the segments by
-// bucket; (4) each segment visits the 27 cells around its own. Any pair that passes
+// bucket; (4) one thread per (segment, cell) scans the 27 cells around each segment's own and
+// appends the accepted candidates; (5) each segment sorts its list. Any pair that passes
 // detect_group's early out has midpoints closer than c, so the partner sits in one of those
 // cells: the visited set contains every candidate, each visited pair runs detect_group's own pair
-// test (pair_accepts), and the accepted indices are kept sorted and unique (a hash can alias two
-// neighbour cells). That sorted list is the brute force's ascending list. A segment with more
+// test (pair_accepts), each bucket is scanned once per segment (a hash can alias two neighbour
+// cells), and the accepted indices are sorted. That sorted list is the brute force's ascending
+// list. A segment with more
 // than kMaxCols candidates reruns the brute force, which keeps the first kMaxCols and flags
 // MAX_COLLISIONS as the reference does.
 #include <cub/cub.cuh>
@@ -33,6 +35,7 @@ __global__ void rg_reach_kernel(const FrameArgs* __restrict__ pa, const float4* 
     const FrameArgs& a = *pa;
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
+    a.ncols[d] = 0;  // the cell pass counts this segment's candidates here
     if (!(a.topo[d].x & F_NEXT)) {
         g.ms[d] = make_float4(0.f, 0.f, 0.f, -1.f);
         return;
@@ -72,14 +75,59 @@ __global__ void rg_scatter_kernel(RopeGrid g, int n) {
     g.sorted[g.start[b] + atomicAdd(g.count + b, 1)] = d;
 }
 
-// Candidates of segment d from the 27 cells around its midpoint; `pos` are the substep-start
-// positions (device order). `flag` raises MAX_COLLISIONS like the brute-force kernel.
-__global__ void rg_query_kernel(const FrameArgs* __restrict__ pa, const float4* __restrict__ pos, RopeGrid g, int n,
-                                int flag) {
+// Candidates of every segment from the 27 cells around its midpoint, one thread per (segment,
+// cell): the thread scans the cell's bucket (skipped when an earlier cell of the same segment
+// hashes to the same bucket, so each candidate is found once) and appends the accepted indices,
+// unordered, to the segment's column list, counting them in ncols. `pos` are the substep-start
+// positions (device order).
+__global__ void rg_cells_kernel(const FrameArgs* __restrict__ pa, const float4* __restrict__ pos, RopeGrid g, int n) {
+    const FrameArgs& a = *pa;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 27LL * n) return;
+    const int d = (int)(t / 27), c = (int)(t - 27LL * d);
+    if (!(a.topo[d].x & F_NEXT)) return;
+    const float4 md = g.ms[d];
+    if (md.w < 0.f) return;  // diverged: no candidates
+    const float ce = cell_edge(g);
+    const int cx = (int)floorf(md.x / ce), cy = (int)floorf(md.y / ce), cz = (int)floorf(md.z / ce);
+    auto bucket_of = [&](int k) { return hash_cell(cx + k % 3 - 1, cy + (k / 3) % 3 - 1, cz + k / 9 - 1, g.T); };
+    const int b = bucket_of(c);
+    for (int k = 0; k < c; k++)
+        if (bucket_of(k) == b) return;
+    const int4 gr = a.grp[d];
+    const f3 p = xyz(pos[d]), p1 = xyz(pos[d + 1]);
+    const f3 a1 = p1 - p;
+    const float ri = fmaxf(a.pad[d], a.pad[d + 1]);
+    const f3 mt = p + a1 * 0.5f;
+    const float ht = 0.5f * len(a1);
+    const int e = g.start[b + 1];
+    for (int k = g.start[b]; k < e; k++) {
+        const int j = g.sorted[k];
+        if (j < gr.x || j >= gr.y) continue;
+        if (j >= gr.z && j < gr.w && abs(j - d) <= 2) continue;
+        // conservative pre-test on the cached midpoints and reaches (one load instead of four): its
+        // bound exceeds pair_accepts' own by 1e-4 relative + 1e-6 m, far more than the rounding
+        // between the two forms, so it rejects only pairs that pair_accepts rejects as well
+        const float4 mj = g.ms[j];
+        const f3 dq = xyz(mj) - xyz(md);
+        const float rq = (md.w + mj.w) * 1.0002f + 2e-6f;
+        if (dot(dq, dq) > rq * rq) continue;
+        const f3 pj0 = xyz(pos[j]), pj1 = xyz(pos[j + 1]);
+        if (!pair_accepts(p, a1, mt, ht, ri, pj0, pj1, fmaxf(a.pad[j], a.pad[j + 1]))) continue;
+        const int q = atomicAdd(a.ncols + d, 1);
+        if (q < kMaxCols) a.cols[(size_t)q * n + d] = j;
+    }
+}
+
+// Per segment: its candidates sorted ascending (the brute force's order) and its step limit; more
+// than kMaxCols candidates rerun the brute force, which keeps the first kMaxCols and flags
+// MAX_COLLISIONS as the reference does (`flag`).
+__global__ void rg_finish_kernel(const FrameArgs* __restrict__ pa, const float4* __restrict__ pos, RopeGrid g, int n,
+                                 int flag) {
     const FrameArgs& a = *pa;
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
-    if (!(a.topo[d].x & F_NEXT)) {
+    if (!(a.topo[d].x & F_NEXT) || g.ms[d].w < 0.f) {
         a.ncols[d] = 0;
         a.maxstep[d] = INFINITY;
         return;
@@ -87,67 +135,31 @@ __global__ void rg_query_kernel(const FrameArgs* __restrict__ pa, const float4* 
     const int4 gr = a.grp[d];
     const f3 p = xyz(pos[d]), p1 = xyz(pos[d + 1]);
     const f3 a1 = p1 - p;
-    const float ri = fmaxf(a.pad[d], a.pad[d + 1]);
-    const f3 mt = p + a1 * 0.5f;
-    const float ht = 0.5f * len(a1);
-    const float4 md = g.ms[d];
-    if (md.w < 0.f) {  // diverged: no candidates
-        a.ncols[d] = 0;
-        a.maxstep[d] = INFINITY;
-        return;
-    }
-    const float c = cell_edge(g);
-    const int cx = (int)floorf(md.x / c), cy = (int)floorf(md.y / c), cz = (int)floorf(md.z / c);
-    int list[kMaxCols];
-    int cnt = 0;
-    bool overflow = false;
-    for (int dz = -1; dz <= 1 && !overflow; dz++)
-        for (int dy = -1; dy <= 1 && !overflow; dy++)
-            for (int dx = -1; dx <= 1 && !overflow; dx++) {
-                const int b = hash_cell(cx + dx, cy + dy, cz + dz, g.T);
-                const int e = g.start[b + 1];
-                for (int k = g.start[b]; k < e; k++) {
-                    const int j = g.sorted[k];
-                    if (j < gr.x || j >= gr.y) continue;
-                    if (j >= gr.z && j < gr.w && abs(j - d) <= 2) continue;
-                    // conservative pre-test on the cached midpoints and reaches (one load instead of
-                    // four): its bound exceeds pair_accepts' own by 1e-4 relative + 1e-6 m, far more
-                    // than the rounding between the two forms, so it rejects only pairs that
-                    // pair_accepts rejects as well
-                    const float4 mj = g.ms[j];
-                    const f3 dq = xyz(mj) - xyz(md);
-                    const float rq = (md.w + mj.w) * 1.0002f + 2e-6f;
-                    if (dot(dq, dq) > rq * rq) continue;
-                    const f3 pj0 = xyz(pos[j]), pj1 = xyz(pos[j + 1]);
-                    if (!pair_accepts(p, a1, mt, ht, ri, pj0, pj1, fmaxf(a.pad[j], a.pad[j + 1]))) continue;
-                    // insert into the sorted unique list
-                    int at = cnt;
-                    while (at > 0 && list[at - 1] > j) at--;
-                    if (at > 0 && list[at - 1] == j) continue;
-                    if (cnt == kMaxCols) {
-                        overflow = true;
-                        break;
-                    }
-                    for (int q = cnt; q > at; q--) list[q] = list[q - 1];
-                    list[at] = j;
-                    cnt++;
-                }
-            }
+    const int cnt = a.ncols[d];
     float lim;
-    if (overflow) {  // more than kMaxCols candidates: the brute force keeps the first kMaxCols
+    if (cnt > kMaxCols) {
         const int total = detect_group(
             a, d, d, gr.x, gr.y, gr.z, gr.w, p, p1, [&](int j) { return a.pad[j]; },
             [&](int j) { return a.topo[j].x; }, [&](int j) { return xyz(pos[j]); }, lim);
         if (flag && total > kMaxCols) atomicMax(a.status, ERR_MAX_COLLISIONS);
         a.ncols[d] = total < kMaxCols ? total : kMaxCols;
     } else {
+        int list[kMaxCols];
+        for (int q = 0; q < cnt; q++) {  // insertion sort (the lists are short)
+            const int j = a.cols[(size_t)q * n + d];
+            int at = q;
+            while (at > 0 && list[at - 1] > j) {
+                list[at] = list[at - 1];
+                at--;
+            }
+            list[at] = j;
+        }
         lim = a.pad[d] - a.det_radius;
         for (int q = 0; q < cnt; q++) {
             const int j = list[q];
             a.cols[(size_t)q * n + d] = j;
             lim = fminf(lim, step_limit_of(p, a1, xyz(pos[j]), xyz(pos[j + 1])));
         }
-        a.ncols[d] = cnt;
     }
     a.maxstep[d] = lim;
 }
@@ -180,7 +192,8 @@ cudaError_t rope_grid_detect(const FrameArgs* pa, const float4* pos, const RopeG
     if (e == cudaSuccess) e = cudaMemsetAsync(g.count, 0, sizeof(int) * (size_t)(g.T + 1), st);
     if (e != cudaSuccess) return e;
     rg_scatter_kernel<<<blocks_of(n, 256), 256, 0, st>>>(g, n);
-    rg_query_kernel<<<blocks_of(n, 128), 128, 0, st>>>(pa, pos, g, n, flag ? 1 : 0);
+    rg_cells_kernel<<<(unsigned)((27LL * n + 127) / 128), 128, 0, st>>>(pa, pos, g, n);
+    rg_finish_kernel<<<blocks_of(n, 128), 128, 0, st>>>(pa, pos, g, n, flag ? 1 : 0);
     return cudaGetLastError();
 }
 
