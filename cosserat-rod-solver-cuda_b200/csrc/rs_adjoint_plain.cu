@@ -23,6 +23,7 @@ namespace {
 
 constexpr int kPosBlock = 128;     // position recompute: 127 owned vertices + the previous halo vertex
 constexpr int kOwned = kPosBlock - 1;
+constexpr int kOwnedRope = kPosBlock / 2 - 1;  // rope-rope recompute: two threads per vertex
 constexpr int kBlock = 128;
 
 __device__ __forceinline__ const float4* static_poses(const FrameArgs& a, int env) {
@@ -142,6 +143,83 @@ __global__ void __launch_bounds__(kPosBlock) padj_position_kernel(const FrameArg
     } else {
         position_solve(dx, f, H, a.accel, im, !touched);
     }
+    b.ld[(size_t)(k + 1) * n + d] = f4(dx, sc);
+}
+
+// Position step k recomputed with rope-rope terms, two threads per vertex: the reference's two
+// candidate sectors (even candidates joining the own terms, odd ones a partial added after them,
+// cosserat.cu:99-182) on their own threads, the same sums in the same order as
+// collision_sectors().
+template <int SURF>
+__global__ void __launch_bounds__(kPosBlock) padj_position_rope_kernel(const FrameArgs* __restrict__ pa, PlainAdjBufs b,
+                                                                       int n, int k) {
+    const FrameArgs& a = *pa;
+    constexpr int V = kPosBlock / 2;
+    __shared__ float4 so[V][5];  // sector 1: fo, f2o, Ho, H2o
+    __shared__ float4 sfa[V], sfb[V];
+    __shared__ float sfc[V];
+    const int lt = threadIdx.x, lv = lt >> 1, sec = lt & 1;
+    const int d = blockIdx.x * kOwnedRope + lv - 1;
+    const bool valid = d >= 0 && d < n;
+    const float4* Dk = b.ld + (size_t)k * n;
+    uint32_t fl = 0;
+    f3 f = zero3(), f2 = zero3(), dx = zero3();
+    sym3 H = sym_zero(), H2 = sym_zero();
+    float im = 0.f;
+    int nc = 0;
+    if (valid) {
+        const int4 tp = a.topo[d];
+        fl = (uint32_t)tp.x;
+        const float4 P = b.x[d];
+        im = P.w;
+        const bool hasNext = fl & F_NEXT;
+        dx = xyz(Dk[d]);
+        const f3 p1 = hasNext ? xyz(b.x[d + 1]) : zero3();
+        const f3 p1dx = hasNext ? xyz(Dk[d + 1]) : zero3();
+        const float damp = a.damping / a.h;
+        nc = hasNext ? a.ncols[d] : 0;
+        if (sec == 0) {
+            const VConst c = vertex_constants(a, im, a.vel[d].w, a.lvel[d].w);
+            const float4* cache = (SURF == SURF_MESHES) ? static_poses(a, tp.w) : nullptr;
+            const uint64_t cand = (SURF == SURF_MESHES) ? b.cand[d] : 0ull;
+            position_terms<SURF>(a, cache, cand, c, hasNext, xyz(P), p1, dx, p1dx, xyz(b.y[d]), b.lq[(size_t)k * n + d],
+                                 damp, f, H, f2, H2);
+        }
+        for (int cc = sec; cc < nc; cc += 2) {
+            const int j = a.cols[(size_t)cc * n + d];
+            collision_term(a, damp, xyz(P), p1, dx, p1dx, xyz(b.x[j]), xyz(b.x[j + 1]), xyz(Dk[j]), xyz(Dk[j + 1]), f, f2,
+                           H, H2);
+        }
+        if (sec == 1) {
+            so[lv][0] = f4(f, f2.x);
+            so[lv][1] = make_float4(f2.y, f2.z, H.xx, H.yy);
+            so[lv][2] = make_float4(H.zz, H.xy, H.xz, H.yz);
+            so[lv][3] = make_float4(H2.xx, H2.yy, H2.zz, H2.xy);
+            so[lv][4] = make_float4(H2.xz, H2.yz, 0.f, 0.f);
+        }
+    }
+    __syncthreads();
+    if (sec == 0) {
+        if (valid && nc > 1) {
+            const float4 o0 = so[lv][0], o1 = so[lv][1], o2 = so[lv][2], o3 = so[lv][3], o4 = so[lv][4];
+            f += xyz(o0);
+            f2 += mk3(o0.w, o1.x, o1.y);
+            sym_add(H, sym3{o1.z, o1.w, o2.x, o2.y, o2.z, o2.w});
+            sym_add(H2, sym3{o3.x, o3.y, o3.z, o3.w, o4.x, o4.y});
+        }
+        sfa[lv] = f4(f2, H2.xx);
+        sfb[lv] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
+        sfc[lv] = H2.yz;
+    }
+    __syncthreads();
+    if (sec != 0 || !valid || lv == 0) return;  // the halo vertex belongs to the previous block
+    if (fl & F_PREV) {
+        const float4 fa = sfa[lv - 1], fb = sfb[lv - 1];
+        f += xyz(fa);
+        H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sfc[lv - 1];
+    }
+    const float lim = (fl & F_PREV) ? fminf(a.maxstep[d], a.maxstep[d - 1]) : a.maxstep[d];
+    const float sc = position_solve_limited(dx, f, H, a.accel, im, lim);
     b.ld[(size_t)(k + 1) * n + d] = f4(dx, sc);
 }
 
@@ -598,7 +676,8 @@ void run_adjoint_plain(const FrameArgs* pa, const AdjArgs& g, const PlainAdjBufs
         if (ROPE && grid) rope_grid_detect(pa, b.x, *grid, n, false, st);
         else if (ROPE) padj_detect_kernel<<<nb, kBlock, 0, st>>>(pa, b, n);
         for (int k = 0; k < iters; k++) {
-            padj_position_kernel<SURF, ROPE><<<blocks_of(n, kOwned), kPosBlock, 0, st>>>(pa, b, n, k);
+            if constexpr (ROPE) padj_position_rope_kernel<SURF><<<blocks_of(n, kOwnedRope), kPosBlock, 0, st>>>(pa, b, n, k);
+            else padj_position_kernel<SURF, ROPE><<<blocks_of(n, kOwned), kPosBlock, 0, st>>>(pa, b, n, k);
             padj_frame_kernel<<<nb, kBlock, 0, st>>>(pa, b, n, k);
         }
         padj_end_kernel<<<nb, kBlock, 0, st>>>(pa, b, n);
