@@ -63,3 +63,26 @@ def test_python_package_imports_and_fails_loudly_without_gpu():
     if not cuda:
         with pytest.raises(RuntimeError):
             ropesim.RopeSim(num_verts=8, dir=np.array([1, 0, 0], np.float32))
+
+
+def test_bake_entry_point_validates_before_device_work():
+    """rs_sdf_bake refuses bad meshes and lattices with RS_EINVAL before touching the device."""
+    import numpy as np
+
+    lib = ctypes.CDLL(LIB)
+    lib.rs_last_error_string.restype = ctypes.c_char_p
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32)
+    f = np.array([[0, 1, 2], [0, 1, 7]], np.int32)  # index 7 is out of range
+    org = np.zeros(3, np.float32)
+    out = np.zeros(8, np.float32)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    F = ctypes.c_float
+    rc = lib.rs_sdf_bake(P(v), 4, P(f), 2, P(org), ctypes.c_double(0.5), 2, 2, 2, F(0.0), F(0.0), P(out), 0, None, None)
+    assert rc == 1 and b"out of range" in lib.rs_last_error_string()
+    f[1, 2] = 3
+    rc = lib.rs_sdf_bake(P(v), 4, P(f), 2, P(org), ctypes.c_double(-1.0), 2, 2, 2, F(0.0), F(0.0), P(out), 0, None, None)
+    assert rc == 1 and b"spacing" in lib.rs_last_error_string()
+    rc = lib.rs_sdf_bake(P(v), 4, P(f), 2, P(org), ctypes.c_double(0.5), 2, 2, 8000, F(0.0), F(0.0), P(out), 0, None, None)
+    assert rc == 1 and b"along z" in lib.rs_last_error_string()
+    rc = lib.rs_sdf_bake(P(v), 4, P(f), 2, P(org), ctypes.c_double(0.5), 2, 2, 2, F(-1.0), F(0.0), P(out), 0, None, None)
+    assert rc == 1 and b"thickness" in lib.rs_last_error_string()
