@@ -198,14 +198,22 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                     position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
                 if constexpr (ROPE)
                     collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, dx, p1dx, f, f2, H, H2);
+                // without rope contact H2 is dd I (position_terms): one float4 carries the exchange
                 EA[t] = f4(f2, H2.xx);
-                EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
-                EC[t].x = H2.yz;
+                if constexpr (ROPE) {
+                    EB[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
+                    EC[t].x = H2.yz;
+                }
                 __syncthreads();
                 if (hasPrev) {
-                    const float4 fa = EA[t - 1], fb = EB[t - 1];
+                    const float4 fa = EA[t - 1];
                     f += xyz(fa);
-                    H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
+                    if constexpr (ROPE) {
+                        const float4 fb = EB[t - 1];
+                        H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += EC[t - 1].x;
+                    } else {
+                        H.xx += fa.w; H.yy += fa.w; H.zz += fa.w;
+                    }
                 }
                 float sc = 1.f;
                 if constexpr (ROPE)

@@ -34,11 +34,11 @@ struct FrameSmem {
     float4 dx[BLOCK];     // current displacement iterate
     float4 p[BLOCK];      // positions at the substep start
     float4 q[2][BLOCK];   // frame rotors, double buffered across frame steps
-    float4 fa[BLOCK];     // segment force on the next vertex (xyz) + H2.xx
-    float4 fb[BLOCK];     // H2.yy, H2.zz, H2.xy, H2.xz
+    float4 fa[BLOCK];     // segment force on the next vertex (xyz) + H2.xx (= dd without rope contact)
+    float4 fb[BLOCK];     // H2.yy, H2.zz, H2.xy, H2.xz (rope contact only)
     float4 qr[BLOCK];     // rest rotation of segment i (vertex i reads slots i-1 and i)
     float4 lv[BLOCK];     // velocity at the previous substep's start (initial-guess extrapolation)
-    float fc[BLOCK];      // H2.yz
+    float fc[BLOCK];      // H2.yz (rope contact only)
     float pad[BLOCK];     // rope-rope detection padding of the substep
     float lim[BLOCK];     // rope-rope step limit of segment i
     int flg[BLOCK];       // vertex flags (rope-rope detection reads the group's)
@@ -266,16 +266,25 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             const bool touched =
                 position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2, btab, mytbox);
             if constexpr (ROPE) collision_sectors(a, ncol, dv, sm.p, sm.dx, damp, p, p1, dx, p1dx, f, f2, H, H2);
+            // Without rope contact the segment's share H2 is its stretch term alone, dd I
+            // (position_terms), so one float4 carries the whole exchange.
             if (act) {
                 sm.fa[t] = f4(f2, H2.xx);
-                sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
-                sm.fc[t] = H2.yz;
+                if constexpr (ROPE) {
+                    sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
+                    sm.fc[t] = H2.yz;
+                }
             }
             __syncthreads();  // B1
             if (hasPrev) {
-                const float4 fa = sm.fa[t - 1], fb = sm.fb[t - 1];
+                const float4 fa = sm.fa[t - 1];
                 f += xyz(fa);
-                H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
+                if constexpr (ROPE) {
+                    const float4 fb = sm.fb[t - 1];
+                    H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
+                } else {
+                    H.xx += fa.w; H.yy += fa.w; H.zz += fa.w;
+                }
             }
             if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
             else position_solve(dx, f, H, a.accel, im, !touched);
