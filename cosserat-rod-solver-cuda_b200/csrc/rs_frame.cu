@@ -47,14 +47,19 @@ struct FrameSmem {
 // The host sizes the CTA's shared memory with 144 B of frame state per thread (rs_batch.cpp).
 static_assert(sizeof(FrameSmem<64>) == 144 * 64 && sizeof(FrameSmem<1024>) == 144 * 1024, "FrameSmem layout");
 
-// Resident CTAs per SM the register allocation targets: 28 warps per SM (<= 72 registers;
-// 24 warps for 256-thread CTAs) without meshes; 24 warps per SM (<= 80 registers) with meshes,
-// where the rarely taken lattice-sampling path spills a few values to L1 (176 B per thread) and
-// the extra resident CTA hides the barrier waits of the vertices that do sample (config 3:
-// 34.3 -> 31.1 ms per frame); 16 warps per SM (<= 128 registers) with rope-rope contact.
+// Resident CTAs per SM the register allocation targets:
+//  - 28 warps per SM (<= 72 registers; 24 warps for 256-thread CTAs) without surfaces, and with
+//    planes in 256-thread bins;
+//  - 20 warps per SM (<= 96 registers; 85 used, so 22 warps resident with 64-thread CTAs) with
+//    planes only in bins of up to 128 threads, where a 72-register cap spills in the sweep and
+//    costs the config-2 frame 2% (3.11 against 3.05 ms);
+//  - 24 warps per SM (<= 80 registers) with meshes, where the rarely taken lattice-sampling path
+//    spills a few values to L1 (176 B per thread) and the extra resident CTA hides the barrier
+//    waits of the vertices that do sample (config 3: 34.3 -> 31.1 ms per frame);
+//  - 16 warps per SM (<= 128 registers) with rope-rope contact.
 #ifndef RS_MIN_BLOCKS
 #define RS_MIN_BLOCKS(B, SURF, ROPE) \
-    ((B) <= 256 ? (((ROPE) ? 512 : (SURF) == SURF_MESHES ? 768 : 896) / (B)) : 1)
+    ((B) <= 256 ? (((ROPE) ? 512 : (SURF) == SURF_MESHES ? 768 : ((SURF) == SURF_PLANES && (B) <= 128) ? 640 : 896) / (B)) : 1)
 #endif
 
 // Mesh part of the contact readout (contact.cuh:172-204) for one warp: every lane calls it
@@ -287,7 +292,11 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
                 }
             }
             if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
-            else position_solve(dx, f, H, a.accel, im, !touched);
+            else if constexpr (SURF == SURF_NONE) position_solve(dx, f, H, a.accel, im, true);
+            // every thread of the CTA runs the sweep, so the vote has the full warp; a warp with
+            // no surface contact skips the 3x3 solve (each lane's result is the same either way)
+            else if (__any_sync(0xffffffffu, touched)) position_solve(dx, f, H, a.accel, im, !touched);
+            else position_solve(dx, f, H, a.accel, im, true);
             if (act) sm.dx[t] = f4(dx, 0.f);
             if constexpr (!ROPE)
                 if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + it) * a.n + a.topo[dv].z, f4(dx, 0.f));

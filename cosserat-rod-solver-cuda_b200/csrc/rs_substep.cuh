@@ -114,13 +114,25 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
                                          float h, f3& f, sym3& H, float* wr, f3* facc, const float* btab = nullptr,
                                          const float4* tbox = nullptr) {
     bool touched = false;
-    for (int pl = 0; pl < a.num_planes; pl++) {
-        const float4 P = a.planes[pl];
+    if (a.num_planes == 1) {
+        // the common single plane as straight-line code: the runtime-bounded loop below costs
+        // the config-2 frame 4% (it keeps the gap test from being scheduled with its neighbours)
+        const float4 P = a.planes[0];
         const f3 n = mk3(P.x, P.y, P.z);
         const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
-        if (gap >= 0.f) continue;
-        surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
-        touched = true;
+        if (gap < 0.f) {
+            surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
+            touched = true;
+        }
+    } else {
+        for (int pl = 0; pl < a.num_planes; pl++) {
+            const float4 P = a.planes[pl];
+            const f3 n = mk3(P.x, P.y, P.z);
+            const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
+            if (gap >= 0.f) continue;
+            surface_contact(n, gap, d, k, h, a.c_mu_s, a.c_mu_k, a.c_vslip, f, H);
+            touched = true;
+        }
     }
     if constexpr (SURF == SURF_MESHES) {
     for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
