@@ -268,8 +268,19 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             f3 f, f2;
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
-            const bool touched =
-                position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2, btab, mytbox);
+            // Planes only: the sweep takes the terms without contact, as with no surfaces, and
+            // flags the lanes whose probe may be in a plane's contact band; those redo their own
+            // terms with contact after the exchange, in the same order (inertia, surfaces,
+            // stretch), so the sweep keeps the register budget of the plane-free kernel.
+            constexpr bool kRedo = SURF == SURF_PLANES && !ROPE;
+            bool touched;
+            if constexpr (kRedo) {
+                position_terms<SURF_NONE>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
+                touched = im != 0.f && near_planes(a, p, dx);
+            } else {
+                touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2,
+                                               btab, mytbox);
+            }
             if constexpr (ROPE) collision_sectors(a, ncol, dv, sm.p, sm.dx, damp, p, p1, dx, p1dx, f, f2, H, H2);
             // Without rope contact the segment's share H2 is its stretch term alone, dd I
             // (position_terms), so one float4 carries the whole exchange.
@@ -291,12 +302,32 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
                     H.xx += fa.w; H.yy += fa.w; H.zz += fa.w;
                 }
             }
+            // every thread of the CTA runs the sweep, so the votes below have the full warp; a warp
+            // with no surface contact skips the 3x3 solve (each lane's result is the same either way)
             if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
             else if constexpr (SURF == SURF_NONE) position_solve(dx, f, H, a.accel, im, true);
-            // every thread of the CTA runs the sweep, so the vote has the full warp; a warp with
-            // no surface contact skips the 3x3 solve (each lane's result is the same either way)
-            else if (__any_sync(0xffffffffu, touched)) position_solve(dx, f, H, a.accel, im, !touched);
-            else position_solve(dx, f, H, a.accel, im, true);
+            else if constexpr (kRedo) {
+                if (__any_sync(0xffffffffu, touched)) {
+                    if (touched) {
+                        f3 g2;
+                        sym3 G2;
+                        touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H,
+                                                       g2, G2);
+                        if (hasPrev) {
+                            const float4 fa = sm.fa[t - 1];
+                            f += xyz(fa);
+                            H.xx += fa.w; H.yy += fa.w; H.zz += fa.w;
+                        }
+                    }
+                    position_solve(dx, f, H, a.accel, im, !touched);
+                } else {
+                    position_solve(dx, f, H, a.accel, im, true);
+                }
+            } else if (__any_sync(0xffffffffu, touched)) {
+                position_solve(dx, f, H, a.accel, im, !touched);
+            } else {
+                position_solve(dx, f, H, a.accel, im, true);
+            }
             if (act) sm.dx[t] = f4(dx, 0.f);
             if constexpr (!ROPE)
                 if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + it) * a.n + a.topo[dv].z, f4(dx, 0.f));

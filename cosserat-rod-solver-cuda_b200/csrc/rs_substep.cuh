@@ -166,6 +166,25 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
     return touched;
 }
 
+// Whether the probe pos + d may be in some plane's contact band: surfaces() decides contact
+// exactly; this flag only has to include every probe it would find in contact. The 1 mm margin
+// covers any difference in evaluating the same gap expression for coordinates up to ~10 km.
+__device__ __forceinline__ bool near_planes(const FrameArgs& a, f3 pos, f3 d) {
+    constexpr float kMargin = 1e-3f;
+    if (a.num_planes == 1) {
+        const float4 P = a.planes[0];
+        const f3 n = mk3(P.x, P.y, P.z);
+        return (dot(n, pos) - P.w) + dot(n, d) - a.c_radius < kMargin;
+    }
+    bool near = false;
+    for (int pl = 0; pl < a.num_planes; pl++) {
+        const float4 P = a.planes[pl];
+        const f3 n = mk3(P.x, P.y, P.z);
+        near |= (dot(n, pos) - P.w) + dot(n, d) - a.c_radius < kMargin;
+    }
+    return near;
+}
+
 // World AABB of a lattice's contact box under the pose (pos, q); an empty box when the lattice
 // can never reach the contact radius.
 __device__ __forceinline__ void contact_box(const GridDesc& g, f3 pos, float4 q, float4* out) {
