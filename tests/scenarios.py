@@ -13,6 +13,8 @@ Scenes restate the benchmark configurations at sizes the FP64 oracle finishes in
             2 planes, sphere/box/capsule meshes with random per-env poses every frame,
             contact-force readout (config 3 at reduced N and frames)
   legacy    constant-velocity roots with clamped root frames (RopeBatch.step legacy path)
+  planes_only  uneven ropes (16..64 verts) swinging onto one or several planes, no meshes,
+            contact-force readout
 """
 from __future__ import annotations
 
@@ -173,6 +175,27 @@ def uneven(mod, sdf_mod, R=6, frames=10, S=50, seed=3, to_dev=None, precision=No
             fo.append(np.asarray(b.contact_forces(), np.float64).reshape(total, 3).copy())
             wr.append(np.asarray(b.mesh_wrenches(), np.float64).copy())
     return np.stack(out), (np.stack(fo) if forces else None), (np.stack(wr) if forces else None), lens
+
+
+def planes_only(mod, planes, R=6, frames=10, S=50, seed=11, to_dev=None, precision=None):
+    """Uneven ropes (16..64 vertices, roots held, 25 degrees from vertical, lowest vertex 2 cm up)
+    swinging onto `planes` alone (no meshes), contact-force readout on: the plane-only kernel
+    with one plane or with several."""
+    kw = {} if precision is None else {"precision": precision}
+    ropes = uneven_ropes(R, seed, lo=16, hi=64)
+    b = mod.RopeBatch.from_ropes(ropes, 0.117, 11473.0, 4.48e-3, 1.0 / 3000.0, 8, **kw)
+    total = sum(len(r) for r in ropes)
+    b.set_gravity(np.array([0, 0, -G], np.float32))
+    b.damping = 0.0
+    b.drag = 0.1
+    b.set_planes(np.asarray(planes, np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
+    b.enable_contact_forces(True)
+    out, fo = [], []
+    for _ in range(frames):
+        b.step_free(1.0 / 60.0, S)
+        out.append(np.asarray(_flat_positions(b), np.float64).copy())
+        fo.append(np.asarray(b.contact_forces(), np.float64).reshape(total, 3).copy())
+    return np.stack(out), np.stack(fo)
 
 
 def _flat_positions(b):

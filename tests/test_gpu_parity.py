@@ -121,6 +121,27 @@ def test_uneven_mesh_contact_noise_floor(mods):
     assert np.abs(ow).max() > 0.0 and np.abs(of).max() > 0.0  # the readout saw contact
 
 
+@pytest.mark.parametrize("planes", [[[0, 0, 1, 0.02]], [[0, 0, 1, 0], [0.3, 0, 1, -0.05], [-0.2, 0.1, 1, -0.03]]],
+                         ids=["one-plane", "three-planes"])
+def test_plane_only_contact_noise_floor(mods, planes):
+    """Plane-only scenes: the sweep flags the lanes near a plane and redoes their terms with
+    contact after the exchange (single plane as straight-line code, several in a loop). Positions
+    and the contact-force readout are held to the FP32 noise floor of the oracle."""
+    rs, orc = mods
+    g, gf = S.planes_only(rs, planes)
+    o, of = S.planes_only(orc, planes, precision="f64")
+    o32, of32 = S.planes_only(orc, planes, precision="f32")
+    d, d32 = dev(g, o), dev(o32, o)
+    touching = int((np.linalg.norm(of, axis=-1) > 0).sum())
+    print(f"\n  {len(planes)} plane(s), 6 uneven ropes, 10 frames: gpu-f64 {d:.2e} m, f32-f64 {d32:.2e} m, "
+          f"first frame {dev(g[0], o[0]):.2e} m; vertex-frames in contact {touching}, |F| max {np.abs(of).max():.2f} N, "
+          f"force dev gpu {np.abs(gf - of).max():.4f} N (f32 {np.abs(of32 - of).max():.4f})")
+    assert touching > 0
+    assert dev(g[0], o[0]) <= 4.0 * dev(o32[0], o[0]) + 1e-6
+    assert d <= 4.0 * d32 + 1e-6
+    assert np.abs(gf[0] - of[0]).max() <= 4.0 * np.abs(of32[0] - of[0]).max() + 1e-3
+
+
 def test_bitwise_replay_and_block_invariance(mods):
     """Fresh objects replay bitwise, and the packed layout (bin size) does not change a single
     bit: every rope's arithmetic is independent of which CTA owns it."""
