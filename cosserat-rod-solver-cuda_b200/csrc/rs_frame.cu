@@ -50,12 +50,13 @@ static_assert(sizeof(FrameSmem<64>) == 144 * 64 && sizeof(FrameSmem<1024>) == 14
 // Resident CTAs per SM the register allocation targets:
 //  - 28 warps per SM (<= 72 registers; 24 warps for 256-thread CTAs) without surfaces, and with
 //    planes in 256-thread bins;
-//  - 20 warps per SM (<= 96 registers; 85 used, so 22 warps resident with 64-thread CTAs) with
+//  - 20 warps per SM (<= 96 registers; 81 used, and registers are allocated per SM sub-partition) with
 //    planes only in bins of up to 128 threads, where a 72-register cap spills in the sweep and
-//    costs the config-2 frame 2% (3.11 against 3.05 ms);
+//    costs a frame of 4096 64-vertex ropes over one plane 2% (3.11 against 3.05 ms);
 //  - 24 warps per SM (<= 80 registers) with meshes, where the rarely taken lattice-sampling path
 //    spills a few values to L1 (176 B per thread) and the extra resident CTA hides the barrier
-//    waits of the vertices that do sample (config 3: 34.3 -> 31.1 ms per frame);
+//    waits of the vertices that do sample (8192 ropes of 16-256 vertices, 8 meshes: 34.3 -> 31.1 ms
+//    per frame);
 //  - 16 warps per SM (<= 128 registers) with rope-rope contact.
 #ifndef RS_MIN_BLOCKS
 #define RS_MIN_BLOCKS(B, SURF, ROPE) \

@@ -115,8 +115,9 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
                                          const float4* tbox = nullptr) {
     bool touched = false;
     if (a.num_planes == 1) {
-        // the common single plane as straight-line code: the runtime-bounded loop below costs
-        // the config-2 frame 4% (it keeps the gap test from being scheduled with its neighbours)
+        // the common single plane as straight-line code: the runtime-bounded loop below costs a
+        // frame of 4096 64-vertex ropes 4% (it keeps the gap test from being scheduled with its
+        // neighbours)
         const float4 P = a.planes[0];
         const f3 n = mk3(P.x, P.y, P.z);
         const float gap = (dot(n, pos) - P.w) + dot(n, d) - a.c_radius;
