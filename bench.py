@@ -1,27 +1,38 @@
 #!/usr/bin/env python
-"""Throughput of the Stable Cosserat Rods substep on B200: vertex-substeps/s.
+"""Throughput of the Stable Cosserat Rods substep on B200: vertex-substeps/s, forward and
+forward + backward, against the plain per-substep-launch path on the same GPU.
 
-Workload (config 2): RopeBatch.from_positions with 4096 ropes x 64 vertices per GPU (seg 0.02 m,
-straight down + N(0, 1e-3) m jitter, vertex 0 pinned), density 0.117 kg/m, EA 11473 N,
-EI 4.48e-3 N m^2, h = 1/6000 s, 8 iterations, 100 substeps per 1/60 s control frame, plane
-z = 0 (radius 6.35 mm), roots on the second-order program: p0 in a 1 m cube (z in [1.4, 2.4]),
-v0 ~ N(0, 0.5) m/s, p1 = p0 + N(0, 0.05) m. Damping 0 and drag 0.2 /s set explicitly.
-One step = one control frame (one persistent kernel launch). Synthetic seeded inputs.
+Default workload (the target configuration): 8192 uneven ropes, V ~ U{16..256} at 2 cm
+(1,107,975 vertices), EA log-U[1e2, 1e4] N and EI log-U[1e-5, 1e-2] N m^2 per rope, per-vertex
+masses x U[0.8, 1.2], two planes, eight kinematic meshes (sphere / box / capsule closed forms on
+64^3 float32 lattices) with per-env random-walk poses every frame, root programs (v0 ~ N(0, 0.1),
+p1 = p0 + N(0, 0.01)), h = 1/6000 s, 8 iterations, 100 substeps per 1/60 s control frame.
+Seeded synthetic inputs (tests/scenarios.py: bench_c3_scene / bench_c3_inputs). One step = one
+control frame: mesh poses in, one persistent kernel launch, status read.
 
-  value   device time of the K timed frames (CUDA events on the solver stream, inputs already
-          resident; L2 flushed between frames outside the events), max over ranks
-  e2e     the same frames through the public API with host buffers: every step copies its
-          root program from pinned host memory and reads the resulting positions back
-  --impl reference: the CPU restatement of the reference's algorithm (the reference itself
-          does not build here: GLM is absent) timed on all host cores, bounded sample.
+  value     device time of the K timed frames (CUDA events on the solver stream; inputs resident
+            in HBM; L2 flushed between frames outside the events), max over ranks
+  e2e       the same frames through the public API from pinned host buffers: every step copies
+            its mesh poses and root program in and reads the positions view back
+  speedup_vs_plain  the same frames through the plain per-substep-launch engine (the
+            reference's launch structure), and the plain engine as the reference's API must run
+            uneven ropes (one RopeBatch per rope length)
+  config2 / config4 / fwd_bwd_over_fwd  the 4096 x 64 config-2 workload and the 1024 x 64
+            differentiable rollouts (forward vs forward + backward), measured in the same run
+  --impl reference: the CPU restatement of the reference's algorithm (the reference's CUDA
+            build needs GLM, absent here) on all host cores, bounded samples of the same scene
 
-Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
+With --gpus N > 1 and no torchrun environment the script re-launches itself under
+torch.distributed.run with N ranks (one per GPU; ropes sharded by rank, no collective on the
+data path).
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -37,50 +48,36 @@ for p in (PKG, os.path.join(ROOT, "tests")):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-METRIC = "vertex-substeps/s"
-N_ROPES, V, S, ITERS, DT = 4096, 64, 100, 8, 1.0 / 60.0
-H = 1.0 / 6000.0
+import scenarios as Sc  # noqa: E402  (the seeded bench scenes, shared with the parity tests)
+
+METRIC = "vertex-substeps/s fwd and fwd+bwd vs plain path, same B200, ≤1e-5 m deviation"
+UNIT = "vertex-substeps/s"
+V, S, ITERS, DT, H = 64, Sc.BENCH_S, Sc.BENCH_ITERS, Sc.BENCH_DT, Sc.BENCH_H
+C2_ROPES, C3_ROPES, M3 = 4096, 8192, 8
 
 
-def c2_inputs(n_ropes, frames, seed):
-    import scenarios as Sc
-
-    pos, roots = Sc.c2_positions(n_ropes, V, seed)
-    rng = np.random.default_rng(seed + 1000)
-    p0 = np.empty((frames, n_ropes, 3), np.float32)
-    v0 = rng.normal(0, 0.5, (frames, n_ropes, 3)).astype(np.float32)
-    p1 = np.empty_like(p0)
-    cur = roots.copy()
-    for f in range(frames):
-        p0[f] = cur
-        p1[f] = (cur + rng.normal(0, 0.05, (n_ropes, 3))).astype(np.float32)
-        cur = p1[f]
-    return pos, p0, v0, p1
-
-
-def configure(b):
-    b.set_gravity(np.array([0, 0, -9.81], np.float32))
-    b.damping = 0.0
-    b.drag = 0.2
-    b.set_planes(np.array([[0, 0, 1, 0]], np.float32), radius=0.00635)
-
-
-def read_flops():
-    path = os.path.join(ROOT, "profiles", "flop_count_config2.txt")
-    for line in open(path):
-        if line.startswith("flops_per_vertex_substep:"):
-            return float(line.split(":")[1])
-    raise RuntimeError("flops_per_vertex_substep missing in " + path)
-
-
-def read_traffic():
-    path = os.path.join(ROOT, "profiles", "frame_kernel_config2.txt")
+def read_profile_value(name, key):
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             return float(line.split(":")[1])
     return None
+
+
+def read_parity():
+    """Summary of tests/test_bench_parity.py's last run on a B200 (profiles/parity_bench_scenes.txt)."""
+    path = os.path.join(ROOT, "profiles", "parity_bench_scenes.txt")
+    if not os.path.exists(path):
+        return None
+    body = "".join(l for l in open(path) if not l.startswith("#"))
+    try:
+        d = json.loads(body)
+    except ValueError:
+        return None
+    d["source"] = "profiles/parity_bench_scenes.txt (tests/test_bench_parity.py on a B200)"
+    return d
 
 
 def measured_peaks():
@@ -144,284 +141,53 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_leg(seconds_target=15.0, threads=None):
-    """The CPU restatement (FP32 instantiation of the oracle) on all host cores: bounded sample
-    of the config-2 workload, ropes split over threads (ropes are independent)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import ropesim_oracle
-
-    threads = threads or os.cpu_count() or 1
-
-    def run(n_ropes, frames):
-        pos, p0, v0, p1 = c2_inputs(n_ropes, frames, 7)
-        chunks = np.array_split(np.arange(n_ropes), threads)
-        sims = []
-        for c in chunks:
-            if len(c) == 0:
-                continue
-            b = ropesim_oracle.RopeBatch.from_positions(pos[c], 0.117, 11473.0, 4.48e-3, H, ITERS, precision="f32")
-            configure(b)
-            sims.append((b, c))
-        t0 = time.perf_counter()
-
-        def work(b, c):
-            for f in range(frames):
-                b.step(p0[f][c], v0[f][c], DT, S, root_pos_end=p1[f][c])
-
-        ts = [threading.Thread(target=work, args=bc) for bc in sims]
-        for t in ts:
-            t.start()
-        for t in ts:
-            t.join()
-        return time.perf_counter() - t0
-
-    probe_ropes = threads
-    t = run(probe_ropes, 1)
-    per = t / (probe_ropes * V * S)
-    n_ropes = int(max(threads, min(N_ROPES, seconds_target / max(per, 1e-12) / (V * S) / 2)))
-    frames = 2
-    t = run(n_ropes, frames)
-    value = n_ropes * V * S * frames / t
-    return {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"{n_ropes} of the {N_ROPES} config-2 ropes x {frames} frames x {S} substeps "
-                      f"(FP32 CPU restatement, {threads} threads, {t:.1f} s)"}
-
-
-def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+# ------------------------------------------------------------------ process plumbing
+def maybe_relaunch(args):
+    """`--gpus N` (N > 1) outside torchrun: re-run this command under torch.distributed.run with
+    N ranks on this node. Inside torchrun, --gpus must equal the world size."""
+    world = os.environ.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != args.gpus:
+            raise SystemExit(f"--gpus {args.gpus} does not match the launcher's WORLD_SIZE {world}")
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import ropesim_oracle
-
-    threads = os.cpu_count() or 1
-    n_ropes = max(threads, int(os.environ.get("RS_REF_ROPES", str(8 * threads))))
-    pos, p0, v0, p1 = c2_inputs(n_ropes, args.warmup + args.steps, 11)
-    chunks = [c for c in np.array_split(np.arange(n_ropes), threads) if len(c)]
-    sims = []
-    for c in chunks:
-        b = ropesim_oracle.RopeBatch.from_positions(pos[c], 0.117, 11473.0, 4.48e-3, H, ITERS, precision="f32")
-        configure(b)
-        sims.append((b, c))
-
-    def frame(f):
-        def work(b, c):
-            b.step(p0[f][c], v0[f][c], DT, S, root_pos_end=p1[f][c])
-
-        ts = [threading.Thread(target=work, args=bc) for bc in sims]
-        for t in ts:
-            t.start()
-        for t in ts:
-            t.join()
-
-    for f in range(args.warmup):
-        frame(f)
-    t0 = time.perf_counter()
-    for f in range(args.warmup, args.warmup + args.steps):
-        frame(f)
-    el = time.perf_counter() - t0
-    value = n_ropes * V * S * args.steps / el
-    sample = (f"{n_ropes} of the {N_ROPES} config-2 ropes per step (64 verts, {S} substeps, {ITERS} itr), "
-              f"FP32 CPU restatement of the reference's algorithm on {threads} threads")
-    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "config2-program-4096x64 (bounded CPU sample)", "ropes_per_step": n_ropes,
-                       "verts_per_rope": V, "substeps": S, "num_itr": ITERS},
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "reference CUDA build unavailable (GLM headers absent); the reference arm is the oracle port"}
-    print(json.dumps(line), flush=True)
-
-
-def config3_scene(n_ropes, seed=3):
-    """Config 3: n_ropes uneven ropes, V ~ U{16..256} at 2 cm, EA log-U[1e2, 1e4] and
-    EI log-U[1e-5, 1e-2] per rope, per-vertex masses x U[0.8, 1.2], two planes, eight meshes
-    (sphere, box, capsule closed forms baked to 64^3 float32 lattices) with per-env poses."""
-    from ropesim import sdf
-
-    rng = np.random.default_rng(seed)
-    verts = rng.integers(16, 257, n_ropes)
-    g = int(np.ceil(np.sqrt(n_ropes)))
-    ropes = []
-    for r in range(n_ropes):
-        L = 0.02 * (verts[r] - 1)
-        root = np.array([(r % g) * 0.7, (r // g) * 0.7, 0.06 + 0.97 * L])
-        tilt = np.deg2rad(rng.uniform(5, 20))
-        az = rng.uniform(0, 2 * np.pi)
-        d = np.array([np.sin(tilt) * np.cos(az), np.sin(tilt) * np.sin(az), -np.cos(tilt)])
-        pts = root + np.outer(np.arange(verts[r]) * 0.02, d)
-        pts[1:] += rng.normal(0, 1e-3, (verts[r] - 1, 3))
-        ropes.append(pts.astype(np.float32))
-    ea = np.exp(rng.uniform(np.log(1e2), np.log(1e4), n_ropes))
-    ei = np.exp(rng.uniform(np.log(1e-5), np.log(1e-2), n_ropes))
-    ea_v = np.concatenate([np.full(v, ea[i]) for i, v in enumerate(verts)]).astype(np.float32)
-    ei_v = np.concatenate([np.full(v, ei[i]) for i, v in enumerate(verts)]).astype(np.float32)
-    m_v = []
-    for i, rope in enumerate(ropes):
-        seg = np.linalg.norm(np.diff(rope.astype(np.float64), axis=0), axis=1)
-        m = np.zeros(len(rope))
-        m[:-1] += 0.5 * 0.117 * seg
-        m[1:] += 0.5 * 0.117 * seg
-        m_v.append(m * rng.uniform(0.8, 1.2, len(rope)))
-    m_v = np.concatenate(m_v).astype(np.float32)
-    n64 = lambda lo, hi: (hi - lo) / 63.0
-    grids = [sdf.from_function(sdf.sdf_sphere(0.12), [-0.2] * 3, [0.2] * 3, n64(-0.2, 0.2)),
-             sdf.from_function(sdf.sdf_box([0.12, 0.08, 0.06], round=0.01), [-0.2] * 3, [0.2] * 3, n64(-0.2, 0.2)),
-             sdf.from_function(sdf.sdf_capsule(0.06, 0.12, axis=0), [-0.2] * 3, [0.2] * 3, n64(-0.2, 0.2))]
-    grids = [grids[i % 3] for i in range(8)]
-    return ropes, verts, ea_v, ei_v, m_v, grids
-
-
-def build_config3(ropesim, scene, engine):
-    ropes, verts, ea_v, ei_v, m_v, grids = scene
-    b = ropesim.RopeBatch.from_ropes(ropes, 0.117, 1000.0, 1e-3, H, ITERS)
-    b.set_stretch_stiffnesses(ea_v)
-    b.set_bend_stiffnesses(ei_v)
-    b.set_masses(m_v)
-    b.set_engine(engine)
-    b.set_gravity(np.array([0, 0, -9.81], np.float32))
-    b.damping = 0.0
-    b.drag = 0.2
-    b.set_planes(np.array([[0, 0, 1, 0], [0.05, 0.0, 1.0, -0.02]], np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
-    for gd in grids:
-        b.add_mesh(*gd.as_args())
-    return b
-
-
-def run_config3(args):
-    """Config 3 forward: persistent (autotuned bins) vs the plain per-substep path, same inputs."""
+    if args.gpus <= 1:
+        return
     import torch
 
-    import ropesim
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import scenarios as Sc
-
-    torch.cuda.set_device(0)
-    R = args.ropes if args.ropes != 4096 else 8192
-    scene = config3_scene(R)
-    ropes, verts = scene[0], scene[1]
-    nv = int(np.sum(verts))
-    rng = np.random.default_rng(17)
-    M = 8
-    frames = args.warmup + args.steps
-    # per-env mesh poses: next to each rope along its length, then a random rigid walk
-    pos0 = np.zeros((R, M, 3), np.float32)
-    for r, rope in enumerate(ropes):
-        L = 0.02 * (len(rope) - 1)
-        for m in range(M):
-            pos0[r, m] = rope[0] + np.array([0.25 * np.cos(0.8 * m), 0.25 * np.sin(0.8 * m), -(0.15 + 0.1 * m) * L])
-    q0 = np.zeros((R, M, 4), np.float32)
-    q0[..., 3] = 1.0
-    poses = []
-    p, q = pos0, q0
-    for f in range(frames):
-        poses.append((torch.as_tensor(p, device="cuda"), torch.as_tensor(q, device="cuda")))
-        p, q = Sc.walk_poses(rng, p, q, step=0.003, ang=0.02)
-    roots = np.stack([r[0] for r in ropes]).astype(np.float32)
-    prog = []
-    cur = roots.copy()
-    for f in range(frames):
-        v0 = rng.normal(0, 0.1, (R, 3)).astype(np.float32)
-        p1 = (cur + rng.normal(0, 0.01, (R, 3))).astype(np.float32)
-        prog.append(tuple(torch.as_tensor(x, device="cuda") for x in (cur, v0, p1)))
-        cur = p1
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    out = {}
-    for engine in ("persistent",) if args.no_plain else ("persistent", "plain"):
-        b = build_config3(ropesim, scene, engine)
-        st = torch.cuda.ExternalStream(b.stream_ptr())
-        ms = []
-        for f in range(frames):
-            b.set_mesh_poses_all(poses[f][0], poses[f][1], teleport=(f == 0))
-            if f >= args.warmup:
-                flush.fill_(float(f))
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(st)
-            b.step(prog[f][0], prog[f][1], DT, S, root_pos_end=prog[f][2])
-            if f >= args.warmup:
-                e1.record(st)
-                e1.synchronize()
-                ms.append(e0.elapsed_time(e1))
-        pos = torch.as_tensor(b.positions()).cpu().numpy()
-        out[engine] = {"ms_per_step": float(np.mean(ms)), "value": nv * S * len(ms) / (sum(ms) * 1e-3),
-                       "finite": bool(np.isfinite(pos).all()), "layout": list(b.layout())}
-        del b
-    if not args.no_plain:
-        out["plain_per_length"] = plain_per_length(ropesim, scene, prog, poses, args, flush)
-    line = {"metric": METRIC, "value": out["persistent"]["value"], "unit": METRIC, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": out["persistent"]["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-3 scene)",
-            "config": {"workload": f"config3-uneven-{R}", "ropes": R, "verts": nv, "verts_per_rope": "U{16..256}",
-                       "substeps": S, "num_itr": ITERS, "planes": 2, "meshes": M, "lattice": "64^3",
-                       "l2": "flushed between frames (256 MB write)"},
-            "persistent": out["persistent"]}
-    if not args.no_plain:
-        line.update({"plain_path": out["plain"], "speedup_vs_plain": out["persistent"]["value"] / out["plain"]["value"],
-                     "plain_per_length": out["plain_per_length"],
-                     "speedup_vs_plain_per_length": out["persistent"]["value"] / out["plain_per_length"]["value"]})
-    print(json.dumps(line), flush=True)
+    if torch.cuda.device_count() < args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} needs {args.gpus} visible GPUs; {torch.cuda.device_count()} found")
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    raise SystemExit(subprocess.call(cmd))
 
 
-def plain_per_length(ropesim, scene, prog, poses, args, flush):
-    """The plain path as the reference's API can run uneven ropes: RopeBatch holds num_envs ropes
-    of one length, so the scene becomes one plain-engine batch per distinct vertex count (each
-    with its own copy of the lattices), stepped in sequence on one stream every frame. Same
-    ropes, stiffnesses, masses, planes, mesh poses and root programs as the single packed batch;
-    a frame is timed with CUDA events on the legacy default stream, which every batch's blocking
-    stream is ordered with."""
+def dist_setup():
+    """(world, rank, local rank, device, dist module or None): one process per GPU over NCCL."""
     import torch
+    import torch.distributed as dist
 
-    ropes, verts, ea_v, ei_v, m_v, grids = scene
-    starts = np.concatenate([[0], np.cumsum(verts)[:-1]])
-    batches = []
-    for V in np.unique(verts):
-        idx = np.nonzero(verts == V)[0]
-        b = ropesim.RopeBatch.from_positions(np.stack([ropes[r] for r in idx]), 0.117, 1000.0, 1e-3, H, ITERS)
-        sel = np.stack([starts[r] + np.arange(V) for r in idx])  # [n_V, V] flat vertex indices
-        b.set_stretch_stiffnesses(ea_v[sel[:, :-1]])
-        b.set_bend_stiffnesses(ei_v[sel[:, :-1]])
-        b.set_masses(m_v[sel])
-        b.set_engine("plain")
-        b.set_gravity(np.array([0, 0, -9.81], np.float32))
-        b.damping = 0.0
-        b.drag = 0.2
-        b.set_planes(np.array([[0, 0, 1, 0], [0.05, 0.0, 1.0, -0.02]], np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
-        for gd in grids:
-            b.add_mesh(*gd.as_args())
-        batches.append((b, torch.as_tensor(idx, device="cuda")))
-    nv = int(np.sum(verts))
-    ms = []
-    nwarm, nsteps = min(args.warmup, 3), min(args.steps, 3)
-    for f in range(nwarm + nsteps):
-        sub = [(b, poses[f][0][i].contiguous(), poses[f][1][i].contiguous(),
-                [prog[f][k][i].contiguous() for k in range(3)]) for b, i in batches]
-        if f >= nwarm:
-            flush.fill_(float(f))
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-        for b, pp, pq, pr in sub:
-            b.set_mesh_poses_all(pp, pq, teleport=(f == 0))
-            b.step(pr[0], pr[1], DT, S, root_pos_end=pr[2])
-        if f >= nwarm:
-            e1.record()
-            e1.synchronize()
-            ms.append(e0.elapsed_time(e1))
-    finite = all(bool(torch.isfinite(torch.as_tensor(b.positions())).all()) for b, _ in batches)
-    res = {"ms_per_step": float(np.mean(ms)), "value": nv * S * len(ms) / (sum(ms) * 1e-3), "batches": len(batches),
-           "steps": nsteps, "finite": finite,
-           "note": "one plain-engine RopeBatch per distinct vertex count (the reference's RopeBatch takes ropes of "
-                   "one length), stepped in sequence"}
-    del batches
-    return res
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+        return world, rank, local, dev, dist
+    return world, rank, local, dev, None
 
 
 def max_over_ranks(x, dist, device):
     """The maximum of a per-rank scalar over every rank: whole-job times are the slowest rank's."""
     import torch
 
+    if dist is None:
+        return float(x)
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
@@ -432,175 +198,423 @@ def job_rate(world, units_per_rank, seconds):
     return world * units_per_rank / seconds
 
 
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-
+def fp32_peak_tflops():
     import ctypes
+
+    lib = ctypes.CDLL(os.path.join(PKG, "ropesim", "libropesim_b200.so"))
+    tf = ctypes.c_double(0)
+    lib.rs_probe_fp32_peak(ctypes.byref(tf), None)
+    return tf.value
+
+
+def timed_frames(fn, frames, stream, flush, kernel_ms=None, b=None):
+    """CUDA-event time of each call of fn(f) on `stream`, L2 flushed before each (outside the events)."""
+    import torch
+
+    ms = []
+    for f in frames:
+        flush.fill_(float(f))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(f)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        if kernel_ms is not None:
+            kernel_ms.append(b.last_frame_ms())
+    return ms
+
+
+# ------------------------------------------------------------------ CPU legs (the oracle port)
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ropesim_oracle
+
+    return ropesim_oracle
+
+
+def _threads_run(sims, work):
+    ts = [threading.Thread(target=work, args=s) for s in sims]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+
+
+def c3_cpu_sims(scene, ropes, threads, precision="f32"):
+    ro = _oracle()
+    chunks = [c for c in np.array_split(np.asarray(ropes), threads) if len(c)]
+    return [(Sc.bench_c3_build(ro, scene, sel=c, precision=precision), c) for c in chunks]
+
+
+def c3_cpu_frame(sims, inputs, f):
+    PP, QQ, p0, v0, p1 = inputs
+
+    def work(o, c):
+        o.set_mesh_poses_all(PP[f][c], QQ[f][c], teleport=(f == 0))
+        o.step(p0[f][c], v0[f][c], DT, S, root_pos_end=p1[f][c])
+
+    _threads_run(sims, work)
+
+
+def cpu_leg_c3(scene, inputs, seconds_target=15.0, threads=None):
+    """The FP32 CPU restatement on all host cores: a bounded sample of the config-3 ropes
+    (ropes split over threads), frames 0..2 of the same inputs."""
+    threads = threads or os.cpu_count() or 1
+    verts = scene[1]
+    probe = np.arange(threads)
+    sims = c3_cpu_sims(scene, probe, threads)
+    t0 = time.perf_counter()
+    c3_cpu_frame(sims, inputs, 0)
+    per = (time.perf_counter() - t0) / max(1, int(verts[probe].sum()))  # s per vertex-frame (all threads)
+    n = int(np.clip(seconds_target / 2 / max(per, 1e-12) / np.mean(verts), threads, len(verts)))
+    sel = np.arange(n)
+    sims = c3_cpu_sims(scene, sel, threads)
+    frames = 2
+    t0 = time.perf_counter()
+    for f in range(frames):
+        c3_cpu_frame(sims, inputs, f)
+    t = time.perf_counter() - t0
+    nv = int(verts[sel].sum())
+    return {"value": nv * S * frames / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the first {n} of the {len(verts)} config-3 ropes ({nv} vertices) x {frames} frames x {S} substeps "
+                      f"(FP32 CPU restatement, {threads} threads, {t:.1f} s)"}
+
+
+def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's algorithm (its CUDA build needs
+    GLM, absent on this image) on all host cores, each step one frame of a bounded sample of the
+    same scene. Rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from ropesim import sdf
+
+    threads = os.cpu_count() or 1
+    frames = args.warmup + args.steps
+    if args.workload == "config2":
+        n_ropes = max(threads, int(os.environ.get("RS_REF_ROPES", str(8 * threads))))
+        pos, p0, v0, p1 = Sc.bench_c2_inputs(n_ropes, frames, 11)
+        ro = _oracle()
+        sims = []
+        for c in [c for c in np.array_split(np.arange(n_ropes), threads) if len(c)]:
+            b = ro.RopeBatch.from_positions(pos[c], 0.117, 11473.0, 4.48e-3, H, ITERS, precision="f32")
+            Sc.bench_c2_configure(b)
+            sims.append((b, c))
+
+        def frame(f):
+            _threads_run(sims, lambda b, c: b.step(p0[f][c], v0[f][c], DT, S, root_pos_end=p1[f][c]))
+
+        nv, workload = n_ropes * V, "config2-program-4096x64"
+        sample = f"{n_ropes} of the 4096 config-2 ropes per step (64 verts)"
+    else:
+        scene = Sc.bench_c3_scene(sdf, C3_ROPES)
+        inputs = Sc.bench_c3_inputs(scene, frames)
+        n_ropes = max(threads, int(os.environ.get("RS_REF_ROPES", str(32 * threads))))
+        sims = c3_cpu_sims(scene, np.arange(n_ropes), threads)
+        nv, workload = int(scene[1][:n_ropes].sum()), f"config3-uneven-{C3_ROPES}"
+        sample = f"the first {n_ropes} of the {C3_ROPES} config-3 ropes per step ({nv} vertices)"
+
+        def frame(f):
+            c3_cpu_frame(sims, inputs, f)
+
+    for f in range(args.warmup):
+        frame(f)
+    t0 = time.perf_counter()
+    for f in range(args.warmup, frames):
+        frame(f)
+    el = time.perf_counter() - t0
+    value = nv * S * args.steps / el
+    sample += f", {S} substeps, {ITERS} itr; FP32 CPU restatement of the reference's algorithm on {threads} threads"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload + " (bounded CPU sample)", "ropes_per_step": n_ropes, "verts_per_step": nv,
+                       "substeps": S, "num_itr": ITERS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference CUDA build unavailable (GLM headers absent); the reference arm is the oracle port"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ config 3 (the target)
+def c3_legs(args, world, rank, local, dev, dist, extras):
+    """Config 3 on this rank's shard: the persistent device-timed leg, the end-to-end leg and (with
+    `extras`, one rank) the plain paths and the CPU baseline. Returns the line's fields."""
+    import torch
+
+    import ropesim
+    from ropesim import sdf
+
+    R = args.ropes or C3_ROPES
+    scene = Sc.bench_c3_scene(sdf, R, seed=3 + 7919 * rank)
+    verts = scene[1]
+    nv = int(np.sum(verts))
+    W, K = args.warmup, args.steps
+    F = 2 * (W + K)
+    inputs = Sc.bench_c3_inputs(scene, F, seed=17 + rank)
+    PP, QQ, p0, v0, p1 = inputs
+    Td = [tuple(torch.as_tensor(x[f], device=dev) for x in inputs) for f in range(W + K)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    b = Sc.bench_c3_build(ropesim, scene)
+    b.set_timing(True)
+    st = torch.cuda.ExternalStream(b.stream_ptr())
+
+    def frame(bb, f, T):
+        bb.set_mesh_poses_all(T[0], T[1], teleport=(f == 0))
+        bb.step(T[2], T[3], DT, S, root_pos_end=T[4])
+
+    for f in range(W):
+        frame(b, f, Td[f])
+    torch.cuda.synchronize()
+    barrier(dist)
+    kernel_ms = []
+    sampler = ClockSampler(local)
+    with sampler:
+        ms = timed_frames(lambda f: frame(b, f, Td[f]), range(W, W + K), st, flush, kernel_ms, b)
+    torch.cuda.synchronize()
+    total_ms = max_over_ranks(sum(ms), dist, dev)
+    barrier(dist)
+    value = job_rate(world, nv * S * K, total_ms * 1e-3)
+    pos_ok = bool(torch.isfinite(torch.as_tensor(b.positions())).all())
+
+    # ---- end to end: pinned host poses and programs in, positions out, through the public API
+    e2e_value = None
+    if not args.no_e2e:
+        hs = [torch.as_tensor(x[W + K:]).pin_memory() for x in inputs]
+        out = torch.empty((nv, 3), dtype=torch.float32).pin_memory()
+        view = torch.as_tensor(b.positions()).reshape(nv, 3)
+
+        def e2e_frame(i):
+            T = tuple(h[i].to(dev, non_blocking=True) for h in hs)
+            frame(b, W + K + i, T)
+            out.copy_(view)
+
+        for i in range(W):
+            e2e_frame(i)
+        torch.cuda.synchronize()
+        barrier(dist)
+        t0 = time.perf_counter()
+        for i in range(W, W + K):
+            e2e_frame(i)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+        e2e_value = job_rate(world, nv * S * K, e2e_s)
+    h2d = R * M3 * 7 * 4 + R * 9 * 4
+    d2h = nv * 3 * 4
+    layout = list(b.layout())
+    del b, Td
+    torch.cuda.empty_cache()
+
+    res = {"value": value, "ms_per_step": total_ms / K, "kernel_ms_per_frame": float(np.mean(kernel_ms)),
+           "R": R, "nv": nv, "layout": layout, "finite": pos_ok, "clocks": sampler.summary(),
+           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "inputs": "per step: mesh poses [R, 8, 7] + root program [R, 9] float32 from pinned host memory; "
+                             "out: positions view [n, 3] to pinned host memory"}}
+    if not extras:
+        return res
+
+    # ---- the plain per-substep-launch engine on the same inputs (one packed batch)
+    nplain_w, nplain = min(W, 3), min(K, 3)
+    pb = Sc.bench_c3_build(ropesim, scene)
+    pb.set_engine("plain")
+    pst = torch.cuda.ExternalStream(pb.stream_ptr())
+    Tp = [tuple(torch.as_tensor(x[f], device=dev) for x in inputs) for f in range(nplain_w + nplain)]
+    for f in range(nplain_w):
+        frame(pb, f, Tp[f])
+    pms = timed_frames(lambda f: frame(pb, f, Tp[f]), range(nplain_w, nplain_w + nplain), pst, flush)
+    pvalue = nv * S * nplain / (sum(pms) * 1e-3)
+    res["plain_path"] = {"value": pvalue, "unit": UNIT, "ms_per_step": float(np.mean(pms)), "steps": nplain,
+                         "launches_per_step": S * (3 + 2 * ITERS) + 3,
+                         "note": "per-substep-launch plain engine over one packed batch of the same ropes (the "
+                                 "reference's launch structure, in-repo; the reference's own CUDA build is unavailable)"}
+    res["speedup_vs_plain"] = res["value"] / world / pvalue
+    del pb, Tp
+    torch.cuda.empty_cache()
+    if not args.no_per_length:
+        res["plain_per_length"] = plain_per_length(ropesim, scene, inputs, dev, flush)
+        res["speedup_vs_plain_per_length"] = res["value"] / world / res["plain_per_length"]["value"]
+    if not args.no_cpu and world == 1:
+        res["cpu_baseline"] = cpu_leg_c3(scene, inputs)
+    return res
+
+
+def plain_per_length(ropesim, scene, inputs, dev, flush, nwarm=2, nsteps=2):
+    """The plain path as the reference's API can run uneven ropes: RopeBatch holds ropes of one
+    length, so the scene becomes one plain-engine batch per distinct vertex count (each with its
+    own copy of the lattices), stepped in sequence on one stream every frame. Same ropes,
+    stiffnesses, masses, planes, mesh poses and root programs as the packed batch; a frame is
+    timed with CUDA events on the legacy default stream, which every batch's blocking stream is
+    ordered with."""
+    import torch
+
+    verts = scene[1]
+    PP, QQ, p0, v0, p1 = inputs
+    batches = []
+    for Vr in np.unique(verts):
+        idx = np.nonzero(verts == Vr)[0]
+        b = Sc.bench_c3_build(ropesim, scene, sel=idx)
+        b.set_engine("plain")
+        batches.append((b, idx))
+    nv = int(np.sum(verts))
+    ms = []
+    for f in range(nwarm + nsteps):
+        sub = [(b, *(torch.as_tensor(np.ascontiguousarray(x[f][i]), device=dev) for x in (PP, QQ, p0, v0, p1)))
+               for b, i in batches]
+        if f >= nwarm:
+            flush.fill_(float(f))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        for b, pp, pq, a0, a1, a2 in sub:
+            b.set_mesh_poses_all(pp, pq, teleport=(f == 0))
+            b.step(a0, a1, DT, S, root_pos_end=a2)
+        if f >= nwarm:
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    finite = all(bool(torch.isfinite(torch.as_tensor(b.positions())).all()) for b, _ in batches)
+    res = {"value": nv * S * len(ms) / (sum(ms) * 1e-3), "unit": UNIT, "ms_per_step": float(np.mean(ms)),
+           "batches": len(batches), "steps": nsteps, "finite": finite,
+           "note": "one plain-engine RopeBatch per distinct vertex count (the reference's RopeBatch takes ropes of "
+                   "one length), stepped in sequence"}
+    del batches
+    torch.cuda.empty_cache()
+    return res
+
+
+# ------------------------------------------------------------------ config 2
+def c2_legs(args, world, rank, local, dev, dist, steps, warmup, e2e=True, plain=True, sampler=None):
+    """Config 2 (4096 x 64 ropes per rank, plane z = 0, program roots): device-timed frames, the
+    end-to-end frames and the plain engine on the same inputs."""
+    import torch
 
     import ropesim
 
-    lib = ctypes.CDLL(os.path.join(PKG, "ropesim", "libropesim_b200.so"))
-    frames = args.warmup + args.steps
-    # frames [0, W+K) drive the device-timed leg; the end-to-end leg continues the same root
-    # programs over frames [W+K, 2(W+K)) (its own W warm-up frames, then K timed)
-    pos, p0, v0, p1 = c2_inputs(N_ROPES, 2 * frames, 1234 + rank)
+    N = C2_ROPES
+    frames = warmup + steps
+    pos, p0, v0, p1 = Sc.bench_c2_inputs(N, 2 * frames, 1234 + rank)
     b = ropesim.RopeBatch.from_positions(pos, 0.117, 11473.0, 4.48e-3, H, ITERS, deterministic=True)
-    configure(b)
+    Sc.bench_c2_configure(b)
     if args.block:
         b.set_block(args.block)
     b.set_timing(True)
-    dev = torch.device("cuda", local)
-    P0 = torch.as_tensor(p0, device=dev)
-    V0 = torch.as_tensor(v0, device=dev)
-    P1 = torch.as_tensor(p1, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    P0, V0, P1 = (torch.as_tensor(x, device=dev) for x in (p0, v0, p1))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     torch.cuda.synchronize()
-
-    # ---- device-timed leg: one persistent launch per frame
-    for f in range(args.warmup):
+    for f in range(warmup):
         b.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    kernel_ms = []
-    frame_ms = []
+    barrier(dist)
     stream = torch.cuda.ExternalStream(b.stream_ptr())
-    sampler = ClockSampler(local)
-    with sampler:
-        for f in range(args.warmup, frames):
-            flush.fill_(float(f))
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            b.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
-            e1.record(stream)
-            e1.synchronize()
-            frame_ms.append(e0.elapsed_time(e1))
-            kernel_ms.append(b.last_frame_ms())
-    torch.cuda.synchronize()
-    total_ms = float(sum(frame_ms))
-    if world > 1:
-        total_ms = max_over_ranks(total_ms, dist, dev)
-        dist.barrier()
-    vs_per_rank = N_ROPES * V * S * args.steps
-    value = job_rate(world, vs_per_rank, total_ms * 1e-3)
+    kernel_ms = []
 
-    # ---- end-to-end leg: host inputs in, host positions out, through the public API
-    if args.no_e2e:
-        frames = args.warmup  # no timed e2e frames
-    hp0 = torch.as_tensor(p0).pin_memory()
-    hv0 = torch.as_tensor(v0).pin_memory()
-    hp1 = torch.as_tensor(p1).pin_memory()
-    out = torch.empty((N_ROPES, V, 3), dtype=torch.float32).pin_memory()
-    view = torch.as_tensor(b.positions())
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    def step(f):
+        b.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
 
-    def e2e_frame(f):
-        a0 = hp0[f].to(dev, non_blocking=True)
-        a1 = hv0[f].to(dev, non_blocking=True)
-        a2 = hp1[f].to(dev, non_blocking=True)
-        b.step(a0, a1, DT, S, root_pos_end=a2)
-        out.copy_(view)
-
-    e2e_first = args.warmup + args.steps
-    for f in range(e2e_first, e2e_first + args.warmup):
-        e2e_frame(f)
+    if sampler is not None:
+        with sampler:
+            ms = timed_frames(step, range(warmup, frames), stream, flush, kernel_ms, b)
+    else:
+        ms = timed_frames(step, range(warmup, frames), stream, flush, kernel_ms, b)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for f in range(e2e_first + args.warmup, e2e_first + frames):
-        e2e_frame(f)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        e2e_s = max_over_ranks(e2e_s, dist, dev)
-    e2e_value = job_rate(world, vs_per_rank, e2e_s) if not args.no_e2e else None
-    h2d = 3 * N_ROPES * 3 * 4
-    d2h = N_ROPES * V * 3 * 4
+    total_ms = max_over_ranks(sum(ms), dist, dev)
+    barrier(dist)
+    vs = N * V * S * steps
+    res = {"value": job_rate(world, vs, total_ms * 1e-3), "unit": UNIT, "ms_per_step": total_ms / steps,
+           "kernel_ms_per_frame": float(np.mean(kernel_ms)), "steps": steps, "bins": list(b.layout())}
+    if e2e:
+        hp0, hv0, hp1 = (torch.as_tensor(x).pin_memory() for x in (p0, v0, p1))
+        out = torch.empty((N, V, 3), dtype=torch.float32).pin_memory()
+        view = torch.as_tensor(b.positions())
 
-    # ---- plain path: the same frames through the per-substep-launch engine (the reference's
-    # launch structure, in-repo), same inputs and device timing
-    plain = None
-    if not args.no_plain:
+        def e2e_frame(f):
+            a0 = hp0[f].to(dev, non_blocking=True)
+            a1 = hv0[f].to(dev, non_blocking=True)
+            a2 = hp1[f].to(dev, non_blocking=True)
+            b.step(a0, a1, DT, S, root_pos_end=a2)
+            out.copy_(view)
+
+        for f in range(frames, frames + warmup):
+            e2e_frame(f)
+        torch.cuda.synchronize()
+        barrier(dist)
+        t0 = time.perf_counter()
+        for f in range(frames + warmup, 2 * frames):
+            e2e_frame(f)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+        res["e2e"] = {"value": job_rate(world, vs, e2e_s), "unit": UNIT, "h2d_bytes_per_step": 3 * N * 3 * 4,
+                      "d2h_bytes_per_step": N * V * 3 * 4}
+    del b
+    if plain:
         pb = ropesim.RopeBatch.from_positions(pos, 0.117, 11473.0, 4.48e-3, H, ITERS, deterministic=True)
-        configure(pb)
+        Sc.bench_c2_configure(pb)
         pb.set_engine("plain")
         pstream = torch.cuda.ExternalStream(pb.stream_ptr())
-        for f in range(args.warmup):
+        for f in range(min(warmup, 3)):
             pb.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
-        torch.cuda.synchronize()
-        pms = []
-        nplain = min(args.steps, 3)
-        for f in range(args.warmup, args.warmup + nplain):
-            flush.fill_(float(f))
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(pstream)
-            pb.step(P0[f], V0[f], DT, S, root_pos_end=P1[f])
-            e1.record(pstream)
-            e1.synchronize()
-            pms.append(e0.elapsed_time(e1))
-        pvalue = N_ROPES * V * S * nplain / (sum(pms) * 1e-3)
-        plain = {"value": pvalue, "unit": METRIC, "ms_per_step": sum(pms) / nplain, "steps": nplain,
-                 "launches_per_step": S * (3 + 2 * ITERS) + 1, "speedup_of_persistent": value / world / pvalue,
-                 "note": "per-substep-launch plain path (reference launch structure, in-repo; the reference's own "
-                         "CUDA build is unavailable)"}
+        nplain = min(steps, 3)
+        pms = timed_frames(lambda f: pb.step(P0[f], V0[f], DT, S, root_pos_end=P1[f]), range(warmup, warmup + nplain),
+                           pstream, flush)
+        pvalue = N * V * S * nplain / (sum(pms) * 1e-3)
+        res["plain_path"] = {"value": pvalue, "unit": UNIT, "ms_per_step": sum(pms) / nplain, "steps": nplain,
+                             "launches_per_step": S * (3 + 2 * ITERS) + 1}
+        res["speedup_vs_plain"] = res["value"] / world / pvalue
         del pb
+    torch.cuda.empty_cache()
+    return res
 
+
+def c2_roofline(c2, fp32_peak):
+    flops_vs = read_profile_value("flop_count_config2.txt", "flops_per_vertex_substep")
+    achieved = flops_vs * C2_ROPES * V * S / (c2["kernel_ms_per_frame"] * 1e-3) / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+            "flops_per_vertex_substep": flops_vs}
+
+
+def run_config2(args):
+    """The config-2 line on its own (4096 x 64 ropes per GPU), as in the earlier headline."""
+    world, rank, local, dev, dist = dist_setup()
+    sampler = ClockSampler(local)
+    c2 = c2_legs(args, world, rank, local, dev, dist, args.steps, args.warmup, e2e=not args.no_e2e,
+                 plain=not args.no_plain, sampler=sampler)
     if rank == 0:
         peaks, source = measured_peaks()
-        tf = ctypes.c_double(0)
-        lib.rs_probe_fp32_peak(ctypes.byref(tf), None)
-        fp32_peak = tf.value
-        flops_vs = read_flops()
-        avg_kernel_ms = float(np.mean(kernel_ms))
-        flops_launch = flops_vs * N_ROPES * V * S
-        achieved = flops_launch / (avg_kernel_ms * 1e-3) / 1e12
-        state_bytes = N_ROPES * V * (6 * 16 + 4 * 16 + 40)  # state in (6 float4), out (4 float4), views
-        line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 ropes and root programs)",
-            "config": {"workload": "config2-program-4096x64", "ropes_per_gpu": N_ROPES, "verts_per_rope": V,
-                       "substeps": S, "num_itr": ITERS, "h": H, "planes": 1, "l2": "flushed between frames (256 MB write)",
-                       "bins": list(b.layout()), "parallelism": f"replicas x{world} (ropes independent)"},
-            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps,
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak, "traffic": read_traffic(),
-                         "peak_source": "measured FP32 FMA probe (rs_probe_fp32_peak) on this GPU",
-                         "flops_per_vertex_substep": flops_vs,
-                         "hbm_view": {"algorithmic_bytes_per_launch": state_bytes,
-                                      "achieved_gbs": state_bytes / (avg_kernel_ms * 1e-3) / 1e9,
-                                      "peak_gbs": peaks.get("hbm_gbs"), "peak_source": source}},
-            "kernel_ms_per_frame": avg_kernel_ms,
-            "plain_path": plain,
-            "clocks": sampler.summary(),
-        }
-        if world == 1 and not args.no_cpu:
-            line["cpu_baseline"] = cpu_leg()
+        fp32 = fp32_peak_tflops()
+        roof = c2_roofline(c2, fp32)
+        state_bytes = C2_ROPES * V * (6 * 16 + 4 * 16 + 40)
+        roof.update({"traffic": read_profile_value("frame_kernel_config2.txt", "dram_bytes_per_launch"),
+                     "peak_source": "measured FP32 FMA probe (rs_probe_fp32_peak) on this GPU",
+                     "hbm_view": {"algorithmic_bytes_per_launch": state_bytes,
+                                  "achieved_gbs": state_bytes / (c2["kernel_ms_per_frame"] * 1e-3) / 1e9,
+                                  "peak_gbs": peaks.get("hbm_gbs"), "peak_source": source}})
+        line = {"metric": METRIC, "value": c2["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": c2["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 ropes and root programs)",
+                "config": {"workload": "config2-program-4096x64", "ropes_per_gpu": C2_ROPES, "verts_per_rope": V,
+                           "substeps": S, "num_itr": ITERS, "h": H, "planes": 1,
+                           "l2": "flushed between frames (256 MB write)", "bins": c2["bins"],
+                           "parallelism": f"ropes sharded by rank x{world} (independent)"},
+                "e2e": c2.get("e2e"), "gpu_launches": args.steps, "roofline": roof,
+                "kernel_ms_per_frame": c2["kernel_ms_per_frame"], "plain_path": c2.get("plain_path"),
+                "speedup_vs_plain": c2.get("speedup_vs_plain"), "clocks": sampler.summary()}
         print(json.dumps(line), flush=True)
-    if world > 1:
+    if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def run_config4(args):
+# ------------------------------------------------------------------ config 4 (differentiable)
+def c4_legs(args, rollouts_warm=3, rollouts=3, R=1024):
     """Config 4: differentiable rollouts of 1024 ropes x 64 vertices (config-1 rope: 3 cm segments,
     0.1 kg/m, EA 500 N, EI 1e-4 N m^2), 30 control frames x 100 substeps, program roots, loss = mean
     squared tip distance to a seeded target curve. One step = one 30-frame rollout: forward only
@@ -611,14 +625,12 @@ def run_config4(args):
     import ropesim
     import ropesim.grad as rg
 
-    torch.cuda.set_device(0)
-    R = args.ropes if args.ropes != 4096 else 1024
-    V, F, S4 = 64, args.frames or 30, 100
+    Vr, F, S4 = 64, args.frames or 30, 100
     seg, density, ea, ei = 0.03, 0.1, 500.0, 1e-4
     rng = np.random.default_rng(4)
     roots = np.stack([rng.uniform(-0.5, 0.5, R), rng.uniform(-0.5, 0.5, R), rng.uniform(2.5, 3.5, R)], 1).astype(np.float32)
-    pos = np.repeat(roots[:, None], V, 1) - np.array([0, 0, seg], np.float32) * np.arange(V, dtype=np.float32)[None, :, None]
-    pos[:, 1:] += rng.normal(0, 1e-3, (R, V - 1, 3)).astype(np.float32)
+    pos = np.repeat(roots[:, None], Vr, 1) - np.array([0, 0, seg], np.float32) * np.arange(Vr, dtype=np.float32)[None, :, None]
+    pos[:, 1:] += rng.normal(0, 1e-3, (R, Vr - 1, 3)).astype(np.float32)
     prog = []
     cur = roots.copy()
     for f in range(F):
@@ -641,11 +653,11 @@ def run_config4(args):
         return b
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    nv = R * V
+    nv = R * Vr
 
-    def timed(fn, rollouts):
+    def timed(fn, n):
         ms = []
-        for k in range(rollouts):
+        for k in range(n):
             flush.fill_(float(k))
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -657,7 +669,8 @@ def run_config4(args):
         return ms
 
     out = {}
-    for engine in ("persistent", "plain"):
+    tape = False if args.no_tape else ("iterates" if args.iterate_tape else True)
+    for engine in ("persistent",) if args.no_plain else ("persistent", "plain"):
         b = make(engine)
         st0 = rg.state(b)
 
@@ -666,8 +679,8 @@ def run_config4(args):
             for f in range(F):
                 b.step(P[0][f], P[1][f], DT, S4, root_pos_end=P[2][f])
 
-        timed(fwd, args.warmup)
-        ms = timed(fwd, args.steps)
+        timed(fwd, rollouts_warm)
+        ms = timed(fwd, rollouts)
         out[engine] = {"ms_per_rollout": float(np.mean(ms)), "value": nv * S4 * F * len(ms) / (sum(ms) * 1e-3)}
         if engine == "persistent":
             par0 = rg.parameters(b)
@@ -680,35 +693,129 @@ def run_config4(args):
                 cur = st
                 loss = 0.0
                 for f in range(F):
-                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4,
-                                   tape=False if args.no_tape else ("iterates" if args.iterate_tape else True))
-                    loss = loss + ((cur[0].view(R, V, 3)[:, -1] - tgt[f]) ** 2).sum(-1).mean()
+                    cur = rg.frame(b, cur, par, pr[0][f], pr[1][f], pr[2][f], DT, S4, tape=tape)
+                    loss = loss + ((cur[0].view(R, Vr, 3)[:, -1] - tgt[f]) ** 2).sum(-1).mean()
                 loss.backward()
                 grads["tensors"] = [t.grad for t in st + par + pr]  # checked after the timed rollouts
                 grads["loss_t"] = loss.detach()
 
-            timed(fwd_bwd, args.warmup)
-            msb = timed(fwd_bwd, args.steps)
+            timed(fwd_bwd, rollouts_warm)
+            msb = timed(fwd_bwd, rollouts)
             grads["finite"] = bool(all(torch.isfinite(t).all() for t in grads["tensors"]))
-            grads["loss"] = float(grads["loss_t"])
             out["fwd_bwd"] = {"ms_per_rollout": float(np.mean(msb)), "value": nv * S4 * F * len(msb) / (sum(msb) * 1e-3),
-                              "grads_finite": grads["finite"], "loss": grads["loss"]}
+                              "grads_finite": grads["finite"], "loss": float(grads["loss_t"])}
+            del grads
         del b
-    line = {"metric": "vertex-substeps/s (fwd+bwd)", "value": out["fwd_bwd"]["value"], "unit": "vertex-substeps/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["fwd_bwd"]["ms_per_rollout"],
+    torch.cuda.empty_cache()
+    res = {"workload": f"config4-diff-{R}x{Vr}", "frames": F, "substeps": S4, "rollouts": rollouts,
+           "backward": "replays each frame" if args.no_tape else (
+               "from the forward's substep and iterate tapes" if args.iterate_tape else "from the forward's substep tapes"),
+           "forward": out["persistent"], "fwd_bwd": out["fwd_bwd"],
+           "fwd_bwd_over_fwd": out["fwd_bwd"]["ms_per_rollout"] / out["persistent"]["ms_per_rollout"]}
+    if "plain" in out:
+        res["plain_path_forward"] = out["plain"]
+        res["fwd_speedup_vs_plain"] = out["persistent"]["value"] / out["plain"]["value"]
+        res["fwd_bwd_speedup_vs_plain_fwd"] = out["fwd_bwd"]["value"] / out["plain"]["value"]
+    return res
+
+
+def run_config4(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    c4 = c4_legs(args, rollouts_warm=args.warmup, rollouts=args.steps, R=args.ropes or 1024)
+    line = {"metric": METRIC + " (config-4 fwd+bwd)", "value": c4["fwd_bwd"]["value"], "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": c4["fwd_bwd"]["ms_per_rollout"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded config-4 rollouts)",
-            "config": {"workload": f"config4-diff-{R}x{V}", "ropes": R, "verts_per_rope": V, "frames": F,
-                       "substeps": S4, "num_itr": ITERS, "step": f"one {F}-frame rollout",
-                       "backward": "replays each frame" if args.no_tape else (
-                           "from the forward's substep and iterate tapes" if args.iterate_tape
-                           else "from the forward's substep tapes"),
+            "config": {"workload": c4["workload"], "frames": c4["frames"], "substeps": c4["substeps"], "num_itr": ITERS,
+                       "step": f"one {c4['frames']}-frame rollout", "backward": c4["backward"],
                        "counted": "forward vertex-substeps of the rollout", "l2": "flushed between rollouts (256 MB write)"},
-            "forward": out["persistent"], "fwd_bwd": out["fwd_bwd"], "plain_path_forward": out["plain"],
-            "fwd_bwd_over_fwd": out["fwd_bwd"]["ms_per_rollout"] / out["persistent"]["ms_per_rollout"],
-            "fwd_bwd_speedup_vs_plain_fwd": out["fwd_bwd"]["value"] / out["plain"]["value"],
-            "fwd_speedup_vs_plain": out["persistent"]["value"] / out["plain"]["value"]}
+            **{k: v for k, v in c4.items() if k not in ("workload", "frames", "substeps", "backward")}}
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ the default line
+def run_target(args):
+    """The default line: config 3 (the target configuration) with the plain paths beside it, and
+    config 2 and config 4 measured in the same run (one rank; with N > 1 ranks each rank runs its
+    own shard of config 3 and the extras are skipped)."""
+    import torch
+
+    world, rank, local, dev, dist = dist_setup()
+    extras = world == 1
+    c3 = c3_legs(args, world, rank, local, dev, dist, extras)
+    c2 = c4 = None
+    if extras and not args.no_extras:
+        c2 = c2_legs(args, world, rank, local, dev, dist, steps=min(args.steps, 10), warmup=args.warmup)
+        c4 = c4_legs(args)
+    if rank == 0:
+        peaks, source = measured_peaks()
+        fp32 = fp32_peak_tflops()
+        flops_vs = read_profile_value("flop_count_config3.txt", "flops_per_vertex_substep")
+        kms = c3["kernel_ms_per_frame"]
+        roof = {"bound": "fp32", "unit": "TFLOP/s", "peak": fp32,
+                "peak_source": "measured FP32 FMA probe (rs_probe_fp32_peak) on this GPU; MEASURED_PEAKS.json carries "
+                               "no FP32 figure",
+                "kernel": "frame_kernel<256, SURF_MESHES> (one launch per frame)", "kernel_ms_per_frame": kms}
+        if flops_vs:
+            achieved = flops_vs * c3["nv"] * S / (kms * 1e-3) / 1e12
+            roof.update({"achieved": achieved, "frac": achieved / fp32, "flops_per_vertex_substep": flops_vs})
+        t = read_profile_value("frame_kernel_config3.txt", "dram_bytes_per_launch")
+        roof["traffic"] = t
+        state_bytes = c3["nv"] * (6 * 16 + 4 * 16 + 40)
+        roof["hbm_view"] = {"algorithmic_bytes_per_launch": state_bytes,
+                            "achieved_gbs": state_bytes / (kms * 1e-3) / 1e9, "peak_gbs": peaks.get("hbm_gbs"),
+                            "peak_source": source}
+        line = {"metric": METRIC, "value": c3["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": c3["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded config-3 scene: uneven ropes, per-rope EA/EI, per-vertex masses, two planes, "
+                        "eight 64^3 lattices with per-env random-walk poses, root programs)",
+                "config": {"workload": f"config3-uneven-{c3['R']}", "ropes_per_gpu": c3["R"], "verts_per_gpu": c3["nv"],
+                           "verts_per_rope": "U{16..256}", "substeps": S, "num_itr": ITERS, "h": H, "planes": 2,
+                           "meshes": M3, "lattice": "64^3 float32", "l2": "flushed between frames (256 MB write)",
+                           "bins": c3["layout"], "parallelism": f"ropes sharded by rank x{world} (independent)"},
+                "e2e": c3["e2e"], "gpu_launches": 4 * args.steps,
+                "gpu_launches_note": "per frame: scatter_targets, stage_motion, frame_kernel, commit",
+                "roofline": roof, "kernel_ms_per_frame": kms, "finite": c3["finite"], "clocks": c3["clocks"]}
+        for k in ("speedup_vs_plain", "plain_path", "speedup_vs_plain_per_length", "plain_per_length", "cpu_baseline"):
+            if k in c3:
+                line[k] = c3[k]
+        if c4 is not None:
+            line["fwd_bwd_over_fwd"] = c4["fwd_bwd_over_fwd"]
+            line["config4"] = c4
+        if c2 is not None:
+            c2["roofline"] = c2_roofline(c2, fp32)
+            line["config2"] = c2
+        par = read_parity()
+        if par is not None:
+            line["parity"] = par
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ config 3 alone (profiling)
+def run_config3(args):
+    """Config 3 forward alone, persistent vs the packed plain path (no extras): the profiling entry."""
+    world, rank, local, dev, dist = dist_setup()
+    args.no_e2e = True
+    c3 = c3_legs(args, world, rank, local, dev, dist, extras=not args.no_plain)
+    if rank == 0:
+        line = {"metric": METRIC, "value": c3["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": c3["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-3 scene)",
+                "config": {"workload": f"config3-uneven-{c3['R']}", "verts": c3["nv"], "bins": c3["layout"]},
+                "kernel_ms_per_frame": c3["kernel_ms_per_frame"], "clocks": c3["clocks"]}
+        for k in ("speedup_vs_plain", "plain_path", "speedup_vs_plain_per_length", "plain_per_length"):
+            if k in c3:
+                line[k] = c3[k]
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def config5_scene(R=256, V=128, seed=5):
@@ -773,7 +880,7 @@ def run_config5(args):
     import ropesim.grad as rg
 
     torch.cuda.set_device(0)
-    R = args.ropes if args.ropes != 4096 else 256
+    R = args.ropes or 256
     V, F, S5 = 128, args.frames or 60, 100
     iters = args.iters or ITERS
     pos, ea_true, ei_true, lattice = config5_scene(R, V)
@@ -894,11 +1001,12 @@ def run_exchange(args):
     import torch
 
     import ropesim
-    import scenarios as Sc
 
     torch.cuda.set_device(0)
-    R = args.ropes if args.ropes != 4096 else 8192
-    scene = config3_scene(R)
+    R = args.ropes or C3_ROPES
+    from ropesim import sdf
+
+    scene = Sc.bench_c3_scene(sdf, R)
     ropes, verts = scene[0], scene[1]
     nv = int(np.sum(verts))
     M = 8
@@ -914,7 +1022,7 @@ def run_exchange(args):
     roots = np.stack([r[0] for r in ropes]).astype(np.float32)
 
     def leg(K, forces):
-        b = build_config3(ropesim, scene, "persistent")
+        b = Sc.bench_c3_build(ropesim, scene)
         b.enable_contact_forces(forces)
         st = torch.cuda.ExternalStream(b.stream_ptr())
         wview = torch.as_tensor(b.mesh_wrenches_view()) if forces else None
@@ -1079,17 +1187,22 @@ def run_bake(args):
 
 
 def main():
-    global N_ROPES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="target",
+                    choices=["target", "config2", "config3", "config4", "config5", "bake", "exchange"],
+                    help="target (default: config 3 with the plain paths, plus config 2 and config 4 in the same run), "
+                         "config2 / config3 / config4 / config5 alone, exchange (the Isaac-bridge loop), bake (mesh baking)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--ropes", type=int, default=N_ROPES, help="ropes per GPU (profiling of smaller cases)")
+    ap.add_argument("--ropes", type=int, default=0, help="ropes per GPU (0 = the workload's own; profiling of smaller cases)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling)")
-    ap.add_argument("--block", type=int, default=0, help="bin size (CTA threads); 0 = the library's choice")
-    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path leg")
+    ap.add_argument("--block", type=int, default=0, help="config2: bin size (CTA threads); 0 = the library's choice")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path legs")
+    ap.add_argument("--no-per-length", action="store_true", help="skip the one-batch-per-rope-length plain leg")
+    ap.add_argument("--no-extras", action="store_true", help="target: skip the config-2 and config-4 legs")
     ap.add_argument("--frames", type=int, default=0,
                     help="control frames per rollout (0 = the workload's own: 30 for config4, 60 for config5)")
     ap.add_argument("--no-tape", action="store_true", help="config4: backward replays frames instead of keeping tapes")
@@ -1098,16 +1211,14 @@ def main():
     ap.add_argument("--fit-steps", type=int, default=0, help="config5: total fitting steps to run (e.g. 50)")
     ap.add_argument("--iters", type=int, default=0, help="config5: Jacobi sweeps per substep (0 = the default 8)")
     ap.add_argument("--bake-subdiv", type=int, default=5, help="bake: icosphere subdivisions of the baked mesh")
-    ap.add_argument("--workload", default="config2",
-                    choices=["config2", "config3", "config4", "config5", "bake", "exchange"],
-                    help="config2 (the headline line), config3 (uneven ropes, planes and meshes vs the plain path) "
-                         "or config4 (differentiable rollouts: forward and forward + backward)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
-    N_ROPES = args.ropes
+    maybe_relaunch(args)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "config2":
+        run_config2(args)
     elif args.workload == "config3":
         run_config3(args)
     elif args.workload == "config4":
@@ -1120,7 +1231,7 @@ def main():
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         run_bake(args)
     else:
-        run_ours(args)
+        run_target(args)
 
 
 if __name__ == "__main__":

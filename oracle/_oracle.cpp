@@ -34,14 +34,14 @@ template <class T>
 static py::array_t<double> v3_out(const std::vector<rso::V3<T>>& v) {
     py::array_t<double> a({(py::ssize_t)v.size(), (py::ssize_t)3});
     auto m = a.mutable_unchecked<2>();
-    for (size_t i = 0; i < v.size(); i++) { m(i, 0) = v[i].x; m(i, 1) = v[i].y; m(i, 2) = v[i].z; }
+    for (size_t i = 0; i < v.size(); i++) { m(i, 0) = (double)v[i].x; m(i, 1) = (double)v[i].y; m(i, 2) = (double)v[i].z; }
     return a;
 }
 template <class T>
 static py::array_t<double> q4_out(const std::vector<rso::Q4<T>>& v) {
     py::array_t<double> a({(py::ssize_t)v.size(), (py::ssize_t)4});
     auto m = a.mutable_unchecked<2>();
-    for (size_t i = 0; i < v.size(); i++) { m(i, 0) = v[i].x; m(i, 1) = v[i].y; m(i, 2) = v[i].z; m(i, 3) = v[i].w; }
+    for (size_t i = 0; i < v.size(); i++) { m(i, 0) = (double)v[i].x; m(i, 1) = (double)v[i].y; m(i, 2) = (double)v[i].z; m(i, 3) = (double)v[i].w; }
     return a;
 }
 template <class T>
@@ -58,9 +58,10 @@ static const float* opt_ptr(const py::object& o, f32a& keep) {
 }
 
 template <class T>
-static void bind_sim(py::module_& m, const char* name) {
+static py::class_<rso::Sim<T>> bind_sim(py::module_& m, const char* name) {
     using S = rso::Sim<T>;
-    py::class_<S>(m, name)
+    py::class_<S> cls(m, name);
+    cls
         .def(py::init([](f32a positions, i32a starts, u8a pinned, float density, float ks, float kb, float max_h, int num_itr,
                          bool fix_root, bool straight_rest, bool per_rope_env, float dead_r, float dead_b) {
                  return new S(positions.data(), starts.data(), (int)starts.shape(0) - 1, pinned.data(), density, ks, kb, max_h,
@@ -174,6 +175,21 @@ static void bind_sim(py::module_& m, const char* name) {
             py::gil_scoped_release rel;
             s.step_program_rows(p.data(), dt, S_);
         })
+        .def("rope_contact_counts", [](S& s) {  // (active rope-rope terms, limited steps) since the last call
+            const auto r = py::make_tuple(s.nCollisionTerms, s.nLimitedSteps);
+            s.nCollisionTerms = s.nLimitedSteps = 0;
+            return r;
+        })
+        .def("contact_forces", [](S& s) { return v3_out(s.contactForce); })
+        .def("wrenches", [](S& s) { return v3_out(s.wrench); });
+    return cls;
+}
+
+// The adjoint (double and float only).
+template <class T>
+static void bind_adjoint(py::class_<rso::Sim<T>>& cls) {
+    using S = rso::Sim<T>;
+    cls
         // Reverse one frame from the current (frame-start) state; leaves the Sim at the frame end.
         .def("frame_backward", [](S& s, py::object prog, float dt, int S_, f64a gx, f64a gv, f64a glv, f64a gq) {
             std::vector<T> p;
@@ -190,14 +206,7 @@ static void bind_sim(py::module_& m, const char* name) {
             d["P0"] = v3_out(g.P0); d["V0"] = v3_out(g.V0); d["P1"] = v3_out(g.P1);
             d["ks"] = s_out(g.ks); d["rho"] = s_out(g.rho); d["w"] = s_out(g.w);
             return d;
-        })
-        .def("rope_contact_counts", [](S& s) {  // (active rope-rope terms, limited steps) since the last call
-            const auto r = py::make_tuple(s.nCollisionTerms, s.nLimitedSteps);
-            s.nCollisionTerms = s.nLimitedSteps = 0;
-            return r;
-        })
-        .def("contact_forces", [](S& s) { return v3_out(s.contactForce); })
-        .def("wrenches", [](S& s) { return v3_out(s.wrench); });
+        });
 }
 
 // Algorithmic operation count of program-driven frames (rso::Sim<OpCount>): positions
@@ -232,8 +241,20 @@ static py::dict count_program_ops(f32a positions, float density, float ks, float
 
 PYBIND11_MODULE(_oracle, m) {
     m.doc() = "CPU restatement (test oracle) of the Stable Cosserat Rods substep";
-    bind_sim<double>(m, "Sim64");
-    bind_sim<float>(m, "Sim32");
+    auto c64 = bind_sim<double>(m, "Sim64");
+    auto c32 = bind_sim<float>(m, "Sim32");
+    bind_adjoint(c64);
+    bind_adjoint(c32);
+    // The op-counting instantiation: the same restated substep in double precision, every
+    // floating-point operation tallied (rs_opcount.hpp) for the algorithmic FLOP figures.
+    bind_sim<rso::OpCount>(m, "SimOps");
+    m.def("op_tally", []() {
+        const rso::OpTally t = rso::op_tally();
+        py::dict d;
+        d["add"] = t.add; d["mul"] = t.mul; d["div"] = t.div; d["sqrt"] = t.sqrt; d["trans"] = t.trans; d["cmp"] = t.cmp;
+        return d;
+    }, "operation tallies of this thread since the last op_tally_reset()");
+    m.def("op_tally_reset", []() { rso::op_tally().reset(); });
     m.def("hardware_threads", []() { return (int)std::thread::hardware_concurrency(); });
     m.def("count_program_ops", &count_program_ops, py::arg("positions"), py::arg("density"), py::arg("k_stretch"),
           py::arg("k_bend"), py::arg("h"), py::arg("num_itr"), py::arg("p0"), py::arg("v0"), py::arg("p1"), py::arg("dt"),

@@ -32,8 +32,10 @@ def _ext():
 
 
 def _sim_class(precision):
+    """f64: the parity target; f32: the float instantiation; ops: double precision with every
+    floating-point operation tallied (_oracle.op_tally), for algorithmic FLOP counts."""
     m = _ext()
-    return {"f64": m.Sim64, "f32": m.Sim32}[precision]
+    return {"f64": m.Sim64, "f32": m.Sim32, "ops": m.SimOps}[precision]
 
 
 def _f32(a):

@@ -198,6 +198,129 @@ def planes_only(mod, planes, R=6, frames=10, S=50, seed=11, to_dev=None, precisi
     return np.stack(out), np.stack(fo)
 
 
+# ---------------------------------------------------------------- the benchmarked scenes
+# The exact seeded inputs bench.py times, shared with the parity tests that replay samples of
+# them rope by rope through the oracle (ropes are independent, so a rope's trajectory does not
+# depend on which other ropes share the launch).
+
+BENCH_H, BENCH_ITERS, BENCH_S, BENCH_DT = 1.0 / 6000.0, 8, 100, 1.0 / 60.0
+
+
+def bench_c2_inputs(n_ropes, frames, seed, V=64):
+    """Config 2: 64-vertex jittered ropes hanging clear of z = 0 and their root programs
+    (v0 ~ N(0, 0.5) m/s, p1 = p0 + N(0, 0.05) m, next p0 = p1) for `frames` frames."""
+    pos, roots = c2_positions(n_ropes, V, seed)
+    rng = np.random.default_rng(seed + 1000)
+    p0 = np.empty((frames, n_ropes, 3), np.float32)
+    v0 = rng.normal(0, 0.5, (frames, n_ropes, 3)).astype(np.float32)
+    p1 = np.empty_like(p0)
+    cur = roots.copy()
+    for f in range(frames):
+        p0[f] = cur
+        p1[f] = (cur + rng.normal(0, 0.05, (n_ropes, 3))).astype(np.float32)
+        cur = p1[f]
+    return pos, p0, v0, p1
+
+
+def bench_c2_configure(b):
+    """Config 2's solver settings (damping 0 and drag 0.2 set explicitly, plane z = 0)."""
+    b.set_gravity(np.array([0, 0, -G], np.float32))
+    b.damping = 0.0
+    b.drag = 0.2
+    b.set_planes(np.array([[0, 0, 1, 0]], np.float32), radius=0.00635)
+
+
+def bench_c3_scene(sdf_mod, n_ropes, seed=3):
+    """Config 3: n_ropes uneven ropes, V ~ U{16..256} at 2 cm, EA log-U[1e2, 1e4] and
+    EI log-U[1e-5, 1e-2] per rope, per-vertex masses x U[0.8, 1.2]; eight 64^3 float32 lattices
+    (sphere, box, capsule closed forms). Returns (ropes, verts, ea_v, ei_v, m_v, grids)."""
+    rng = np.random.default_rng(seed)
+    verts = rng.integers(16, 257, n_ropes)
+    g = int(np.ceil(np.sqrt(n_ropes)))
+    ropes = []
+    for r in range(n_ropes):
+        L = 0.02 * (verts[r] - 1)
+        root = np.array([(r % g) * 0.7, (r // g) * 0.7, 0.06 + 0.97 * L])
+        tilt = np.deg2rad(rng.uniform(5, 20))
+        az = rng.uniform(0, 2 * np.pi)
+        d = np.array([np.sin(tilt) * np.cos(az), np.sin(tilt) * np.sin(az), -np.cos(tilt)])
+        pts = root + np.outer(np.arange(verts[r]) * 0.02, d)
+        pts[1:] += rng.normal(0, 1e-3, (verts[r] - 1, 3))
+        ropes.append(pts.astype(np.float32))
+    ea = np.exp(rng.uniform(np.log(1e2), np.log(1e4), n_ropes))
+    ei = np.exp(rng.uniform(np.log(1e-5), np.log(1e-2), n_ropes))
+    ea_v = np.concatenate([np.full(v, ea[i]) for i, v in enumerate(verts)]).astype(np.float32)
+    ei_v = np.concatenate([np.full(v, ei[i]) for i, v in enumerate(verts)]).astype(np.float32)
+    m_v = []
+    for rope in ropes:
+        seg = np.linalg.norm(np.diff(rope.astype(np.float64), axis=0), axis=1)
+        m = np.zeros(len(rope))
+        m[:-1] += 0.5 * 0.117 * seg
+        m[1:] += 0.5 * 0.117 * seg
+        m_v.append(m * rng.uniform(0.8, 1.2, len(rope)))
+    m_v = np.concatenate(m_v).astype(np.float32)
+    n64 = (0.4) / 63.0
+    grids = [sdf_mod.from_function(sdf_mod.sdf_sphere(0.12), [-0.2] * 3, [0.2] * 3, n64),
+             sdf_mod.from_function(sdf_mod.sdf_box([0.12, 0.08, 0.06], round=0.01), [-0.2] * 3, [0.2] * 3, n64),
+             sdf_mod.from_function(sdf_mod.sdf_capsule(0.06, 0.12, axis=0), [-0.2] * 3, [0.2] * 3, n64)]
+    grids = [grids[i % 3] for i in range(8)]
+    return ropes, verts, ea_v, ei_v, m_v, grids
+
+
+def bench_c3_build(mod, scene, sel=None, **kw):
+    """A RopeBatch (product or oracle module) of the config-3 scene, or of the ropes `sel` of it
+    (same per-vertex EA, EI and masses): two planes, the eight lattices, damping 0, drag 0.2."""
+    ropes, verts, ea_v, ei_v, m_v, grids = scene
+    if sel is not None:
+        starts = np.concatenate([[0], np.cumsum(verts)])
+        idx = np.concatenate([np.arange(starts[r], starts[r + 1]) for r in sel])
+        ropes = [ropes[r] for r in sel]
+        ea_v, ei_v, m_v = ea_v[idx], ei_v[idx], m_v[idx]
+    b = mod.RopeBatch.from_ropes(ropes, 0.117, 1000.0, 1e-3, BENCH_H, BENCH_ITERS, **kw)
+    b.set_stretch_stiffnesses(ea_v)
+    b.set_bend_stiffnesses(ei_v)
+    b.set_masses(m_v)
+    b.set_gravity(np.array([0, 0, -G], np.float32))
+    b.damping = 0.0
+    b.drag = 0.2
+    b.set_planes(np.array([[0, 0, 1, 0], [0.05, 0.0, 1.0, -0.02]], np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
+    for gd in grids:
+        b.add_mesh(*gd.as_args())
+    return b
+
+
+def bench_c3_inputs(scene, frames, seed=17, M=8):
+    """Per-frame mesh poses (per env: next to its rope along its length, then a random rigid walk)
+    and root programs (v0 ~ N(0, 0.1), p1 = p0 + N(0, 0.01)) of config 3: pos [F, R, M, 3],
+    quat [F, R, M, 4], p0 / v0 / p1 [F, R, 3], all float32. Frame 0's poses teleport."""
+    ropes = scene[0]
+    R = len(ropes)
+    rng = np.random.default_rng(seed)
+    p = np.zeros((R, M, 3), np.float32)
+    for r, rope in enumerate(ropes):
+        L = 0.02 * (len(rope) - 1)
+        for m in range(M):
+            p[r, m] = rope[0] + np.array([0.25 * np.cos(0.8 * m), 0.25 * np.sin(0.8 * m), -(0.15 + 0.1 * m) * L])
+    q = np.zeros((R, M, 4), np.float32)
+    q[..., 3] = 1.0
+    PP = np.empty((frames, R, M, 3), np.float32)
+    QQ = np.empty((frames, R, M, 4), np.float32)
+    for f in range(frames):
+        PP[f], QQ[f] = p, q
+        p, q = walk_poses(rng, p, q, step=0.003, ang=0.02)
+    roots = np.stack([r[0] for r in ropes]).astype(np.float32)
+    p0 = np.empty((frames, R, 3), np.float32)
+    v0 = np.empty_like(p0)
+    p1 = np.empty_like(p0)
+    cur = roots.copy()
+    for f in range(frames):
+        p0[f] = cur
+        v0[f] = rng.normal(0, 0.1, (R, 3)).astype(np.float32)
+        p1[f] = (cur + rng.normal(0, 0.01, (R, 3))).astype(np.float32)
+        cur = p1[f]
+    return PP, QQ, p0, v0, p1
+
+
 def _flat_positions(b):
     p = b.positions()
     try:
