@@ -11,7 +11,6 @@ origin = lo rounded to float32, nodes per axis = max(ceil((hi - lo) / spacing) +
 """
 from __future__ import annotations
 
-import math
 from dataclasses import dataclass
 
 import numpy as np
@@ -199,9 +198,3 @@ def bake_mesh(vertices, triangles, spacing, margin, thickness=0.0, round=0.0, de
     if not np.isfinite(values).all():
         raise ValueError("bake_mesh produced non-finite distances")
     return SdfGrid(values, origin, float(spacing))
-
-
-def _roundtrip_check():  # pragma: no cover - developer aid
-    g = from_function(sdf_sphere(0.1), [-0.2] * 3, [0.2] * 3, 0.01)
-    phi, inside = g.sample(np.zeros((1, 3)))
-    assert inside[0] and math.isclose(phi[0], -0.1, abs_tol=1e-3)
