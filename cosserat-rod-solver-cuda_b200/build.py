@@ -5,6 +5,9 @@
    only, IEEE division / square root (no fast math), static CUDA runtime.
 2. ropesim/_ropesim*.so: the pybind11 module (RopeSim, RopeBatch, CudaView) linked against (1)
    with an $ORIGIN rpath, so the package directory is self-contained.
+3. The checked build: the same sources with -DROPESIM_CHECKED (every kernel index the topology
+   or the data could push out of range is tested; the first failure is recorded, nothing traps)
+   as libropesim_b200_checked.so and ropesim/_ropesim_checked*.so, for the bounds tests.
 
 Usage: python cosserat-rod-solver-cuda_b200/build.py [--force] [-v]
 """
@@ -27,12 +30,12 @@ CPP_SOURCES = ["rs_batch.cpp", "rs_capi.cpp"]
 HEADERS = ["rs_types.h", "rs_device.cuh", "rs_substep.cuh", "rs_adjoint.cuh", "rs_kernels.h", "rs_batch.h"]
 
 
-def lib_path() -> str:
-    return os.path.join(PKG, "libropesim_b200.so")
+def lib_path(checked: bool = False) -> str:
+    return os.path.join(PKG, "libropesim_b200_checked.so" if checked else "libropesim_b200.so")
 
 
-def ext_path() -> str:
-    return os.path.join(PKG, "_ropesim" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+def ext_path(checked: bool = False) -> str:
+    return os.path.join(PKG, ("_ropesim_checked" if checked else "_ropesim") + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
 
 
 def _nvcc() -> str:
@@ -56,12 +59,14 @@ def _run(cmd, verbose):
     subprocess.check_call(cmd)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def _build_one(checked: bool, force: bool, verbose: bool) -> str:
     nvcc = _nvcc()
-    objdir = os.path.join(HERE, "_build")
+    objdir = os.path.join(HERE, "_build_checked" if checked else "_build")
     os.makedirs(objdir, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "ropesim_b200.h")]
     common = ["-std=c++17", "-O3", "-I", CSRC, "-I", INCLUDE, "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off"]
+    if checked:
+        common.append("-DROPESIM_CHECKED")
     objs = []
     for src in CU_SOURCES + CPP_SOURCES:
         s = os.path.join(CSRC, src)
@@ -73,22 +78,34 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if src.endswith(".cu") and not verbose:
                 cmd.remove("-Xptxas"); cmd.remove("-v")
             _run(cmd, verbose)
-    lib = lib_path()
+    lib = lib_path(checked)
     if force or _stale(lib, objs):
         _run([nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", lib + ".tmp"] + objs, verbose)
         os.replace(lib + ".tmp", lib)
 
     import pybind11
 
-    ext = ext_path()
+    ext = ext_path(checked)
     src = os.path.join(CSRC, "rs_pybind.cpp")
     if force or _stale(ext, [src, lib, os.path.join(INCLUDE, "ropesim_b200.h")]):
         cxx = os.environ.get("CXX", "g++")
+        name = "ropesim_b200_checked" if checked else "ropesim_b200"
         cmd = [cxx, "-O2", "-std=c++17", "-shared", "-fPIC", "-fvisibility=hidden",
                "-I", sysconfig.get_paths()["include"], "-I", pybind11.get_include(), "-I", INCLUDE,
-               src, "-o", ext + ".tmp", "-L", PKG, "-lropesim_b200", "-Wl,-rpath,$ORIGIN"]
+               src, "-o", ext + ".tmp", "-L", PKG, "-l" + name, "-Wl,-rpath,$ORIGIN"]
+        if checked:
+            cmd.insert(1, "-DRS_MODULE_NAME=_ropesim_checked")
         _run(cmd, verbose)
         os.replace(ext + ".tmp", ext)
+    return ext
+
+
+def build(force: bool = False, verbose: bool = False, checked: bool = True) -> str:
+    """The engine (libropesim_b200.so + ropesim._ropesim) and, unless checked=False, its checked
+    build (libropesim_b200_checked.so + ropesim._ropesim_checked)."""
+    ext = _build_one(False, force, verbose)
+    if checked:
+        _build_one(True, force, verbose)
     return ext
 
 

@@ -75,8 +75,13 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
 
     const Bin bin = a.bins[blockIdx.x];
     const int t = threadIdx.x;
-    const bool act = t < bin.vcount;
+    bool act = t < bin.vcount;
     const int dv = bin.vstart + t;
+    if constexpr (kChecked)
+        if (act && !(bin.vstart >= 0 && bin.vcount <= BLOCK && dv < a.n)) {
+            check_fail(a.status, CHK_BIN);
+            act = false;
+        }
     uint32_t fl = 0;
     int uidx = 0, env = 0, lrope = 0;
     float im = 0.f, lr = 1.f, ks = 0.f;
@@ -95,6 +100,11 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
         fl = (uint32_t)tp.x; lrope = tp.y; uidx = tp.z; env = tp.w;
         im = a.pos[dv].w; lr = a.vel[dv].w; ks = a.lvel[dv].w;
         QR[t] = a.qrest[dv];
+        if constexpr (kChecked)
+            if (!checked_vertex(a, bin, t, uidx, fl, lrope, env, nsdf)) {
+                act = false;
+                uidx = 0;
+            }
     }
     const bool hasNext = fl & F_NEXT, hasPrev = fl & F_PREV, nextOrient = fl & F_NEXT_ORIENT;
     const bool upd = hasNext && !(fl & F_FIX_ORIENT);
@@ -112,6 +122,11 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
         if (act) {
             const int4 gr = a.grp[dv];
             g0 = gr.x - bin.vstart; g1 = gr.y - bin.vstart; r0 = gr.z - bin.vstart; r1 = gr.w - bin.vstart;
+            if constexpr (kChecked)
+                if (!(0 <= g0 && g0 <= r0 && r0 <= t && t < r1 && r1 <= g1 && g1 <= bin.vcount)) {
+                    check_fail(a.status, CHK_GROUP);
+                    g0 = g1 = r0 = r1 = t;  // no candidates
+                }
         }
     }
     const float h = a.h, invH = 1.f / h;
@@ -149,6 +164,11 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             }
             p = xyz(t0); v = xyz(t1); lvin = xyz(t2); q = t3;
             cand = (uint64_t)(uint32_t)__float_as_int(t0.w) | ((uint64_t)(uint32_t)__float_as_int(t1.w) << 32);
+            if constexpr (kChecked)
+                if (cand & ~all_meshes(nsdf)) {  // the tape's mask names a mesh the pose cache does not hold
+                    check_fail(a.status, CHK_POSE);
+                    cand &= all_meshes(nsdf);
+                }
         }
         const float4* mycache = PC + (size_t)lrope * nsdf * kPoseF4;
         f3 dx, y;
@@ -197,7 +217,7 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 const bool touched =
                     position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
                 if constexpr (ROPE)
-                    collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, dx, p1dx, f, f2, H, H2);
+                    collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, dx, p1dx, f, f2, H, H2, bin.vcount);
                 // without rope contact H2 is dd I (position_terms): one float4 carries the exchange
                 EA[t] = f4(f2, H2.xx);
                 if constexpr (ROPE) {
@@ -242,7 +262,7 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             const f3 ob = vb * (1.f - a.drag * h);
             f3 vbar = ob;
             if (a.drag_quad > 0.f) {
-                const float4 tq = hasNext ? q : LQ[(size_t)I * BLOCK + t - 1];
+                const float4 tq = hasNext ? q : LQ[(size_t)I * BLOCK + ((kChecked && t == 0) ? 0 : t - 1)];
                 const f3 tg = qtangent(tq);
                 const f3 vv = dx * invH;
                 const float tv = dot(tg, vv);
@@ -333,7 +353,9 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             if constexpr (ROPE) {
                 f3 fd = zero3(), f2d = zero3();
                 sym3 HcB = sym_zero();
-                if (hasNext) collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, xyz(Dk[t]), xyz(Dk[t + 1]), fd, f2d, HcA, HcB);
+                if (hasNext)
+                    collision_sectors(a, ncol, dv, X, Dk, damp, p, p1, xyz(Dk[t]), xyz(Dk[t + 1]), fd, f2d, HcA, HcB,
+                                      bin.vcount);
                 HB0[t] = make_float4(HcB.xx, HcB.yy, HcB.zz, HcB.xy);
                 HB1[t] = make_float4(HcB.xz, HcB.yz, 0.f, 0.f);
             }

@@ -546,12 +546,14 @@ FrameArgs Batch::frame_args(int root_mode, bool has_q0, bool has_q1, float dt, i
     a.poses = d_poses_; a.motion = d_motion_;
     for (int m = 0; m < (int)grids_.size(); m++) a.grids[m] = grids_[m];
     a.n = n_;
+    a.num_ropes = R_;
     a.rope_contact = rope_contact_ ? 1 : 0;
     a.rc_radius = rc_radius_; a.rc_barrier = rc_barrier_; a.rc_kcol = rc_kcol_; a.rc_mu = rc_mu_; a.rc_kfric = rc_kfric_;
     a.det_radius = rc_radius_ + 0.5f * rc_barrier_;          // uploadMeta, YarnBall.cu:262-263
     a.sdet_radius = a.det_radius * rc_scaler_;
     a.grp = d_grp_; a.cols = d_cols_; a.ncols = d_ncols_; a.maxstep = d_maxstep_; a.pad = d_pad_;
-    a.sdf_skip = 1;
+    a.sdf_skip = culling_ ? 1 : 0;
+    a.surf_cull = culling_ ? 1 : 0;
     // stage the lattices' block bounds in each CTA's shared memory when they take <= 48 KB and
     // the CTA's shared memory (frame state 144 B per thread, pose cache, bounds) stays <= 200 KB
     const size_t btot = grids_.empty() ? 0 : (size_t)(grids_.back().boff + grids_.back().bcount);
@@ -603,6 +605,14 @@ const RopeGrid* Batch::rope_grid() {
 }
 
 // ------------------------------------------------------------------ plain engine
+int Batch::bounds_violation() {
+    if (!d_status_) return 0;
+    int v = 0;
+    check(cudaStreamSynchronize(stream_), "sync");
+    check(cudaMemcpy(&v, d_status_ + 3, sizeof(int), cudaMemcpyDeviceToHost), "download(status)");
+    return v;
+}
+
 void Batch::set_engine(int e) {
     if (e != 0 && e != 1) throw std::invalid_argument("engine must be 0 (persistent) or 1 (plain)");
     engine_ = e;
@@ -802,7 +812,9 @@ void Batch::step_program_static_scratch(const float* p0, const float* v0, const 
     h_ = dt / (float)substeps;
     FrameArgs a = frame_args(ROOT_PROGRAM, q0 != nullptr, q1 != nullptr, dt, substeps);
     a.cols = cols;
+    if (timing_) check(cudaEventRecord(ev0_, stream_), "event");
     check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
+    if (timing_) check(cudaEventRecord(ev1_, stream_), "event");
     host_dyn_valid_ = false;
     time_ += dt;
     sdf_end(substeps);
@@ -815,6 +827,11 @@ void Batch::step_program_static_scratch(const float* p0, const float* v0, const 
         check(cudaMemsetAsync(d_status_, 0, sizeof(int) * 4, stream_), "reset status");
         if (err) { last_error_ = err; throw solver_error("MAX_COLLISIONS_PER_SEGMENT exceeded"); }
     }
+    if (timing_) {
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, ev0_, ev1_), "elapsed");
+        last_frame_ms_ = ms;
+    }
 }
 
 void Batch::step_legacy(const float* p, const float* v, const float* q, float dt, int substeps, bool host_inputs) {
@@ -822,7 +839,7 @@ void Batch::step_legacy(const float* p, const float* v, const float* q, float dt
     ensure_device();
     stage_rows(p, v, nullptr, q, nullptr, host_inputs);
     sdf_begin();
-    // exactly `substeps` substeps through the biased max_h of batch.cu:444-452 (float ceil)
+    // exactly `substeps` substeps through the biased max_h of batch.cu:306-308 (float ceil)
     const float mh = (dt / (float)substeps) * 1.000001f;
     int steps = (int)std::ceil(dt / mh);
     if (steps < 1) steps = 1;
@@ -896,7 +913,7 @@ void Batch::set_rope_contact(bool on, float radius, float barrier, float k_colli
                              float detection_scaler, int group_ropes) {
     if (on) {
         // uploadMeta enforces this every step (YarnBall.cu:268): check it here so a bad call
-        // leaves the old state (batch.cu:509-512)
+        // leaves the old state (batch.cu:372-375)
         if (2.f * min_seg_ < 2.f * radius + barrier)
             throw std::invalid_argument("rope contact needs 2 * radius + barrier <= 2 * shortest segment");
         if (!(detection_scaler > 1.f)) throw std::invalid_argument("Detection scaler must be greater than 1.");
@@ -978,6 +995,27 @@ void Batch::set_planes(int count, const float* rows) {
     num_planes_ = count;
 }
 
+// 1 / L for the trilinear interpolant of a lattice: within a cell d(phi)/dx is a bilinear blend of
+// the cell's four x-edge differences over the spacing, so |d(phi)/dx| <= Dx (the largest x-edge
+// difference of the lattice over the spacing), likewise y and z, and the interpolant (continuous
+// across cells) is Lipschitz with L = |(Dx, Dy, Dz)|. Accumulated in double, L is rounded up and
+// 1 / L down; a constant field gives a large finite value.
+static float lattice_lipschitz_inv(const float* v, int nx, int ny, int nz, float spacing) {
+    double D[3] = {0.0, 0.0, 0.0};
+    auto at = [&](int i, int j, int k) { return (double)v[((size_t)i * ny + j) * nz + k]; };
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const double c = at(i, j, k);
+                if (i + 1 < nx) D[0] = std::max(D[0], std::fabs(at(i + 1, j, k) - c));
+                if (j + 1 < ny) D[1] = std::max(D[1], std::fabs(at(i, j + 1, k) - c));
+                if (k + 1 < nz) D[2] = std::max(D[2], std::fabs(at(i, j, k + 1) - c));
+            }
+    const double L = std::sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]) / (double)spacing * (1.0 + 1e-6);
+    const double inv = 1.0 / std::max(L, 1e-6);
+    return std::nextafter((float)inv, 0.f);
+}
+
 int Batch::add_mesh(const float* values, int nx, int ny, int nz, const float* origin, float spacing, float mu_s,
                     float mu_k, const float* pos, const float* quat, int rows) {
     if ((int)grids_.size() >= kMaxSdf) throw std::invalid_argument("at most 64 meshes per sim");
@@ -1013,6 +1051,8 @@ int Batch::add_mesh(const float* values, int nx, int ny, int nz, const float* or
     const cudaError_t e3 = cudaMemcpy(db, bmin.data(), sizeof(float) * bmin.size(), cudaMemcpyHostToDevice);
     if (e3 != cudaSuccess) { cudaFree(d); cudaFree(db); check(e3, "upload(sdf block bounds)"); }
     g.bmin = db; g.by = by; g.bz = bz;
+    g.lip_inv = lattice_lipschitz_inv(values, nx, ny, nz, spacing);
+    g.status = d_status_;
     g.bcount = (int)bmin.size();
     g.boff = grids_.empty() ? 0 : grids_.back().boff + grids_.back().bcount;
     grids_.push_back(g);

@@ -89,6 +89,7 @@ public:
     void advance(float dt, int substeps);   // RopeSim.advance: substeps 0 = float ceil(dt / max_h)
     float time() const { return time_; }
     int last_error() const { return last_error_; }
+    int bounds_violation();  // the checked build's first failed index check (status word 3)
     int last_warning() const { return last_warning_; }
     int nonfinite() const { return nonfinite_; }
 
@@ -163,7 +164,7 @@ public:
     void contact_forces_host(float* out);   // [n, 3]
     void wrenches_host(float* out);         // [R, M, 6]
 
-    // ---- rope-rope contact (RopeBatch::set_rope_contact, batch.cu:504-522): group_ropes
+    // ---- rope-rope contact (RopeBatch::set_rope_contact, batch.cu:367-385): group_ropes
     // consecutive ropes form one contact group; groups never interact
     void set_rope_contact(bool on, float radius, float barrier, float k_collision, float mu, float k_friction,
                           float detection_scaler, int group_ropes);
@@ -179,6 +180,7 @@ public:
     // candidate bin size each (results are bitwise identical across bin sizes), then the
     // fastest is kept and remembered for this workload signature in this process.
     void set_autotune(bool on) { autotune_ = on; }
+    void set_culling(bool on) { culling_ = on; }  // the persistent kernel's exact early outs
     // Engine: 0 = one persistent launch per frame (default), 1 = the per-substep-launch plain
     // path (root, init, num_itr x (position, frame), end kernels per substep, graph-replayed).
     void set_engine(int e);
@@ -247,6 +249,7 @@ private:
     bool timing_ = false;
     double last_frame_ms_ = 0.0;
     bool autotune_ = true, tuned_ = false;
+    bool culling_ = true;
     int engine_ = 0;
     // rope-rope contact
     bool rope_contact_ = false;

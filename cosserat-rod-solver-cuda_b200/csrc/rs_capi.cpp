@@ -203,6 +203,13 @@ int rs_batch_set_autotune(rs_batch* b, int on) {
         s.set_autotune(on != 0);
     });
 }
+int rs_batch_set_culling(rs_batch* b, int on) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_culling(on != 0);
+    });
+}
 int rs_batch_set_engine(rs_batch* b, int engine) {
     return guarded([&] {
         rs::Batch& s = B(b);
@@ -423,6 +430,14 @@ int rs_batch_status(rs_batch* b, int* last_error, int* last_warning, int* nonfin
         if (last_error) *last_error = s.last_error();
         if (last_warning) *last_warning = s.last_warning();
         if (nonfinite) *nonfinite = s.nonfinite();
+    });
+}
+int rs_batch_bounds_check(rs_batch* b, int* code, int* checked) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        if (code) *code = s.bounds_violation();
+        if (checked) *checked = rs::kChecked ? 1 : 0;
     });
 }
 int rs_batch_stream(rs_batch* b, void** stream) {

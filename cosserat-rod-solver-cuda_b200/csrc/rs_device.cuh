@@ -13,6 +13,11 @@
 
 namespace rsd {
 
+// Checked builds: record the first failed check (rs_types.h, CHK_*) in status[3].
+__device__ __forceinline__ void check_fail(int* status, int code) {
+    if (status) atomicCAS(status + 3, 0, code);
+}
+
 struct f3 {
     float x, y, z;
 };
@@ -136,6 +141,10 @@ __device__ __forceinline__ bool sdf_sample(const rs::GridDesc& g, f3 p, float& p
           u.z < float(g.nz - 1)))
         return false;
     const int i = (int)u.x, j = (int)u.y, k = (int)u.z;
+    if (rs::kChecked && !(i >= 0 && j >= 0 && k >= 0 && i <= g.nx - 2 && j <= g.ny - 2 && k <= g.nz - 2)) {
+        check_fail(g.status, rs::CHK_LATTICE);
+        return false;
+    }
     const f3 fr = (p - (o + mk3(float(i), float(j), float(k)) * g.h)) * g.invH;
     const float fx = fminf(fmaxf(fr.x, 0.f), 1.f), fy = fminf(fmaxf(fr.y, 0.f), 1.f), fz = fminf(fmaxf(fr.z, 0.f), 1.f);
     const int sy = g.nz, sx = g.ny * g.nz;
@@ -200,7 +209,31 @@ __device__ __forceinline__ bool sdf_block_clear(const rs::GridDesc& g, const flo
         return true;  // outside the lattice: sdf_sample reports no contact either
     const int bi = (int)u.x / rs::kSdfBlock, bj = (int)u.y / rs::kSdfBlock, bk = (int)u.z / rs::kSdfBlock;
     const int idx = (bi * g.by + bj) * g.bz + bk;
+    if (rs::kChecked && !(bi >= 0 && bj >= 0 && bk >= 0 && bj < g.by && bk < g.bz && idx < g.bcount)) {
+        check_fail(g.status, rs::CHK_BLOCK);
+        return false;  // not cleared: the sample (itself checked) decides
+    }
     return (btab ? btab[g.boff + idx] : __ldg(g.bmin + idx)) - R > 1e-5f;
+}
+
+// How far the probe (pos - P.pos) + d of a vertex can move (|d|) before it could touch lattice g
+// at radius R, from its position at d = 0 (the rotation into the lattice preserves |d|):
+//  - outside the lattice: the distance back into it (no contact outside, sdf_sample);
+//  - inside: (phi(0) - R) / L, since phi(d) >= phi(0) - L |d| (GridDesc::lip_inv).
+// Margins (1e-4 relative, 1e-6 m outside, 1e-5 m on phi) cover the FP32 evaluation of both the
+// probe and phi, so a probe with |d| below the slack has gap >= 0 in sdf_contact_at. A negative
+// slack means "may touch at any |d|".
+__device__ __forceinline__ float sdf_slack(const rs::GridDesc& g, const PoseV& P, f3 pos, float R) {
+    const f3 po = qrot(qconj(P.q), pos - P.pos);
+    const f3 u = (po - mk3(g.ox, g.oy, g.oz)) * g.invH;
+    const f3 ex = mk3(fmaxf(fmaxf(-u.x, u.x - float(g.nx - 1)), 0.f), fmaxf(fmaxf(-u.y, u.y - float(g.ny - 1)), 0.f),
+                      fmaxf(fmaxf(-u.z, u.z - float(g.nz - 1)), 0.f));
+    const float e2 = dot(ex, ex);
+    if (e2 > 0.f) return sqrtf(e2) * g.h * 0.9999f - 1e-6f;
+    float phi;
+    f3 gr;
+    if (!sdf_sample(g, po, phi, gr)) return -1.f;  // on the lattice's upper faces: evaluate every iteration
+    return (phi - R - 1e-5f) * g.lip_inv * 0.9999f;
 }
 
 // Contact of a vertex with one posed lattice at probe (pos - P.pos) + d, contact.cuh:94-110.

@@ -85,8 +85,9 @@ __device__ __forceinline__ void mesh_readout_warp(const FrameArgs& a, const floa
         f3 fm = zero3(), tq = zero3();
         bool hit = false;
         if ((cand >> m) & 1ull) {
-            const float4 lo4 = tbox[2 * m], hi4 = tbox[2 * m + 1];
             const f3 pr = pos + d;
+            const float4 lo4 = tbox ? tbox[2 * m] : make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            const float4 hi4 = tbox ? tbox[2 * m + 1] : make_float4(INFINITY, INFINITY, INFINITY, 0.f);
             if (pr.x >= lo4.x && pr.x <= hi4.x && pr.y >= lo4.y && pr.y <= hi4.y && pr.z >= lo4.z && pr.z <= hi4.z) {
                 const PoseV P = load_pose(cache + m * kPoseF4);
                 f3 n, dRel;
@@ -127,10 +128,21 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
     FrameSmem<BLOCK>& sm = *reinterpret_cast<FrameSmem<BLOCK>*>(dyn_smem);
     float4* pose_smem = dyn_smem + sizeof(FrameSmem<BLOCK>) / sizeof(float4);
 
+    // Without rope contact the sweep takes the terms without contact, as with no surfaces, and
+    // flags only the lanes whose iterate may reach a surface this substep (|dx| at or above the
+    // substep's slack); those redo their own terms with contact after the exchange, in the same
+    // order (inertia, surfaces, stretch), so the sweep keeps the register budget of the
+    // surface-free kernel and results are those of the full evaluation, bit for bit.
+    constexpr bool kRedo = (SURF == SURF_PLANES || SURF == SURF_MESHES) && !ROPE;
     const Bin bin = a.bins[blockIdx.x];
     const int t = threadIdx.x;
-    const bool act = t < bin.vcount;
+    bool act = t < bin.vcount;
     const int dv = bin.vstart + t;
+    if constexpr (kChecked)
+        if (act && !(bin.vstart >= 0 && bin.vcount <= BLOCK && dv < a.n)) {
+            check_fail(a.status, CHK_BIN);
+            act = false;
+        }
 
     // ---- load this vertex: dynamic state in registers for the whole frame, rest rotations
     // and the previous substep's start velocity in shared memory
@@ -149,6 +161,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         q = a.q[dv];
         sm.qr[t] = a.qrest[dv];
         fl = (uint32_t)tp.x; lrope = tp.y; env = tp.w;
+        if constexpr (kChecked)
+            if (!checked_vertex(a, bin, t, tp.z, fl, lrope, env, SURF == SURF_MESHES ? a.num_sdf : 0)) act = false;
     }
     const bool hasNext = fl & F_NEXT, hasPrev = fl & F_PREV;
     const bool isRoot = (fl & F_ROOT) != 0;
@@ -160,6 +174,11 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         if (act) {
             const int4 gr = a.grp[dv];
             g0 = gr.x - bin.vstart; g1 = gr.y - bin.vstart; r0 = gr.z - bin.vstart; r1 = gr.w - bin.vstart;
+            if constexpr (kChecked)
+                if (!(0 <= g0 && g0 <= r0 && r0 <= t && t < r1 && r1 <= g1 && g1 <= bin.vcount)) {
+                    check_fail(a.status, CHK_GROUP);
+                    g0 = g1 = r0 = r1 = t;  // no candidates
+                }
         }
     }
     int ncol = 0;
@@ -235,7 +254,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             }
         }
         const float4* mycache = cache + lrope * nsdf * kPoseF4;
-        const float4* mytbox = (SURF == SURF_MESHES) ? tbox + lrope * nsdf * 2 : nullptr;
+        const float4* mytbox = (SURF == SURF_MESHES && a.surf_cull) ? tbox + lrope * nsdf * 2 : nullptr;
 
         // ---- inertial prediction and initial guess
         f3 dx, y;
@@ -248,6 +267,16 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         }
         __syncthreads();  // B0
         const f3 p1 = hasNext ? xyz(sm.p[t + 1]) : zero3();
+        // the substep's slack, squared: no plane and no candidate lattice (this substep's poses are
+        // in the cache after B0) can be touched while |dx|^2 < slack2; -1 = evaluate every iteration
+        float slack2 = -1.f;
+        if constexpr (kRedo)
+            if (im != 0.f && a.surf_cull) {
+                float sl = plane_slack(a, p);
+                if constexpr (SURF == SURF_MESHES)
+                    if (cand && sl > 0.f) sl = fminf(sl, mesh_slack(a, mycache, cand, p));
+                slack2 = sl > 0.f ? (sl * sl) * 0.99998f : -1.f;
+            }
 
         // ---- rope-rope detection over the CTA-resident group (ascending j, cap kMaxCols) and
         // the step limit of segment i, batch.cu:19-49 and collision.cu:103-136
@@ -269,20 +298,15 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
             f3 f, f2;
             sym3 H, H2;
             const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
-            // Planes only: the sweep takes the terms without contact, as with no surfaces, and
-            // flags the lanes whose probe may be in a plane's contact band; those redo their own
-            // terms with contact after the exchange, in the same order (inertia, surfaces,
-            // stretch), so the sweep keeps the register budget of the plane-free kernel.
-            constexpr bool kRedo = SURF == SURF_PLANES && !ROPE;
             bool touched;
             if constexpr (kRedo) {
                 position_terms<SURF_NONE>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
-                touched = im != 0.f && near_planes(a, p, dx);
+                touched = im != 0.f && !(dot(dx, dx) < slack2);
             } else {
                 touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2,
                                                btab, mytbox);
             }
-            if constexpr (ROPE) collision_sectors(a, ncol, dv, sm.p, sm.dx, damp, p, p1, dx, p1dx, f, f2, H, H2);
+            if constexpr (ROPE) collision_sectors(a, ncol, dv, sm.p, sm.dx, damp, p, p1, dx, p1dx, f, f2, H, H2, bin.vcount);
             // Without rope contact the segment's share H2 is its stretch term alone, dd I
             // (position_terms), so one float4 carries the whole exchange.
             if (act) {
@@ -313,7 +337,7 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
                         f3 g2;
                         sym3 G2;
                         touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H,
-                                                       g2, G2);
+                                                       g2, G2, btab, mytbox);
                         if (hasPrev) {
                             const float4 fa = sm.fa[t - 1];
                             f += xyz(fa);
@@ -350,7 +374,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         // ---- velocity, drag, readout (planes, then meshes warp-cooperatively), advection, broad phase
         f3 fv = zero3();
         if (im != 0.f) {
-            const f3 tg = (a.drag_quad > 0.f) ? (hasNext ? qtangent(q) : qtangent(sm.q[cur][t - 1])) : zero3();
+            const f3 tg = (a.drag_quad > 0.f) ? (hasNext ? qtangent(q) : qtangent(sm.q[cur][(kChecked && t == 0) ? 0 : t - 1]))
+                                              : zero3();
             v = end_velocity(a, dx, invH, tg);
             if (SURF != SURF_NONE && a.forces_on) {
                 sym3 Hs = sym_zero();
@@ -359,7 +384,8 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
         }
         if constexpr (SURF == SURF_MESHES)
             if (a.forces_on && nsdf > 0)
-                mesh_readout_warp(a, mycache, (act && im != 0.f) ? cand : 0ull, p, dx, c.kc, h, env, fv, btab, mytbox);
+                mesh_readout_warp(a, mycache, (act && im != 0.f && !(dot(dx, dx) < slack2)) ? cand : 0ull, p, dx, c.kc,
+                                  h, env, fv, btab, mytbox);
         if (SURF != SURF_NONE && a.forces_on) facc += fv;
         p += dx;
         if (SURF == SURF_MESHES && nsdf > 0) cand = (im != 0.f) ? build_candidates(a, mycache, nsdf, p, dx) : 0ull;

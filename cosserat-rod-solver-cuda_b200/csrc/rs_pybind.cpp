@@ -394,7 +394,10 @@ std::unique_ptr<RopeBatch> make_batch(int N, const std::vector<int>& verts, cons
 
 }  // namespace
 
-PYBIND11_MODULE(_ropesim, m) {
+#ifndef RS_MODULE_NAME
+#define RS_MODULE_NAME _ropesim
+#endif
+PYBIND11_MODULE(RS_MODULE_NAME, m) {
     m.doc() = "B200 Stable Cosserat Rods engine (persistent sm_100a frame kernel) behind the ropesim API";
     m.attr("__version__") = rs_version();
 
@@ -913,6 +916,7 @@ PYBIND11_MODULE(_ropesim, m) {
         })
         .def("set_sync", [](RopeBatch& b, bool every_frame) { ok(rs_batch_set_sync(b.h, every_frame ? 1 : 0)); })
         .def("set_autotune", [](RopeBatch& b, bool on) { ok(rs_batch_set_autotune(b.h, on ? 1 : 0)); })
+        .def("set_culling", [](RopeBatch& b, bool on) { ok(rs_batch_set_culling(b.h, on ? 1 : 0)); }, py::arg("on"))
         .def("set_engine", [](RopeBatch& b, const std::string& e) {
             if (e != "persistent" && e != "plain") throw py::value_error("engine must be 'persistent' or 'plain'");
             ok(rs_batch_set_engine(b.h, e == "plain" ? 1 : 0));
@@ -924,6 +928,11 @@ PYBIND11_MODULE(_ropesim, m) {
         .def_property_readonly("last_error", [](RopeBatch& b) { int e; ok(rs_batch_status(b.h, &e, nullptr, nullptr)); return e; })
         .def_property_readonly("last_warning", [](RopeBatch& b) { int w; ok(rs_batch_status(b.h, nullptr, &w, nullptr)); return w; })
         .def_property_readonly("nonfinite", [](RopeBatch& b) { int f; ok(rs_batch_status(b.h, nullptr, nullptr, &f)); return f; })
+        .def("bounds_check", [](RopeBatch& b) {
+            int code = 0, checked = 0;
+            ok(rs_batch_bounds_check(b.h, &code, &checked));
+            return py::make_tuple(code, (bool)checked);
+        })
         .def_property_readonly("num_envs", [](RopeBatch& b) { return b.R; })
         .def_property_readonly("verts_per_rope", [](RopeBatch& b) { return b.V; })
         .def_property_readonly("rope_verts", [](RopeBatch& b) { return b.verts; })

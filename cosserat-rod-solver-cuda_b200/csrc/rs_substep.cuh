@@ -26,6 +26,34 @@ constexpr int kPoseF4 = 5;  // float4 per cached pose
 
 __device__ __forceinline__ uint64_t all_meshes(int n) { return n >= 64 ? ~0ull : ((1ull << n) - 1ull); }
 
+// Checked builds: the load-time checks of one vertex at bin-local index t (caller index uidx, its
+// rope's slot lrope among the bin's ropes, its rope's caller index env; nsdf meshes in the pose
+// cache). Flags whose neighbour reads would leave the bin are cleared, an out-of-range rope slot
+// is replaced by 0; returns false when the caller or rope index is out of range (the kernel then
+// drops the vertex: no reads or writes through those indices).
+__device__ __forceinline__ bool checked_vertex(const FrameArgs& a, const Bin& bin, int t, int uidx, uint32_t& fl,
+                                               int& lrope, int& env, int nsdf) {
+    if ((fl & (F_NEXT | F_NEXT_ORIENT)) && t + 1 >= bin.vcount) {
+        check_fail(a.status, CHK_NEXT);
+        fl &= ~(F_NEXT | F_NEXT_ORIENT);
+    }
+    if (((fl & F_PREV) || !(fl & F_NEXT)) && t < 1) {  // the rope's last vertex reads t - 1 as well
+        check_fail(a.status, CHK_PREV);
+        fl &= ~F_PREV;
+    }
+    if (nsdf > 0 && !(lrope >= 0 && lrope < bin.rcount && (lrope + 1) * nsdf <= a.pose_cache)) {
+        check_fail(a.status, CHK_POSE);
+        lrope = 0;
+    }
+    if (!(uidx >= 0 && uidx < a.n && env >= 0 && env < a.num_ropes)) {
+        check_fail(a.status, CHK_CALLER);
+        fl = 0;
+        env = 0;
+        return false;
+    }
+    return true;
+}
+
 // Shortest-arc SLERP with an nlerp fallback above dot 0.9995, batch.cu:106-114.
 __device__ __forceinline__ float4 slerp4(float4 a, float4 b, float t) {
     float d = dot4(a, b);
@@ -167,23 +195,30 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
     return touched;
 }
 
-// Whether the probe pos + d may be in some plane's contact band: surfaces() decides contact
-// exactly; this flag only has to include every probe it would find in contact. The 1 mm margin
-// covers any difference in evaluating the same gap expression for coordinates up to ~10 km.
-__device__ __forceinline__ bool near_planes(const FrameArgs& a, f3 pos, f3 d) {
-    constexpr float kMargin = 1e-3f;
-    if (a.num_planes == 1) {
-        const float4 P = a.planes[0];
-        const f3 n = mk3(P.x, P.y, P.z);
-        return (dot(n, pos) - P.w) + dot(n, d) - a.c_radius < kMargin;
+// The smallest sdf_slack over a vertex's candidate meshes at this substep's poses: while the
+// iterate d satisfies |d| < slack, surfaces() finds no mesh contact (persistent kernel: the mesh
+// terms are then skipped without rotating the probe into any lattice).
+__device__ __forceinline__ float mesh_slack(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos) {
+    float s = INFINITY;
+    for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
+        const int m = __ffsll((long long)mm) - 1;
+        if (a.grids[m].never) continue;
+        s = fminf(s, sdf_slack(a.grids[m], load_pose(cache + m * kPoseF4), pos, a.c_radius));
     }
-    bool near = false;
+    return s;
+}
+
+// How far a vertex's iterate d may move this substep before the probe pos + d could reach a
+// plane's contact band: gap(d) = (n.pos - w) + n.d - R >= (n.pos - w - R) - |d| for a unit
+// normal n, less a 1 mm margin that covers any difference in evaluating the gap expression for
+// coordinates up to ~10 km. INFINITY without planes.
+__device__ __forceinline__ float plane_slack(const FrameArgs& a, f3 pos) {
+    float s = INFINITY;
     for (int pl = 0; pl < a.num_planes; pl++) {
         const float4 P = a.planes[pl];
-        const f3 n = mk3(P.x, P.y, P.z);
-        near |= (dot(n, pos) - P.w) + dot(n, d) - a.c_radius < kMargin;
+        s = fminf(s, ((dot(mk3(P.x, P.y, P.z), pos) - P.w) - a.c_radius) - 1e-3f);
     }
-    return near;
+    return s;
 }
 
 // World AABB of a lattice's contact box under the pose (pos, q); an empty box when the lattice
@@ -387,12 +422,16 @@ __device__ __forceinline__ int detect_group(const FrameArgs& a, int t, int dv, i
 // (the reference's two sectors, cosserat.cu:99-182).
 __device__ __forceinline__ void collision_sectors(const FrameArgs& a, int ncol, int dv, const float4* P, const float4* D,
                                                   float damp, f3 p, f3 p1, f3 dx, f3 p1dx, f3& f, f3& f2, sym3& H,
-                                                  sym3& H2) {
+                                                  sym3& H2, int nloc = 0x7fffffff) {
     if (ncol <= 0) return;
     f3 fo = zero3(), f2o = zero3();
     sym3 Ho = sym_zero(), H2o = sym_zero();
     for (int cc = 0; cc < ncol; cc++) {
         const int j = a.cols[(size_t)cc * a.n + dv];
+        if (kChecked && !(j >= 0 && j + 1 < nloc)) {  // nloc: the vertices P and D hold
+            check_fail(a.status, CHK_CANDIDATE);
+            continue;
+        }
         const f3 b0 = xyz(P[j]), b1 = xyz(P[j + 1]);
         const f3 db0 = xyz(D[j]), db1 = xyz(D[j + 1]);
         if (cc & 1) collision_term(a, damp, p, p1, dx, p1dx, b0, b1, db0, db1, fo, f2o, Ho, H2o);

@@ -34,6 +34,28 @@ constexpr int kMaxCols = 128;    // rope-rope candidates per segment (YarnBall.h
 // Solver status words (YarnBall.h:204-208).
 enum : int { ERR_NONE = 0, ERR_MAX_COLLISIONS = 1, WARN_INTERPENETRATION = 2 };
 
+// Checked builds (-DROPESIM_CHECKED): the frame and adjoint kernels test every index that the
+// topology or the data could push out of range and record the first failing check's code in the
+// fourth status word (the access is then skipped or redirected in range; nothing traps). The
+// regular build compiles the checks away.
+#ifdef ROPESIM_CHECKED
+constexpr bool kChecked = true;
+#else
+constexpr bool kChecked = false;
+#endif
+enum : int {
+    CHK_NONE = 0,
+    CHK_BIN = 1,         // a bin's vertex range outside [0, n) or larger than the CTA
+    CHK_NEXT = 2,        // a next-vertex / next-segment flag on the bin's last vertex (reads t + 1)
+    CHK_PREV = 3,        // a previous-vertex read (t - 1) at the bin's first vertex
+    CHK_CALLER = 4,      // a caller-order index or rope (env) index out of range
+    CHK_GROUP = 5,       // a rope-rope contact group or rope range outside the bin
+    CHK_CANDIDATE = 6,   // a rope-rope candidate segment outside the bin
+    CHK_POSE = 7,        // a pose-cache slot outside the cache, or a mesh bit beyond num_sdf
+    CHK_LATTICE = 8,     // a lattice node outside its grid
+    CHK_BLOCK = 9,       // a lattice block-bound index outside its table
+};
+
 // One bin = one CTA: a contiguous range of device vertices and of device ropes.
 struct Bin {
     int vstart, vcount;   // device vertices [vstart, vstart + vcount)
@@ -64,6 +86,11 @@ struct GridDesc {
     // bound <= radius + 1e-5), padded by 1e-4; never = 1 when no block qualifies
     float tlo[3], thi[3];
     int never;
+    int* status;   // the batch's status words (checked builds record lattice index failures there)
+    // 1 / L, rounded down, with L = |(Dx, Dy, Dz)| and D the largest node difference along an axis
+    // divided by the spacing: the trilinear field is Lipschitz with constant L, so a probe moved by
+    // |d| changes phi by at most L |d| (the persistent kernel's per-substep contact slack)
+    float lip_inv;
 };
 
 // Kinematic pose of (env, mesh) at the end of a substep: position, rotor (x, y, z, w),
@@ -128,9 +155,10 @@ struct FrameArgs {
     int pose_cache;          // pose cache entries per buffer (= max ropes per bin * num_sdf)
     const Pose* poses;       // [envs * 64] committed static poses
     const Motion* motion;    // [envs * 64] this frame's motion (sdf_moving)
-    // rope-rope contact (YarnBall.h:175-192; batch.cu:19-49, 504-522)
+    // rope-rope contact (YarnBall.h:175-192; batch.cu:19-49, 367-385)
     int rope_contact;        // 0 = off
     int n;                   // vertices (stride of the candidate lists)
+    int num_ropes;           // ropes (rows of the root program, envs of the mesh poses)
     float rc_radius, rc_barrier, rc_kcol, rc_mu, rc_kfric;
     float det_radius, sdet_radius;  // radius + barrier/2, and that times the detection scaler
     const int4* grp;         // per device vertex: (group start, group end, rope start, rope end)
@@ -140,6 +168,7 @@ struct FrameArgs {
     float* pad;              // [n] detection paddings (plain engine)
     GridDesc grids[kMaxSdf];
     int sdf_skip;            // 1: a lattice block whose lower bound clears the radius skips the sample
+    int surf_cull;           // 1: the persistent kernel skips surface terms below the substep's slack (exact)
     int sdf_btab;            // floats of block bounds staged per CTA in shared memory (0 = read from L2)
     // differentiable frames: when set, the state after each substep's root program is written to
     // tape[(s * 4 + f) * n + u] for f = x, v, lv (previous substep's start velocity), q and the

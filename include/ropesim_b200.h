@@ -45,7 +45,7 @@ RS_API const char* rs_last_error_string(void);
 RS_API const char* rs_version(void);
 
 /* ---------------------------------------------------------------- construction
- * Replaces RopeBatch::RopeBatch + Sim::configure/setKStretch/setKBend (csrc/batch.cu:330-413,
+ * Replaces RopeBatch::RopeBatch + Sim::configure/setKStretch/setKBend (csrc/batch.cu:193-276,
  * YarnBall.cu:112-259) and RopeSim::RopeSim (bindings.cpp:196-265).
  * rope_verts[num_ropes] (each >= 3, <= 1024; uneven lengths allowed), positions host
  * [sum(rope_verts), 3], pinned host [sum(rope_verts)] or NULL (each rope's first vertex).
@@ -88,6 +88,13 @@ RS_API int rs_batch_layout(rs_batch* b, int* block, int* num_bins);
  * one candidate bin size, then the fastest is kept (results are bitwise identical across bin
  * sizes) and remembered per workload signature for the process. */
 RS_API int rs_batch_set_autotune(rs_batch* b, int on);
+/* The persistent kernel's exact early outs (default on): per substep, the iterate displacement
+ * below which no plane and no candidate lattice can be reached (Lipschitz bound of the trilinear
+ * field), per lattice the world box of the blocks that can reach the contact radius, and the
+ * blocks whose lower bound clears it. They only skip evaluations whose gap is >= 0, so results
+ * are bitwise the same either way; off evaluates every surface at every iteration, as the
+ * reference does (for checking that claim). No counterpart in the reference. */
+RS_API int rs_batch_set_culling(rs_batch* b, int on);
 /* Engine: 0 = one persistent kernel per control frame (default); 1 = the per-substep-launch
  * plain path (the reference's launch structure: root, init, num_itr x (position, frame), end
  * kernels per substep, the iterations replayed from a CUDA graph), the in-repo baseline. */
@@ -142,7 +149,10 @@ RS_API int rs_batch_step_free(rs_batch* b, float dt, int substeps);
  * vertices, pending host edits, contact groups larger than one CTA, and the plain engine. The
  * array's device address is looked up on the first call on each device (keep that first call
  * outside any stream capture). All such calls share the array: calls that overlap on the GPU
- * race. Results equal rs_batch_step_program's. */
+ * race. Results equal rs_batch_step_program's, bit for bit. The handle's own candidate buffer
+ * is still allocated when rope contact is enabled (rs_batch_set_rope_contact, at set-up), so
+ * the static array saves no memory: what it removes is any allocation while stepping. With
+ * rs_batch_set_timing on, rs_batch_last_frame_ms reports this call's frame kernel too. */
 RS_API int rs_batch_step_program_static_scratch(rs_batch* b, const float* p0, const float* v0, const float* p1,
                                                 const float* q0, const float* q1, float dt, int substeps);
 RS_API int rs_batch_advance(rs_batch* b, float dt, int substeps);
@@ -158,6 +168,15 @@ RS_API int rs_batch_views(rs_batch* b, float** pos, float** vel, float** quat);
 /* Solver status (Sim::lastErrorCode / lastWarningCode, bindings.cpp:578-579) and a sticky
  * flag raised when a frame produced a non-finite position. */
 RS_API int rs_batch_status(rs_batch* b, int* last_error, int* last_warning, int* nonfinite);
+/* The checked build (libropesim_b200_checked.so, compiled with -DROPESIM_CHECKED) tests every
+ * neighbour, candidate, pose-cache, lattice, caller and group index its frame and adjoint kernels
+ * use and records the first failed check (code: 1 bin range, 2 next-vertex read, 3 previous-vertex
+ * read, 4 caller / rope index, 5 contact-group range, 6 candidate segment, 7 pose-cache slot or
+ * mesh bit, 8 lattice node, 9 lattice block bound; 0 = none) instead of trapping; the access is
+ * skipped or kept in range. *code: that record (sticky; always 0 in the regular build);
+ * *checked: 1 in the checked build. No counterpart in the reference (a stand-in for running the
+ * kernels under a memory checker). */
+RS_API int rs_batch_bounds_check(rs_batch* b, int* code, int* checked);
 /* CUDA stream the handle's device work runs on. */
 RS_API int rs_batch_stream(rs_batch* b, void** stream);
 /* Device time of the last frame kernel in ms (after rs_batch_set_timing(b, 1)). */
@@ -170,7 +189,7 @@ RS_API int rs_batch_last_frame_ms(rs_batch* b, double* ms);
 RS_API int rs_batch_set_contact(rs_batch* b, float radius, float mu_s, float mu_k, float v_slip, float kappa);
 RS_API int rs_batch_get_contact(rs_batch* b, float* radius, float* mu_s, float* mu_k);
 RS_API int rs_batch_set_planes(rs_batch* b, int count, const float* rows);
-/* RopeBatch::set_rope_contact (batch.cu:504-522, bindings.cpp:939-950): YarnBall's rope-rope
+/* RopeBatch::set_rope_contact (batch.cu:367-385, bindings.cpp:939-950): YarnBall's rope-rope
  * model (log barrier at 2 radius + barrier, friction spring capped at mu N, step limit) on
  * candidates from a per-group brute-force detector; group_ropes consecutive ropes form one
  * contact group. Groups that fit one CTA (<= 1024 vertices) stay on the persistent kernel;

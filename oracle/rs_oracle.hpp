@@ -11,8 +11,8 @@
 // Parity pin: the reference cannot be built here (GLM is absent), so this restatement is
 // pinned by the reference's own known-answer tests (hanging elongation, cantilever droop,
 // pendulum period, Coulomb incline, rest support = weight, program endpoint, ...), ported
-// to run against it on the CPU (tests/test_oracle_*.py). Golden fixtures generated from it
-// live in tests/golden/.
+// to run against it on the CPU (tests/test_physics.py, tests/test_accept_*.py, the oracle
+// backend of each parametrized test). Golden fixtures generated from it live in tests/golden/.
 //
 // Reference files followed (paths within the reference project):
 //   third_party/yarnball/KittenEngine/YarnBall/YarnBall.cu:11-61,112-259,261-272   setup
@@ -21,8 +21,8 @@
 //   third_party/yarnball/KittenEngine/YarnBall/sim/contact.cuh:27-204              surfaces
 //   third_party/yarnball/KittenEngine/YarnBall/sim/collision.cu:103-136            step limit
 //   third_party/yarnball/KittenEngine/YarnBall/sim/step.cpp:37-57                  advance
-//   csrc/batch.cu:19-49,90-159,178-189,330-413                                     batch driver
-//   csrc/sdf.cu:25-92,137-360                                                      mesh poses
+//   csrc/batch.cu:19-49,90-159,178-276,288-413                                     batch driver
+//   csrc/sdf.cu:25-92,137-270                                                      mesh poses
 //   third_party/yarnball/KittenEngine/KittenEngine/includes/modules/Rotor.h:57-188 rotor algebra
 //   third_party/yarnball/KittenEngine/KittenEngine/includes/modules/Common.h:327-345 seg-seg
 #pragma once

@@ -53,7 +53,8 @@ def c2_positions(N, V, seed):
     return pos.astype(np.float32), roots.astype(np.float32)
 
 
-def program(mod, N=8, V=64, frames=20, S=100, seed=1, to_dev=None, precision=None, views=None, v_std=0.5, p_std=0.05):
+def program(mod, N=8, V=64, frames=20, S=100, seed=1, to_dev=None, precision=None, views=None, v_std=0.5, p_std=0.05,
+            tweak=None):
     """Config 2's workload (64-vertex jittered ropes hanging clear of the plane z = 0, program
     roots with v0 ~ N(0, v_std), p1 = p0 + N(0, p_std)) at reduced N and frames."""
     kw = {} if precision is None else {"precision": precision}
@@ -63,6 +64,8 @@ def program(mod, N=8, V=64, frames=20, S=100, seed=1, to_dev=None, precision=Non
     b.damping = 0.0
     b.drag = 0.0
     b.set_planes(np.array([[0, 0, 1, 0]], np.float32), radius=0.00635)
+    if tweak:
+        tweak(b)
     rng = np.random.default_rng(seed + 100)
     p0 = roots.copy()
     out = []
@@ -123,7 +126,7 @@ def walk_poses(rng, pos, q, step=0.004, ang=0.02):
     return pos, qn.astype(np.float32)
 
 
-def uneven(mod, sdf_mod, R=6, frames=10, S=50, seed=3, to_dev=None, precision=None, forces=True):
+def uneven(mod, sdf_mod, R=6, frames=10, S=50, seed=3, to_dev=None, precision=None, forces=True, tweak=None):
     """Config 3's workload at reduced size: uneven ropes, per-rope EA/EI, per-vertex masses,
     two planes, three meshes teleported to random per-env poses and then walked randomly."""
     kw = {} if precision is None else {"precision": precision}
@@ -157,6 +160,8 @@ def uneven(mod, sdf_mod, R=6, frames=10, S=50, seed=3, to_dev=None, precision=No
         b.add_mesh(*g.as_args(), pos=p[0, 0], quat=q[0, 0])
     if forces:
         b.enable_contact_forces(True)
+    if tweak:
+        tweak(b)
     out, fo, wr = [], [], []
     M = len(grids)
     # meshes start next to each rope (offsets from its root along its length), random frames
@@ -177,7 +182,7 @@ def uneven(mod, sdf_mod, R=6, frames=10, S=50, seed=3, to_dev=None, precision=No
     return np.stack(out), (np.stack(fo) if forces else None), (np.stack(wr) if forces else None), lens
 
 
-def planes_only(mod, planes, R=6, frames=10, S=50, seed=11, to_dev=None, precision=None):
+def planes_only(mod, planes, R=6, frames=10, S=50, seed=11, to_dev=None, precision=None, tweak=None):
     """Uneven ropes (16..64 vertices, roots held, 25 degrees from vertical, lowest vertex 2 cm up)
     swinging onto `planes` alone (no meshes), contact-force readout on: the plane-only kernel
     with one plane or with several."""
@@ -190,6 +195,8 @@ def planes_only(mod, planes, R=6, frames=10, S=50, seed=11, to_dev=None, precisi
     b.drag = 0.1
     b.set_planes(np.asarray(planes, np.float32), radius=0.005, mu_s=0.5, mu_k=0.4)
     b.enable_contact_forces(True)
+    if tweak:
+        tweak(b)
     out, fo = [], []
     for _ in range(frames):
         b.step_free(1.0 / 60.0, S)

@@ -174,3 +174,28 @@ def test_bitwise_replay_and_block_invariance(mods):
         assert l2[0] == block
         for x, y in zip(ref, other):
             np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+def test_exact_culling_is_bitwise_inert(mods):
+    """The persistent kernel's early outs (the per-substep surface slack, the lattices' contact
+    boxes and block bounds) only skip evaluations whose gap is >= 0: with them off (every plane
+    and every candidate lattice evaluated at every iteration, as the reference does) positions,
+    contact forces and mesh wrenches are the same bit for bit, on plane-only scenes (one plane
+    and three), the uneven scene with teleported and walking meshes, and config-2 ropes."""
+    rs, _ = mods
+    from ropesim import sdf
+
+    off = lambda b: b.set_culling(False)
+    for planes in ([[0, 0, 1, 0.02]], [[0, 0, 1, 0], [0.3, 0, 1, -0.05], [-0.2, 0.1, 1, -0.03]]):
+        a, af = S.planes_only(rs, planes, frames=4)
+        b, bf = S.planes_only(rs, planes, frames=4, tweak=off)
+        np.testing.assert_array_equal(a.view(np.uint64), b.view(np.uint64))
+        np.testing.assert_array_equal(af.view(np.uint64), bf.view(np.uint64))
+    g, gf, gw, _ = S.uneven(rs, sdf, to_dev=to_dev, frames=4)
+    h, hf, hw, _ = S.uneven(rs, sdf, to_dev=to_dev, frames=4, tweak=off)
+    assert np.abs(gw).max() > 0.0
+    for x, y in ((g, h), (gf, hf), (gw, hw)):
+        np.testing.assert_array_equal(x.view(np.uint64), y.view(np.uint64))
+    c = S.program(rs, N=6, frames=4, to_dev=to_dev, views=views)
+    d = S.program(rs, N=6, frames=4, to_dev=to_dev, views=views, tweak=off)
+    np.testing.assert_array_equal(c.view(np.uint64), d.view(np.uint64))

@@ -5,9 +5,12 @@ GPU's memory for their own allocator, control loops whose memory is fixed at sta
 runtimes that forbid allocation after initialisation. For them the library keeps the rope-rope
 candidate lists in a static device array instead of a buffer of the handle. This test drives two
 identical batches in rope-rope contact through the C-ABI, one with the regular entry point
-(rs_batch_step_program) and one with the allocation-free one, for two frames in a row, and
-requires the same positions to the parity tolerance of the other GPU tests (1e-5 m); it also
-checks that a batch larger than the static array is refused with a clear error.
+(rs_batch_step_program) and one with the allocation-free one, for two frames in a row. Both run
+the same kernel on the same inputs and bins, so the positions must agree bit for bit (well within
+the 1e-5 m parity tolerance of the other GPU tests). The device's free memory must not change
+across the second allocation-free call (the first call on a device may load the kernel module),
+and the call reports its frame time when timing is on. A batch larger than the static array is
+refused with a clear error.
 """
 import ctypes
 import os
@@ -67,6 +70,7 @@ def test_static_scratch_step_matches_regular_step():
     L = lib()
     a, pos = make(L)
     b, _ = make(L)
+    ok(L, L.rs_batch_set_timing(b, 1))
     ropes, verts = pos.shape[:2]
     roots = pos[:, 0].copy()
     sway = (np.arange(ropes) % 2 - 0.5)[:, None] * np.array([0.0, 0.02, 0.0], np.float32)
@@ -77,13 +81,22 @@ def test_static_scratch_step_matches_regular_step():
         v0 = ((p1 - p0) * 60).contiguous()
         torch.cuda.synchronize()
         ok(L, L.rs_batch_step_program(a, ptr(p0), ptr(v0), ptr(p1), None, None, F(1 / 60), 50, 0))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         ok(L, L.rs_batch_step_program_static_scratch(b, ptr(p0), ptr(v0), ptr(p1), None, None, F(1 / 60), 50))
+        free1 = torch.cuda.mem_get_info()[0]
+        ms = ctypes.c_double(0.0)
+        ok(L, L.rs_batch_last_frame_ms(b, ctypes.byref(ms)))
         xa, xb = download(L, a, ropes * verts), download(L, b, ropes * verts)
         d = np.max(np.linalg.norm(xa - xb, axis=1))
         moved = np.max(np.linalg.norm(xa - pos.reshape(-1, 3), axis=1))
-        print(f"\n  frame {f}: regular vs allocation-free step {d:.2e} m (ropes moved up to {moved:.3f} m)")
+        print(f"\n  frame {f}: regular vs allocation-free step {d:.2e} m (ropes moved up to {moved:.3f} m), "
+              f"free device memory {free0} -> {free1} B, frame kernel {ms.value:.3f} ms")
         assert np.isfinite(xb).all() and moved > 1e-4
-        assert d <= TOL
+        assert d <= TOL and np.array_equal(xa.astype(np.float32).view(np.uint32), xb.astype(np.float32).view(np.uint32))
+        assert ms.value > 0.0
+        if f == 1:
+            assert free1 == free0, "the allocation-free step changed the device's free memory"
     for h in (a, b):
         ok(L, L.rs_batch_destroy(h))
 
