@@ -97,6 +97,7 @@ Batch::Batch(int num_ropes, const int* rope_verts, const float* positions, const
     check(cudaStreamCreate(&stream_), "cudaStreamCreate");
     check(cudaEventCreate(&ev0_), "cudaEventCreate");
     check(cudaEventCreate(&ev1_), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&ev_cost_, cudaEventDisableTiming), "cudaEventCreate");
     host_dyn_valid_ = true;
     device_valid_ = false;
     layout_valid_ = false;
@@ -113,7 +114,8 @@ Batch::~Batch() {
     }
     void* bufs[] = {d_bins_, d_ropes_, d_topo_, d_pos_, d_vel_, d_lvel_, d_q_, d_qrest_, d_qdir_, d_init_pos_, d_init_q_,
                     d_out_pos_, d_out_vel_, d_out_q_, d_prog_, d_status_, d_ranges_, d_boxes_, d_cur_, d_tgt_,
-                    d_tele_, d_motion_, d_poses_, d_stage_, d_stage_tele_, d_force_, d_wrench_};
+                    d_tele_, d_motion_, d_poses_, d_stage_, d_stage_tele_, d_force_, d_wrench_, d_queue_, d_order_,
+                    d_bin_cost_};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (pl_graph_) cudaGraphExecDestroy(pl_graph_);
@@ -128,6 +130,9 @@ Batch::~Batch() {
     if (h_status_) cudaFreeHost(h_status_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
+    if (ev_cost_) cudaEventDestroy(ev_cost_);
+    if (h_bin_cost_) cudaFreeHost(h_bin_cost_);
+    if (h_order_) cudaFreeHost(h_order_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -286,6 +291,15 @@ void Batch::alloc_device() {
         check(cudaMalloc(p, bytes), what);
     };
     alloc((void**)&d_bins_, sizeof(Bin) * bins_.size(), "cudaMalloc(bins)");
+    alloc((void**)&d_order_, sizeof(int) * bins_.size(), "cudaMalloc(bin order)");
+    alloc((void**)&d_bin_cost_, sizeof(float) * bins_.size(), "cudaMalloc(bin times)");
+    if (!d_queue_) alloc((void**)&d_queue_, sizeof(int), "cudaMalloc(work queue)");
+    if (h_bin_cost_) cudaFreeHost(h_bin_cost_);
+    if (h_order_) cudaFreeHost(h_order_);
+    h_bin_cost_ = nullptr;
+    h_order_ = nullptr;
+    check(cudaMallocHost((void**)&h_bin_cost_, sizeof(float) * bins_.size()), "cudaMallocHost(bin times)");
+    check(cudaMallocHost((void**)&h_order_, sizeof(int) * bins_.size()), "cudaMallocHost(bin order)");
     alloc((void**)&d_ropes_, sizeof(Rope) * dropes_.size(), "cudaMalloc(ropes)");
     if (!d_pos_) {
         const size_t n4 = sizeof(float4) * n_;
@@ -345,6 +359,9 @@ void Batch::ensure_device() {
                 }
             }
         check(cudaMemcpy(d_bins_, bins_.data(), sizeof(Bin) * bins_.size(), cudaMemcpyHostToDevice), "upload(bins)");
+        for (size_t i = 0; i < bins_.size(); i++) h_order_[i] = (int)i;  // first frame: packing order
+        check(cudaMemcpy(d_order_, h_order_, sizeof(int) * bins_.size(), cudaMemcpyHostToDevice), "upload(bin order)");
+        costs_inflight_ = false;
         check(cudaMemcpy(d_ropes_, dropes_.data(), sizeof(Rope) * dropes_.size(), cudaMemcpyHostToDevice), "upload(ropes)");
         check(cudaMemcpy(d_topo_, topo.data(), sizeof(int4) * n_, cudaMemcpyHostToDevice), "upload(topo)");
         check(cudaMemcpy(d_init_pos_, ip.data(), sizeof(float4) * n_, cudaMemcpyHostToDevice), "upload(init pos)");
@@ -529,6 +546,8 @@ void Batch::stage_rows(const float* p0, const float* v0, const float* p1, const 
 FrameArgs Batch::frame_args(int root_mode, bool has_q0, bool has_q1, float dt, int steps) const {
     FrameArgs a{};
     a.bins = d_bins_; a.ropes = d_ropes_; a.topo = d_topo_;
+    a.num_bins = (int)bins_.size();
+    a.queue = nullptr; a.order = nullptr; a.bin_cost = nullptr;  // static grid unless run_frame queues
     a.pos = d_pos_; a.vel = d_vel_; a.lvel = d_lvel_; a.q = d_q_; a.qrest = d_qrest_;
     a.out_pos = d_out_pos_; a.out_vel = d_out_vel_; a.out_q = d_out_q_;
     a.out_force = d_force_; a.wrench = d_wrench_; a.status = d_status_;
@@ -570,12 +589,56 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
     FrameArgs a = frame_args(root_mode, has_q0, has_q1, dt, steps);
     a.tape = pending_tape_;
     a.itape = pending_itape_;
+    const bool plain = engine_ == 1 || (rope_contact_ && oversize_);
+    const bool queued = queue_ && !plain;
+    if (queued) {
+        // the previous frame's bin times, if they have arrived, set this frame's order
+        if (costs_inflight_) {
+            if (cudaEventQuery(ev_cost_) == cudaSuccess) reorder_bins();
+            else cudaGetLastError();  // "not ready" is no error: keep the previous order
+            costs_inflight_ = false;
+        }
+        check(cudaMemsetAsync(d_queue_, 0, sizeof(int), stream_), "zero(work queue)");
+        a.queue = d_queue_; a.order = d_order_; a.bin_cost = d_bin_cost_;
+    }
     const bool timed = timing_ || tuning();
     if (timed) check(cudaEventRecord(ev0_, stream_), "event");
-    if (engine_ == 1 || (rope_contact_ && oversize_)) run_frame_plain(a);
+    if (plain) run_frame_plain(a);
     else check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");
     if (timed) check(cudaEventRecord(ev1_, stream_), "event");
+    if (queued && sync_every_frame) {
+        check(cudaMemcpyAsync(h_bin_cost_, d_bin_cost_, sizeof(float) * bins_.size(), cudaMemcpyDeviceToHost, stream_),
+              "download(bin times)");
+        check(cudaEventRecord(ev_cost_, stream_), "event");
+        costs_inflight_ = true;
+    }
     host_dyn_valid_ = false;
+}
+
+// Longest-processing-time-first order of the bins from the last frame's measured times, so the
+// work queue hands the slowest bins out first and no slow bin starts last. A counting pass over
+// 64 equal-width cost buckets (slowest bucket first, packing order within a bucket) keeps the
+// host's turn between frames O(bins): exact LPT is not needed, only no slow bin at the end.
+void Batch::reorder_bins() {
+    constexpr int kBuckets = 64;
+    const int nb = (int)bins_.size();
+    float lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < nb; i++) {
+        lo = std::min(lo, h_bin_cost_[i]);
+        hi = std::max(hi, h_bin_cost_[i]);
+    }
+    if (!(hi > lo)) return;  // uniform (or unmeasured) bins: keep the order
+    const float scale = (kBuckets - 1) / (hi - lo);
+    int count[kBuckets + 1] = {};
+    order_scratch_.resize(nb);
+    for (int i = 0; i < nb; i++) {
+        const int k = kBuckets - 1 - std::min(kBuckets - 1, std::max(0, (int)((h_bin_cost_[i] - lo) * scale)));
+        order_scratch_[i] = k;
+        count[k + 1]++;
+    }
+    for (int k = 0; k < kBuckets; k++) count[k + 1] += count[k];
+    for (int i = 0; i < nb; i++) h_order_[count[order_scratch_[i]]++] = i;
+    check(cudaMemcpyAsync(d_order_, h_order_, sizeof(int) * nb, cudaMemcpyHostToDevice, stream_), "upload(bin order)");
 }
 
 // The grid broad phase serves contact groups larger than one CTA (the brute force's O(V²) pairs

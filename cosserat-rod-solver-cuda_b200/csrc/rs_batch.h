@@ -181,6 +181,7 @@ public:
     // fastest is kept and remembered for this workload signature in this process.
     void set_autotune(bool on) { autotune_ = on; }
     void set_culling(bool on) { culling_ = on; }  // the persistent kernel's exact early outs
+    void set_work_queue(bool on) { queue_ = on; costs_inflight_ = false; }  // the frame kernel's bin scheduling
     // Engine: 0 = one persistent launch per frame (default), 1 = the per-substep-launch plain
     // path (root, init, num_itr x (position, frame), end kernels per substep, graph-replayed).
     void set_engine(int e);
@@ -246,6 +247,18 @@ private:
     int* h_status_ = nullptr;       // pinned [4]
     int2* d_ranges_ = nullptr;      // [R] reset ranges
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    // the frame kernel's work queue (frame_kernel): counter, bin order (longest measured first),
+    // per-bin times of the last frame (device and pinned host copies)
+    bool queue_ = true;
+    int* d_queue_ = nullptr;
+    int* d_order_ = nullptr;
+    float* d_bin_cost_ = nullptr;
+    float* h_bin_cost_ = nullptr;
+    int* h_order_ = nullptr;
+    std::vector<int> order_scratch_;
+    bool costs_inflight_ = false;
+    cudaEvent_t ev_cost_ = nullptr;
+    void reorder_bins();
     bool timing_ = false;
     double last_frame_ms_ = 0.0;
     bool autotune_ = true, tuned_ = false;

@@ -210,6 +210,13 @@ int rs_batch_set_culling(rs_batch* b, int on) {
         s.set_culling(on != 0);
     });
 }
+int rs_batch_set_work_queue(rs_batch* b, int on) {
+    return guarded([&] {
+        rs::Batch& s = B(b);
+        std::lock_guard<std::mutex> g(s.mutex());
+        s.set_work_queue(on != 0);
+    });
+}
 int rs_batch_set_engine(rs_batch* b, int engine) {
     return guarded([&] {
         rs::Batch& s = B(b);

@@ -18,6 +18,7 @@
 // displacement publish; the frame step reads a double-buffered rotor array and needs none).
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
 
 #include "rs_device.cuh"
@@ -121,8 +122,9 @@ __device__ __forceinline__ void mesh_readout_warp(const FrameArgs& a, const floa
     }
 }
 
+// One bin of a frame: every substep of the bin's ropes, state in registers and shared memory.
 template <int BLOCK, int SURF, bool ROPE>
-__global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame_kernel(const FrameArgs a) {
+__device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
     // FrameSmem<BLOCK>, the pose cache [2][pose_cache][kPoseF4], then the lattice block bounds
     extern __shared__ float4 dyn_smem[];
     FrameSmem<BLOCK>& sm = *reinterpret_cast<FrameSmem<BLOCK>*>(dyn_smem);
@@ -134,7 +136,6 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
     // order (inertia, surfaces, stretch), so the sweep keeps the register budget of the
     // surface-free kernel and results are those of the full evaluation, bit for bit.
     constexpr bool kRedo = (SURF == SURF_PLANES || SURF == SURF_MESHES) && !ROPE;
-    const Bin bin = a.bins[blockIdx.x];
     const int t = threadIdx.x;
     bool act = t < bin.vcount;
     const int dv = bin.vstart + t;
@@ -412,6 +413,47 @@ __global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame
     }
 }
 
+// The frame: one bin per CTA (grid = bins), or, with the work queue (a.queue), resident CTAs
+// that take bins from an atomic counter in the order a.order gives (the host's longest-first
+// order of the previous frame's measured bin times) until none is left, so contact-heavy bins
+// start first and the frame does not end on a few late, slow bins. Each bin's time (SM clock
+// cycles from its start to its end) goes to a.bin_cost. A bin's result does not depend on which
+// CTA runs it or when: the schedule changes no bit of the output.
+template <int BLOCK, int SURF, bool ROPE>
+__global__ void __launch_bounds__(BLOCK, RS_MIN_BLOCKS(BLOCK, SURF, ROPE)) frame_kernel(const FrameArgs a) {
+    __shared__ int next;
+    int k = blockIdx.x;
+    for (;;) {
+        if (a.queue) {
+            __syncthreads();  // the previous bin is done with shared memory and has read `next`
+            if (threadIdx.x == 0) next = atomicAdd(a.queue, 1);
+            __syncthreads();
+            k = next;
+        }
+        if (k >= a.num_bins) break;
+        const int b = a.order ? a.order[k] : k;
+        const long long c0 = clock64();
+        frame_bin<BLOCK, SURF, ROPE>(a, a.bins[b]);
+        if (a.bin_cost && threadIdx.x == 0) a.bin_cost[b] = float(clock64() - c0);
+        if (!a.queue) break;
+    }
+}
+
+// Resident CTAs of a kernel on this device (occupancy x SMs), cached per kernel and shared size.
+static int resident_ctas(const void* kernel, int block, size_t dyn_smem) {
+    static std::mutex mtx;
+    static std::map<std::pair<const void*, size_t>, int> cache;
+    std::lock_guard<std::mutex> g(mtx);
+    const auto key = std::make_pair(kernel, dyn_smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, dyn_smem) != cudaSuccess)
+        return 0;
+    return cache[key] = sms * per;
+}
+
 // ------------------------------------------------------------------ launch
 template <int BLOCK, int SURF, bool ROPE>
 static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_bytes, cudaStream_t s) {
@@ -421,7 +463,13 @@ static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
         if (e != cudaSuccess) return e;
     }
-    k<<<num_bins, BLOCK, dyn_smem, s>>>(a);
+    int grid = num_bins;
+    if (a.queue) {  // the work queue: as many CTAs as can be resident at once
+        const int res = resident_ctas(reinterpret_cast<const void*>(k), BLOCK, dyn_smem);
+        if (res <= 0) return cudaErrorInvalidConfiguration;
+        grid = res < num_bins ? res : num_bins;
+    }
+    k<<<grid, BLOCK, dyn_smem, s>>>(a);
     return cudaGetLastError();
 }
 

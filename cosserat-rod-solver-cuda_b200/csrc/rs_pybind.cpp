@@ -917,6 +917,7 @@ PYBIND11_MODULE(RS_MODULE_NAME, m) {
         .def("set_sync", [](RopeBatch& b, bool every_frame) { ok(rs_batch_set_sync(b.h, every_frame ? 1 : 0)); })
         .def("set_autotune", [](RopeBatch& b, bool on) { ok(rs_batch_set_autotune(b.h, on ? 1 : 0)); })
         .def("set_culling", [](RopeBatch& b, bool on) { ok(rs_batch_set_culling(b.h, on ? 1 : 0)); }, py::arg("on"))
+        .def("set_work_queue", [](RopeBatch& b, bool on) { ok(rs_batch_set_work_queue(b.h, on ? 1 : 0)); }, py::arg("on"))
         .def("set_engine", [](RopeBatch& b, const std::string& e) {
             if (e != "persistent" && e != "plain") throw py::value_error("engine must be 'persistent' or 'plain'");
             ok(rs_batch_set_engine(b.h, e == "plain" ? 1 : 0));

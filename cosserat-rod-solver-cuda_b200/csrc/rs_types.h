@@ -123,6 +123,13 @@ enum : int { ROOT_NONE = 0, ROOT_PROGRAM = 1, ROOT_SET = 2 };
 struct FrameArgs {
     // topology (device order)
     const Bin* bins;
+    int num_bins;
+    // the work queue (rs_frame.cu, frame_kernel): with `queue` set, resident CTAs take bins from
+    // *queue (zeroed before the launch) in the order `order` gives; `bin_cost` receives each bin's
+    // time in SM cycles (both may be null)
+    int* queue;
+    const int* order;
+    float* bin_cost;
     const Rope* ropes;
     const int4* topo;        // (flags, local rope within the bin, uidx, env)
     // state (device order), updated in place

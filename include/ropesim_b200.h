@@ -95,6 +95,11 @@ RS_API int rs_batch_set_autotune(rs_batch* b, int on);
  * are bitwise the same either way; off evaluates every surface at every iteration, as the
  * reference does (for checking that claim). No counterpart in the reference. */
 RS_API int rs_batch_set_culling(rs_batch* b, int on);
+/* Bin scheduling of the frame kernel (default on): resident CTAs take bins from a work queue in
+ * longest-first order of the previous frame's measured bin times (measured when the step reads
+ * its status every frame); off launches one CTA per bin in packing order. Results are bitwise
+ * the same either way. No counterpart in the reference (its substep launches per kernel). */
+RS_API int rs_batch_set_work_queue(rs_batch* b, int on);
 /* Engine: 0 = one persistent kernel per control frame (default); 1 = the per-substep-launch
  * plain path (the reference's launch structure: root, init, num_itr x (position, frame), end
  * kernels per substep, the iterations replayed from a CUDA graph), the in-repo baseline. */

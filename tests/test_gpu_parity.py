@@ -199,3 +199,21 @@ def test_exact_culling_is_bitwise_inert(mods):
     c = S.program(rs, N=6, frames=4, to_dev=to_dev, views=views)
     d = S.program(rs, N=6, frames=4, to_dev=to_dev, views=views, tweak=off)
     np.testing.assert_array_equal(c.view(np.uint64), d.view(np.uint64))
+
+
+def test_work_queue_schedule_is_bitwise_inert(mods):
+    """Bins taken from the work queue in longest-first order of the previous frame's times, or one
+    CTA per bin in packing order: the same bits, on config-2 ropes and the uneven mesh scene (the
+    order changes from the second frame on, once bin times have been measured)."""
+    rs, _ = mods
+    from ropesim import sdf
+
+    grid = lambda b: b.set_work_queue(False)
+    a = S.program(rs, N=12, frames=4, to_dev=to_dev, views=views)
+    b = S.program(rs, N=12, frames=4, to_dev=to_dev, views=views, tweak=grid)
+    np.testing.assert_array_equal(a.view(np.uint64), b.view(np.uint64))
+    g, gf, gw, _ = S.uneven(rs, sdf, to_dev=to_dev, frames=4)
+    h, hf, hw, _ = S.uneven(rs, sdf, to_dev=to_dev, frames=4, tweak=grid)
+    for x, y in ((g, h), (gf, hf)):
+        np.testing.assert_array_equal(x.view(np.uint64), y.view(np.uint64))
+    np.testing.assert_allclose(gw, hw, rtol=1e-5, atol=1e-6)  # float atomics: summation order
