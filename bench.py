@@ -871,9 +871,11 @@ def run_config5(args):
     forced): every frame starts from the target state, the loss is the predicted frame-end
     positions' mean squared distance to the target (mm^2) summed over the frames, and each frame
     is differentiated on its own (a frame whose gradient overflows FP32 is left out and counted).
-    One step = --frames such frames forward (with tapes) and backward, then one Adam step on
-    per-rope log EA / log EI. Reported: fitting steps/s, forward + backward vertex-substeps/s, the
-    forward-only rollout, and with --fit-steps N the parameter errors after N steps."""
+    One step = the frames of --fit-window (default: all --frames) forward (with tapes) and
+    backward, then one Adam step (--lr) on per-rope log EA / log EI, each frame's gradient clipped
+    to --clip (norm over both parameter vectors; 0 = no clipping). Reported: fitting steps/s,
+    forward + backward vertex-substeps/s, the forward-only rollout, and with --fit-steps N the
+    parameter errors after N steps (with the loss and errors of every step)."""
     import torch
 
     import ropesim
@@ -913,7 +915,7 @@ def run_config5(args):
     rng = np.random.default_rng(6)
     log_ea = torch.tensor(np.log(ea_true) + rng.normal(0, 0.3, R), device="cuda", dtype=torch.float32, requires_grad=True)
     log_ei = torch.tensor(np.log(ei_true) + rng.normal(0, 0.3, R), device="cuda", dtype=torch.float32, requires_grad=True)
-    opt = torch.optim.Adam([log_ea, log_ei], lr=0.05, eps=1e-12)
+    opt = torch.optim.Adam([log_ea, log_ei], lr=args.lr, eps=1e-12)
 
     def errors():
         with torch.no_grad():
@@ -921,17 +923,23 @@ def run_config5(args):
             e_ei = (log_ei.exp() / true_ei).log().abs().median()
         return float(e_ea), float(e_ei)
 
-    info = {"dropped_frames": 0}
+    info = {"dropped_frames": 0, "clipped_frames": 0, "history": []}
+    f0, f1 = (int(x) for x in args.fit_window.split(":")) if args.fit_window else (0, F)
+    fit_frames = range(max(0, f0), min(F, f1))
 
     def fit_step():
         g_ea, g_ei = torch.zeros_like(log_ea), torch.zeros_like(log_ei)
         total = 0.0
-        for f in range(F):
+        for f in fit_frames:
             par = (per_vertex(log_ea.exp()), per_vertex(log_ei.exp()), mass)
             out = rg.frame(b, traj[f], par, None, None, None, DT, S5)
             loss = ((out[0] - traj[f + 1][0]) ** 2).sum(-1).mean() * 1e6  # mm^2
             ga, gi = torch.autograd.grad(loss, (log_ea, log_ei))
             if bool(torch.isfinite(ga).all() and torch.isfinite(gi).all()):
+                gn = float(torch.sqrt((ga * ga).sum() + (gi * gi).sum()))
+                if args.clip > 0 and gn > args.clip:
+                    ga, gi = ga * (args.clip / gn), gi * (args.clip / gn)
+                    info["clipped_frames"] += 1
                 g_ea += ga
                 g_ei += gi
             else:
@@ -940,6 +948,7 @@ def run_config5(args):
         log_ea.grad, log_ei.grad = g_ea, g_ei
         info["loss"] = total
         opt.step()
+        info["history"].append([round(total, 6), *[round(e, 5) for e in errors()]])
 
     def fwd_only():
         b.set_state(*st0)
@@ -969,8 +978,10 @@ def run_config5(args):
         fit["steps_done"] = args.fit_steps
     err1 = errors()
     fit.update({"objective": "one-step-ahead (teacher forced) frame-end positions, mm^2 summed over frames",
+                "window": [fit_frames.start, fit_frames.stop], "lr": args.lr, "clip": args.clip,
                 "loss_first_step": loss_first, "loss_last_step": info["loss"],
-                "frames_dropped_for_overflow": info["dropped_frames"],
+                "frames_dropped_for_overflow": info["dropped_frames"], "frames_clipped": info["clipped_frames"],
+                "history_loss_err_ea_err_ei": info["history"],
                 "median_abs_log_error_ea": [err0[0], err1[0]], "median_abs_log_error_ei": [err0[1], err1[1]]})
     timed(fwd_only, 1)
     msf = timed(fwd_only, max(1, min(args.steps, 3)))
@@ -1210,6 +1221,9 @@ def main():
                     help="config4: keep only the substep tapes (the backward recomputes the iterates)")
     ap.add_argument("--fit-steps", type=int, default=0, help="config5: total fitting steps to run (e.g. 50)")
     ap.add_argument("--iters", type=int, default=0, help="config5: Jacobi sweeps per substep (0 = the default 8)")
+    ap.add_argument("--fit-window", default="", help="config5: frames a:b the fit's loss uses (default all)")
+    ap.add_argument("--clip", type=float, default=0.0, help="config5: clip each frame's gradient norm to this (0 = off)")
+    ap.add_argument("--lr", type=float, default=0.05, help="config5: Adam learning rate on log EA / log EI")
     ap.add_argument("--bake-subdiv", type=int, default=5, help="bake: icosphere subdivisions of the baked mesh")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -228,6 +228,23 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
     uint64_t cand = all_meshes(nsdf);  // the first substep of a frame visits every mesh
     f3 facc = zero3();
 
+    // Without rope contact a lane's Hessian without contact terms is the same diagonal matrix
+    // (m / h^2 + k_i / l_i + k_{i-1} / l_{i-1}) I at every iteration of the frame: its diagonal and
+    // the solve's scale accel / H.xx are formed once, in the order position_terms and the
+    // exchange form them (inertia, own stretch share, the previous segment's share), so lanes
+    // without contact step with the same bits and the sweep builds no Hessian.
+    float dd_prev = 0.f, solve_scale = 0.f;
+    if constexpr (!ROPE) {
+        const float dd_own = hasNext ? ((c.ks * c.invl) * c.invl) * (1.f + damp) : 0.f;
+        sm.fc[t] = dd_own;
+        __syncthreads();
+        dd_prev = hasPrev ? sm.fc[t - 1] : 0.f;
+        float hxx = c.Hd;
+        if (hasNext) hxx += dd_own;
+        if (hasPrev) hxx += dd_prev;
+        solve_scale = a.accel / hxx;
+    }
+
     int cur = 0;
     if (act) sm.q[0][t] = q;
 
@@ -308,10 +325,10 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                                                btab, mytbox);
             }
             if constexpr (ROPE) collision_sectors(a, ncol, dv, sm.p, sm.dx, damp, p, p1, dx, p1dx, f, f2, H, H2, bin.vcount);
-            // Without rope contact the segment's share H2 is its stretch term alone, dd I
-            // (position_terms), so one float4 carries the whole exchange.
+            // Without rope contact the segment's share H2 is its stretch term alone, dd I, the same
+            // at every iteration (dd_prev above), so only the force share is exchanged.
             if (act) {
-                sm.fa[t] = f4(f2, H2.xx);
+                sm.fa[t] = f4(f2, ROPE ? H2.xx : 0.f);
                 if constexpr (ROPE) {
                     sm.fb[t] = make_float4(H2.yy, H2.zz, H2.xy, H2.xz);
                     sm.fc[t] = H2.yz;
@@ -324,35 +341,28 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                 if constexpr (ROPE) {
                     const float4 fb = sm.fb[t - 1];
                     H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
-                } else {
-                    H.xx += fa.w; H.yy += fa.w; H.zz += fa.w;
                 }
             }
-            // every thread of the CTA runs the sweep, so the votes below have the full warp; a warp
-            // with no surface contact skips the 3x3 solve (each lane's result is the same either way)
-            if constexpr (ROPE) position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
-            else if constexpr (SURF == SURF_NONE) position_solve(dx, f, H, a.accel, im, true);
-            else if constexpr (kRedo) {
-                if (__any_sync(0xffffffffu, touched)) {
-                    if (touched) {
-                        f3 g2;
-                        sym3 G2;
-                        touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H,
-                                                       g2, G2, btab, mytbox);
-                        if (hasPrev) {
-                            const float4 fa = sm.fa[t - 1];
-                            f += xyz(fa);
-                            H.xx += fa.w; H.yy += fa.w; H.zz += fa.w;
-                        }
+            // lanes flagged by the slack redo their terms with contact and take the adjugate solve;
+            // the others (and flagged lanes that found no contact) take the frame's diagonal scale
+            if constexpr (ROPE) {
+                position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
+            } else if constexpr (SURF == SURF_NONE) {
+                if (im != 0.f) dx += f * solve_scale;
+            } else {
+                if (touched) {
+                    f3 g2;
+                    sym3 G2;
+                    touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, g2,
+                                                   G2, btab, mytbox);
+                    if (hasPrev) {
+                        f += xyz(sm.fa[t - 1]);
+                        H.xx += dd_prev; H.yy += dd_prev; H.zz += dd_prev;
                     }
                     position_solve(dx, f, H, a.accel, im, !touched);
-                } else {
-                    position_solve(dx, f, H, a.accel, im, true);
+                } else if (im != 0.f) {
+                    dx += f * solve_scale;
                 }
-            } else if (__any_sync(0xffffffffu, touched)) {
-                position_solve(dx, f, H, a.accel, im, !touched);
-            } else {
-                position_solve(dx, f, H, a.accel, im, true);
             }
             if (act) sm.dx[t] = f4(dx, 0.f);
             if constexpr (!ROPE)
