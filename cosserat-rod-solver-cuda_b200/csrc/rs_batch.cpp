@@ -1150,7 +1150,7 @@ void Batch::set_mesh_friction(int index, float mu_s, float mu_k) {
 }
 
 void Batch::set_mesh_targets(int index, const float* pos, const float* quat, int rows, const uint8_t* tele, bool tele_all,
-                             bool on_device) {
+                             bool on_device, bool tele_on_host) {
     const int M = (int)grids_.size();
     if (index >= M || (index < 0 && M == 0)) throw std::invalid_argument("mesh index out of range");
     ensure_device();
@@ -1172,6 +1172,11 @@ void Batch::set_mesh_targets(int index, const float* pos, const float* quat, int
         }
         // pageable sources: wait so the caller's arrays may die after the call
         check(cudaStreamSynchronize(stream_), "stage targets");
+    } else if (tele_on_host && tele && !tele_all) {
+        // device poses with host teleport flags: stage the flags
+        check(cudaMemcpyAsync(d_stage_tele_, tele, R_, cudaMemcpyHostToDevice, stream_), "upload(teleport flags)");
+        check(cudaStreamSynchronize(stream_), "stage teleport flags");
+        dt = d_stage_tele_;
     }
     check(launch_scatter_targets(d_tgt_, d_tele_, index, dp, dq, rows, M, tele_all ? nullptr : dt, tele_all ? 1 : 0, R_,
                                  stream_),

@@ -154,7 +154,7 @@ public:
     void set_mesh_friction(int index, float mu_s, float mu_k);
     // Targets of mesh `index` (rows 1 or R) or of every mesh (index -1, [R, M] rows).
     void set_mesh_targets(int index, const float* pos, const float* quat, int rows, const uint8_t* tele, bool tele_all,
-                          bool on_device);
+                          bool on_device, bool tele_on_host = false);
     void clear_meshes();
     void enable_forces(bool on);
     bool forces_enabled() const { return forces_on_; }

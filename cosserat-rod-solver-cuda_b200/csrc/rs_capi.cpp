@@ -545,7 +545,7 @@ int rs_batch_set_mesh_poses(rs_batch* b, int index, const float* pos, const floa
         rs::Batch& s = B(b);
         need(pos && quat, "null argument");
         std::lock_guard<std::mutex> g(s.mutex());
-        s.set_mesh_targets(index, pos, quat, rows, tele, tele_all != 0, on_device != 0);
+        s.set_mesh_targets(index, pos, quat, rows, tele, tele_all != 0, (on_device & 1) != 0, (on_device & 2) != 0);
     });
 }
 int rs_batch_clear_meshes(rs_batch* b) {

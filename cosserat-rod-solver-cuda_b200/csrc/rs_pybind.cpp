@@ -820,9 +820,8 @@ PYBIND11_MODULE(RS_MODULE_NAME, m) {
                      const uintptr_t p = parse_cai(pos, {b.R, 3}, "pos"), q = parse_cai(quat, {b.R, 4}, "quat");
                      if (t.device) {
                          ok(rs_batch_set_mesh_poses(b.h, index, (const float*)p, (const float*)q, b.R, t.ptr, 0, 1));
-                     } else if (!t.all && t.ptr) {
-                         // host flags with device poses: stage the flags through a device copy of the rows
-                         throw py::value_error("set_mesh_poses: CUDA poses need teleport as a bool or a CUDA bool array");
+                     } else if (!t.all && t.ptr) {  // host flags with device poses: the library stages them
+                         ok(rs_batch_set_mesh_poses(b.h, index, (const float*)p, (const float*)q, b.R, t.ptr, 0, 3));
                      } else {
                          ok(rs_batch_set_mesh_poses(b.h, index, (const float*)p, (const float*)q, b.R, nullptr, t.all ? 1 : 0, 1));
                      }
@@ -843,10 +842,9 @@ PYBIND11_MODULE(RS_MODULE_NAME, m) {
                  if (dp != dq) throw py::value_error("set_mesh_poses_all: pos and quat must both be host arrays or both CUDA arrays");
                  if (dp) {
                      const uintptr_t p = parse_cai(pos, {N, M, 3}, "pos"), q = parse_cai(quat, {N, M, 4}, "quat");
-                     if (!t.device && !t.all && t.ptr)
-                         throw py::value_error("set_mesh_poses_all: CUDA poses need teleport as a bool or a CUDA bool array");
-                     ok(rs_batch_set_mesh_poses(b.h, -1, (const float*)p, (const float*)q, N * M, t.device ? t.ptr : nullptr,
-                                                t.all ? 1 : 0, 1));
+                     const bool host_flags = !t.device && !t.all && t.ptr;  // staged by the library
+                     ok(rs_batch_set_mesh_poses(b.h, -1, (const float*)p, (const float*)q, N * M, t.all ? nullptr : t.ptr,
+                                                t.all ? 1 : 0, host_flags ? 3 : 1));
                      return;
                  }
                  if (t.device) throw py::value_error("set_mesh_poses_all: host poses need teleport as a bool or a host bool array");

@@ -209,7 +209,8 @@ RS_API int rs_batch_add_mesh(rs_batch* b, const float* values, int nx, int ny, i
 RS_API int rs_batch_set_mesh_friction(rs_batch* b, int index, float mu_s, float mu_k);
 /* SdfStore::set_targets / set_targets_host (sdf.cu:165-189): index >= 0 with rows 1 or
  * num_ropes, or index = -1 with [num_ropes, M] rows; tele [num_ropes] or NULL; tele_all;
- * on_device = 1 when pos/quat/tele are device memory. */
+ * on_device = 1 when pos/quat/tele are device memory, 3 when pos/quat are device memory and tele
+ * is host memory (staged, as the reference stages host flags given with CUDA poses). */
 RS_API int rs_batch_set_mesh_poses(rs_batch* b, int index, const float* pos, const float* quat, int rows,
                             const uint8_t* tele, int tele_all, int on_device);
 RS_API int rs_batch_clear_meshes(rs_batch* b);

@@ -284,9 +284,14 @@ def bench_c3_build(mod, scene, sel=None, **kw):
         ropes = [ropes[r] for r in sel]
         ea_v, ei_v, m_v = ea_v[idx], ei_v[idx], m_v[idx]
     b = mod.RopeBatch.from_ropes(ropes, 0.117, 1000.0, 1e-3, BENCH_H, BENCH_ITERS, **kw)
-    b.set_stretch_stiffnesses(ea_v)
-    b.set_bend_stiffnesses(ei_v)
-    b.set_masses(m_v)
+    lens = {len(r) for r in ropes}
+    if len(lens) == 1:  # ropes of one length make a uniform batch: per-segment [N, V-1], per-vertex [N, V]
+        Vr = lens.pop()
+        ea_v, ei_v, m_v = (x.reshape(-1, Vr) for x in (ea_v, ei_v, m_v))
+        ea_v, ei_v = ea_v[:, :-1], ei_v[:, :-1]
+    b.set_stretch_stiffnesses(np.ascontiguousarray(ea_v))
+    b.set_bend_stiffnesses(np.ascontiguousarray(ei_v))
+    b.set_masses(np.ascontiguousarray(m_v))
     b.set_gravity(np.array([0, 0, -G], np.float32))
     b.damping = 0.0
     b.drag = 0.2
