@@ -2,7 +2,8 @@
 
 1. libropesim_b200.so: the sm_100a kernels, the C++ driver and the extern "C" boundary
    (include/ropesim_b200.h), compiled by nvcc for `-gencode arch=compute_100a,code=sm_100a`
-   only, IEEE division / square root (no fast math), static CUDA runtime.
+   only, IEEE division / square root (no fast math), no compiler FMA contraction (the fused
+   multiply-adds are written out in the sources), static CUDA runtime.
 2. ropesim/_ropesim*.so: the pybind11 module (RopeSim, RopeBatch, CudaView) linked against (1)
    with an $ORIGIN rpath, so the package directory is self-contained.
 3. The checked build: the same sources with -DROPESIM_CHECKED (every kernel index the topology
@@ -73,7 +74,9 @@ def _build_one(checked: bool, force: bool, verbose: bool) -> str:
         o = os.path.join(objdir, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            extra = ARCH + ["-lineinfo", "-Xptxas", "-v"] if src.endswith(".cu") else ARCH
+            # -fmad=false: the sources spell out every fused multiply-add (fmaf), so each kernel
+            # instantiation rounds identically whatever its block size or surface variant
+            extra = ARCH + ["-lineinfo", "-fmad=false", "-Xptxas", "-v"] if src.endswith(".cu") else ARCH
             cmd = [nvcc] + common + extra + ["-c", s, "-o", o]
             if src.endswith(".cu") and not verbose:
                 cmd.remove("-Xptxas"); cmd.remove("-v")

@@ -3,6 +3,12 @@
 //
 // Every function keeps the operation order of the reference routine it cites so that a
 // single-precision run tracks the reference within rounding (IEEE div/sqrt, no fast math).
+//
+// The engine is compiled with -fmad=false: the compiler fuses nothing, and every fused
+// multiply-add is written out here (fmaf, one rounding). A sum of products is evaluated as
+// an fmaf chain from its first term, e.g. dot = fma(z, z', fma(y, y', x x')). Every kernel
+// instantiation (block size, surface variant) therefore does the same arithmetic, and a rope's
+// result does not depend on the launch configuration that stepped it.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,43 +38,47 @@ __device__ __forceinline__ f3 operator/(f3 a, float s) { return f3{a.x / s, a.y 
 __device__ __forceinline__ f3& operator+=(f3& a, f3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
 __device__ __forceinline__ f3& operator-=(f3& a, f3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; return a; }
 __device__ __forceinline__ f3& operator*=(f3& a, float s) { a.x *= s; a.y *= s; a.z *= s; return a; }
-__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)); }
+// a * s + b, fused per component
+__device__ __forceinline__ f3 fma3(f3 a, float s, f3 b) { return f3{fmaf(a.x, s, b.x), fmaf(a.y, s, b.y), fmaf(a.z, s, b.z)}; }
 __device__ __forceinline__ f3 cross(f3 a, f3 b) {
-    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return f3{fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x))};
 }
 __device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
-__device__ __forceinline__ f3 lerp3(f3 a, f3 b, float t) { return a * (1.f - t) + b * t; }
+__device__ __forceinline__ f3 lerp3(f3 a, f3 b, float t) { return fma3(b, t, a * (1.f - t)); }
 __device__ __forceinline__ f3 xyz(float4 v) { return f3{v.x, v.y, v.z}; }
 __device__ __forceinline__ float4 f4(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 
 // Rotor (x, y, z = bivector part, w = scalar) products, Rotor.h:96-105 and :185-188.
 __device__ __forceinline__ float4 qmul(float4 a, float4 b) {
     const f3 av = xyz(a), bv = xyz(b);
-    const f3 v = bv * a.w + av * b.w + cross(av, bv);
-    return make_float4(v.x, v.y, v.z, a.w * b.w - dot(av, bv));
+    const f3 v = fma3(av, b.w, fma3(bv, a.w, cross(av, bv)));
+    return make_float4(v.x, v.y, v.z, fmaf(a.w, b.w, -dot(av, bv)));
 }
 __device__ __forceinline__ float4 qconj(float4 a) { return make_float4(-a.x, -a.y, -a.z, a.w); }
-__device__ __forceinline__ float dot4(float4 a, float4 b) { return (a.x * b.x + a.y * b.y) + (a.z * b.z + a.w * b.w); }
+__device__ __forceinline__ float dot4(float4 a, float4 b) {
+    return fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)));
+}
 __device__ __forceinline__ float4 scale4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
 __device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float4 normalize4(float4 a) { return scale4(a, 1.f / sqrtf(dot4(a, a))); }
 __device__ __forceinline__ f3 qrot(float4 q, f3 v) {
     const f3 qv = xyz(q);
-    const f3 a = v * q.w + cross(qv, v);
+    const f3 a = fma3(v, q.w, cross(qv, v));
     const float c = dot(v, qv);
-    return a * q.w + cross(qv, a) + qv * c;
+    return fma3(qv, c, fma3(a, q.w, cross(qv, a)));
 }
 // q * e1, the tangent of the segment frame: qrot(q, e1) with the zero terms of e1 dropped
 // (a = (w, z, -y), c = x; exact, as multiplying by 1 and adding 0 are).
 __device__ __forceinline__ f3 qtangent(float4 q) {
     const f3 qv = xyz(q);
     const f3 a = mk3(q.w, q.z, -q.y);
-    return a * q.w + cross(qv, a) + qv * q.x;
+    return fma3(qv, q.x, fma3(a, q.w, cross(qv, a)));
 }
 // (v, 0) * b for a pure vector v: the rotor product with the zero scalar's terms dropped.
 __device__ __forceinline__ float4 qmul_pure(f3 v, float4 b) {
     const f3 bv = xyz(b);
-    const f3 r = v * b.w + cross(v, bv);
+    const f3 r = fma3(v, b.w, cross(v, bv));
     return make_float4(r.x, r.y, r.z, -dot(v, bv));
 }
 // c * (1, 0, 0, 0): a signed permutation of c's components.
@@ -84,21 +94,22 @@ __device__ __forceinline__ void sym_add(sym3& a, const sym3& b) {
     a.xx += b.xx; a.yy += b.yy; a.zz += b.zz; a.xy += b.xy; a.xz += b.xz; a.yz += b.yz;
 }
 __device__ __forceinline__ void sym_add_scaled_outer(sym3& a, f3 n, float s) {  // a += (n n^T) * s
-    a.xx += (n.x * n.x) * s; a.yy += (n.y * n.y) * s; a.zz += (n.z * n.z) * s;
-    a.xy += (n.x * n.y) * s; a.xz += (n.x * n.z) * s; a.yz += (n.y * n.z) * s;
+    a.xx = fmaf(n.x * n.x, s, a.xx); a.yy = fmaf(n.y * n.y, s, a.yy); a.zz = fmaf(n.z * n.z, s, a.zz);
+    a.xy = fmaf(n.x * n.y, s, a.xy); a.xz = fmaf(n.x * n.z, s, a.xz); a.yz = fmaf(n.y * n.z, s, a.yz);
 }
 // a -= (n n^T - I) * s
 __device__ __forceinline__ void sym_sub_scaled_outer_minus_I(sym3& a, f3 n, float s) {
-    a.xx -= (n.x * n.x - 1.f) * s; a.yy -= (n.y * n.y - 1.f) * s; a.zz -= (n.z * n.z - 1.f) * s;
-    a.xy -= (n.x * n.y) * s; a.xz -= (n.x * n.z) * s; a.yz -= (n.y * n.z) * s;
+    a.xx = fmaf(-fmaf(n.x, n.x, -1.f), s, a.xx); a.yy = fmaf(-fmaf(n.y, n.y, -1.f), s, a.yy);
+    a.zz = fmaf(-fmaf(n.z, n.z, -1.f), s, a.zz);
+    a.xy = fmaf(-(n.x * n.y), s, a.xy); a.xz = fmaf(-(n.x * n.z), s, a.xz); a.yz = fmaf(-(n.y * n.z), s, a.yz);
 }
 // x = H^-1 f through the adjugate of the symmetric matrix (cofactor expansion).
 __device__ __forceinline__ f3 sym_solve(const sym3& H, f3 f) {
-    const float c00 = H.yy * H.zz - H.yz * H.yz, c01 = H.xz * H.yz - H.xy * H.zz, c02 = H.xy * H.yz - H.xz * H.yy;
-    const float c11 = H.xx * H.zz - H.xz * H.xz, c12 = H.xy * H.xz - H.xx * H.yz, c22 = H.xx * H.yy - H.xy * H.xy;
-    const float idet = 1.f / (H.xx * c00 + H.xy * c01 + H.xz * c02);
-    return f3{(c00 * f.x + c01 * f.y + c02 * f.z) * idet, (c01 * f.x + c11 * f.y + c12 * f.z) * idet,
-              (c02 * f.x + c12 * f.y + c22 * f.z) * idet};
+    const float c00 = fmaf(H.yy, H.zz, -(H.yz * H.yz)), c01 = fmaf(H.xz, H.yz, -(H.xy * H.zz));
+    const float c02 = fmaf(H.xy, H.yz, -(H.xz * H.yy)), c11 = fmaf(H.xx, H.zz, -(H.xz * H.xz));
+    const float c12 = fmaf(H.xy, H.xz, -(H.xx * H.yz)), c22 = fmaf(H.xx, H.yy, -(H.xy * H.xy));
+    const float idet = 1.f / dot(mk3(H.xx, H.xy, H.xz), mk3(c00, c01, c02));
+    return f3{dot(mk3(c00, c01, c02), f) * idet, dot(mk3(c01, c11, c12), f) * idet, dot(mk3(c02, c12, c22), f) * idet};
 }
 
 // Closest points of segments a0a1 / b0b1 as (u, v), Common.h:327-345.
@@ -118,18 +129,18 @@ __device__ __forceinline__ void seg_closest(f3 a0, f3 a1, f3 b0, f3 b1, float& u
 __device__ __forceinline__ void surface_contact(f3 n, float gap, f3 d, float k, float h, float muS, float muK,
                                                 float vslip, f3& f, sym3& H) {
     const float N = -k * gap;
-    f += n * N;
+    f = fma3(n, N, f);
     sym_add_scaled_outer(H, n, k);
-    const f3 ut = d - n * dot(n, d);
+    const f3 ut = fma3(n, -dot(n, d), d);
     const float ul = len(ut);
     const float vt = ul / h;
     float kt;
     if (vt <= vslip) kt = muS * N / (vslip * h);
     else {
         const float s = 1.f - fminf(1.f, vt / vslip - 1.f);
-        kt = (s * muS + (1.f - s) * muK) * N / ul;
+        kt = fmaf(s, muS, (1.f - s) * muK) * N / ul;
     }
-    f -= ut * kt;
+    f = fma3(ut, -kt, f);
     sym_sub_scaled_outer_minus_I(H, n, kt);
 }
 
@@ -145,19 +156,19 @@ __device__ __forceinline__ bool sdf_sample(const rs::GridDesc& g, f3 p, float& p
         check_fail(g.status, rs::CHK_LATTICE);
         return false;
     }
-    const f3 fr = (p - (o + mk3(float(i), float(j), float(k)) * g.h)) * g.invH;
+    const f3 fr = (p - fma3(mk3(float(i), float(j), float(k)), g.h, o)) * g.invH;
     const float fx = fminf(fmaxf(fr.x, 0.f), 1.f), fy = fminf(fmaxf(fr.y, 0.f), 1.f), fz = fminf(fmaxf(fr.z, 0.f), 1.f);
     const int sy = g.nz, sx = g.ny * g.nz;
     const float* c = g.v + (size_t)i * sx + (size_t)j * sy + k;
     const float c000 = __ldg(c), c001 = __ldg(c + 1), c010 = __ldg(c + sy), c011 = __ldg(c + sy + 1);
     const float c100 = __ldg(c + sx), c101 = __ldg(c + sx + 1), c110 = __ldg(c + sx + sy), c111 = __ldg(c + sx + sy + 1);
     const float dx00 = c100 - c000, dx01 = c101 - c001, dx10 = c110 - c010, dx11 = c111 - c011;
-    const float c00 = c000 + fx * dx00, c01 = c001 + fx * dx01, c10 = c010 + fx * dx10, c11 = c011 + fx * dx11;
+    const float c00 = fmaf(fx, dx00, c000), c01 = fmaf(fx, dx01, c001), c10 = fmaf(fx, dx10, c010), c11 = fmaf(fx, dx11, c011);
     const float dy0 = c10 - c00, dy1 = c11 - c01;
-    const float c0 = c00 + fy * dy0, c1 = c01 + fy * dy1;
-    phi = c0 + fz * (c1 - c0);
-    const float gx0 = dx00 + fy * (dx10 - dx00), gx1 = dx01 + fy * (dx11 - dx01);
-    grad = mk3(gx0 + fz * (gx1 - gx0), dy0 + fz * (dy1 - dy0), c1 - c0) * g.invH;
+    const float c0 = fmaf(fy, dy0, c00), c1 = fmaf(fy, dy1, c01);
+    phi = fmaf(fz, c1 - c0, c0);
+    const float gx0 = fmaf(fy, dx10 - dx00, dx00), gx1 = fmaf(fy, dx11 - dx01, dx01);
+    grad = mk3(fmaf(fz, gx1 - gx0, gx0), fmaf(fz, dy1 - dy0, dy0), c1 - c0) * g.invH;
     return true;
 }
 
@@ -250,7 +261,7 @@ __device__ __forceinline__ bool sdf_contact_at(const rs::GridDesc& g, const Pose
     if (!(gl > 0.f)) return false;
     n = qrot(P.q, gr / gl);
     dRel = d;
-    if (moving) dRel -= (P.vel + cross(P.om, pos - P.pos)) * h;
+    if (moving) dRel = fma3(P.vel + cross(P.om, pos - P.pos), -h, dRel);
     return true;
 }
 

@@ -348,20 +348,27 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             if constexpr (ROPE) {
                 position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
             } else if constexpr (SURF == SURF_NONE) {
-                if (im != 0.f) dx += f * solve_scale;
+                if (im != 0.f) dx = fma3(f, solve_scale, dx);
             } else {
                 if (touched) {
+                    // a flagged lane that finds no contact keeps the sweep's force, so the slack
+                    // test decides only how much work is done, never a bit of the result
+                    const f3 f0 = f;
                     f3 g2;
                     sym3 G2;
                     touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, g2,
                                                    G2, btab, mytbox);
-                    if (hasPrev) {
-                        f += xyz(sm.fa[t - 1]);
-                        H.xx += dd_prev; H.yy += dd_prev; H.zz += dd_prev;
+                    if (touched) {
+                        if (hasPrev) {
+                            f += xyz(sm.fa[t - 1]);
+                            H.xx += dd_prev; H.yy += dd_prev; H.zz += dd_prev;
+                        }
+                        position_solve(dx, f, H, a.accel, im, false);
+                    } else {
+                        dx = fma3(f0, solve_scale, dx);
                     }
-                    position_solve(dx, f, H, a.accel, im, !touched);
                 } else if (im != 0.f) {
-                    dx += f * solve_scale;
+                    dx = fma3(f, solve_scale, dx);
                 }
             }
             if (act) sm.dx[t] = f4(dx, 0.f);

@@ -239,11 +239,11 @@ __device__ __forceinline__ void contact_box(const GridDesc& g, f3 pos, float4 q,
 __device__ __forceinline__ void init_vertex(f3 vel0, f3 lv_old, float im, float h, float last_h, f3 g, float g2, f3& dx,
                                             f3& y) {
     dx = vel0 * h;
-    y = dx + g * (h * h);
+    y = fma3(g, h * h, dx);
     if (im != 0.f && g2 > 0.f) {
         const f3 acc = (vel0 - lv_old) / last_h;
         const float sg = fminf(fmaxf(dot(acc, g) / g2, 0.f), 1.f);
-        dx += g * (h * h * sg);
+        dx = fma3(g, h * h * sg, dx);
     }
 }
 
@@ -279,11 +279,11 @@ __device__ __forceinline__ bool position_terms(const FrameArgs& a, const float4*
     f2 = zero3();
     H2 = sym_zero();
     if (hasNext) {
-        const f3 cc = ((p1 - p) + (p1dx - dx)) * c.invl - qtangent(q);
+        const f3 cc = fma3((p1 - p) + (p1dx - dx), c.invl, -qtangent(q));
         const float k = c.ks * c.invl;
         float dd = k * c.invl;
-        f += cc * k - dx * (damp * dd);
-        f2 += cc * (-k) - p1dx * (damp * dd);
+        f = fma3(dx, -(damp * dd), fma3(cc, k, f));
+        f2 = fma3(p1dx, -(damp * dd), cc * (-k));
         dd *= 1.f + damp;
         H.xx += dd; H.yy += dd; H.zz += dd;
         H2.xx += dd; H2.yy += dd; H2.zz += dd;
@@ -315,18 +315,18 @@ __device__ __forceinline__ void collision_term(const FrameArgs& a, float damp, f
     const float logd = logf(dist);
     float dH = (-3.f + (2.f + invd) * invd - 2.f * logd) * kCol * invb;
     const float ff = -(1.f - dist) * (dist - 1.f + 2.f * dist * logd) * invd * kCol;
-    f += nrm * (ff * wa - damp * dH * wa * wa * dot(nrm, d));
-    f2 += nrm * (ff * wb - damp * dH * wb * wb * dot(nrm, p1d));
+    f = fma3(nrm, fmaf(ff, wa, -(damp * dH * wa * wa * dot(nrm, d))), f);
+    f2 = fma3(nrm, fmaf(ff, wb, -(damp * dH * wb * wb * dot(nrm, p1d))), f2);
     dH *= 1.f + damp;
     sym_add_scaled_outer(H, nrm, dH * wa * wa);
     sym_add_scaled_outer(H2, nrm, dH * wb * wb);
-    const f3 uu = ddpos - nrm * dot(nrm, ddpos);
+    const f3 uu = fma3(nrm, -dot(nrm, ddpos), ddpos);
     const float ul = len(uu);
     if (ul > 0.f) {
         const float f1 = fminf(a.rc_kfric, a.rc_mu * ff / ul);
-        f -= uu * (f1 * wa);
+        f = fma3(uu, -(f1 * wa), f);
         sym_sub_scaled_outer_minus_I(H, nrm, wa * wa * f1);
-        f2 -= uu * (f1 * wb);
+        f2 = fma3(uu, -(f1 * wb), f2);
         sym_sub_scaled_outer_minus_I(H2, nrm, wb * wb * f1);
     }
 }
@@ -354,14 +354,14 @@ __device__ __forceinline__ float step_limit_of(f3 a0, f3 a1, f3 pj0, f3 pj1) {
 // Local solve dx += accel * H^-1 f of a free vertex, cosserat.cu:206-209. Without contact
 // terms (`diag`) H is a multiple of the identity and the solve is one division.
 __device__ __forceinline__ void position_solve(f3& dx, f3 f, const sym3& H, float accel, float im, bool diag) {
-    if (im != 0.f) dx += diag ? f * (accel / H.xx) : sym_solve(H, f) * accel;
+    if (im != 0.f) dx = diag ? fma3(f, accel / H.xx, dx) : fma3(sym_solve(H, f), accel, dx);
 }
 // The same with the step limit of rope-rope contact, cosserat.cu:211-214. Returns the limit's
 // scale lim / |dx| (1 when the step is not limited).
 __device__ __forceinline__ float position_solve_limited(f3& dx, f3 f, const sym3& H, float accel, float im, float lim) {
     float sc = 1.f;
     if (im != 0.f) {
-        dx += sym_solve(H, f) * accel;
+        dx = fma3(sym_solve(H, f), accel, dx);
         const float l = len(dx);
         if (l > lim && l > 0.f) {
             sc = lim / l;
@@ -459,7 +459,8 @@ __device__ __forceinline__ float4 frame_update(float4 q, f3 seg, float invl, flo
     }
     const float lambda = len(vv) + sqrtf(dot4(b, b));
     const float4 m = qmul_e1(qmul_pure(vv, b));
-    return normalize4(add4(m, scale4(b, lambda)));
+    return normalize4(make_float4(fmaf(b.x, lambda, m.x), fmaf(b.y, lambda, m.y), fmaf(b.z, lambda, m.z),
+                                  fmaf(b.w, lambda, m.w)));
 }
 
 // New velocity of a free vertex: dx / h, quadratic drag split by the segment tangent `tg`
@@ -470,8 +471,8 @@ __device__ __forceinline__ f3 end_velocity(const FrameArgs& a, f3 dx, float invH
     if (kn > 0.f) {
         const f3 vt = tg * dot(tg, vv);
         f3 vn = vv - vt;
-        vn = vn / (1.f + kn * len(vn) * a.h);
-        const f3 vt2 = vt / (1.f + a.drag_quad_t * len(vt) * a.h);
+        vn = vn / fmaf(kn * len(vn), a.h, 1.f);
+        const f3 vt2 = vt / fmaf(a.drag_quad_t * len(vt), a.h, 1.f);
         vv = vn + vt2;
     }
     return vv * (1.f - a.drag * a.h);
