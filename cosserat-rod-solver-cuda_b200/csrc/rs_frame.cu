@@ -48,20 +48,20 @@ struct FrameSmem {
 // The host sizes the CTA's shared memory with 144 B of frame state per thread (rs_batch.cpp).
 static_assert(sizeof(FrameSmem<64>) == 144 * 64 && sizeof(FrameSmem<1024>) == 144 * 1024, "FrameSmem layout");
 
-// Resident CTAs per SM the register allocation targets:
+// Resident CTAs per SM the register allocation targets (measured on one B200):
 //  - 28 warps per SM (<= 72 registers; 24 warps for 256-thread CTAs) without surfaces, and with
 //    planes in 256-thread bins;
-//  - 20 warps per SM (<= 96 registers; 81 used, and registers are allocated per SM sub-partition) with
-//    planes only in bins of up to 128 threads, where a 72-register cap spills in the sweep and
-//    costs a frame of 4096 64-vertex ropes over one plane 2% (3.11 against 3.05 ms);
-//  - 24 warps per SM (<= 80 registers) with meshes, where the rarely taken lattice-sampling path
-//    spills a few values to L1 (176 B per thread) and the extra resident CTA hides the barrier
-//    waits of the vertices that do sample (8192 ropes of 16-256 vertices, 8 meshes: 34.3 -> 31.1 ms
-//    per frame);
+//  - 24 warps per SM (<= 80 registers) with planes only in bins of up to 128 threads: 4096 64-vertex
+//    ropes over one plane in 64-thread bins, 2.72 ms per frame against 2.83 ms at 20 warps (<= 96
+//    registers);
+//  - 16 warps per SM (<= 128 registers) with meshes: with fewer registers the inlined lattice path
+//    (taken by few lanes) makes the allocator spill values that every lane's Jacobi sweep reloads.
+//    8192 ropes of 16-256 vertices, 8 meshes: 24.7 ms per frame against 28.2 ms at 24 warps
+//    (<= 80 registers), and 17.0 against 20.5 ms with the meshes out of reach;
 //  - 16 warps per SM (<= 128 registers) with rope-rope contact.
 #ifndef RS_MIN_BLOCKS
 #define RS_MIN_BLOCKS(B, SURF, ROPE) \
-    ((B) <= 256 ? (((ROPE) ? 512 : (SURF) == SURF_MESHES ? 768 : ((SURF) == SURF_PLANES && (B) <= 128) ? 640 : 896) / (B)) : 1)
+    ((B) <= 256 ? (((ROPE) ? 512 : (SURF) == SURF_MESHES ? 512 : ((SURF) == SURF_PLANES && (B) <= 128) ? 768 : 896) / (B)) : 1)
 #endif
 
 // Mesh part of the contact readout (contact.cuh:172-204) for one warp: every lane calls it
