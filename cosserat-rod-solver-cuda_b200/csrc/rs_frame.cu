@@ -122,6 +122,53 @@ __device__ __forceinline__ void mesh_readout_warp(const FrameArgs& a, const floa
     }
 }
 
+// Poses of a bin's (rope, mesh) pairs at the end of substep s, eight lanes per pair. Every lane of
+// a pair computes the pair's kinematics (the same arithmetic on all eight) and one corner of the
+// lattice box and one of the contact box; the world AABBs are min/max-reduced over the eight lanes,
+// which is exact in any order. The cache and the contact boxes hold what compute_pose and
+// contact_box store, in an eighth of the serial latency (the rest of the CTA waits at the next
+// barrier meanwhile).
+template <int BLOCK>
+__device__ __forceinline__ void bin_poses(const FrameArgs& a, const Bin& bin, int nsdf, int nPose, int s, int S, float h,
+                                          float4* cache, float4* tbox) {
+    static_assert(BLOCK % 32 == 0, "pose groups of eight lanes stay within a warp");
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    for (int e8 = threadIdx.x; e8 < nPose * 8; e8 += BLOCK) {  // the eight lanes of a pair iterate together
+        const int e = e8 >> 3, c = e8 & 7;
+        const int r = e / nsdf, m = e % nsdf;
+        f3 Pp, Pv, Pw;
+        float4 Pq;
+        pose_kinematics(a, a.ropes[bin.rstart + r].user, m, s, S, h, Pp, Pq, Pv, Pw);
+        const GridDesc& gd = a.grids[m];
+        f3 lo_o, hi_o;
+        lattice_box(gd, lo_o, hi_o);
+        const f3 tl = mk3(gd.tlo[0], gd.tlo[1], gd.tlo[2]), th = mk3(gd.thi[0], gd.thi[1], gd.thi[2]);
+        const f3 w = qrot(Pq, mk3((c & 1) ? hi_o.x : lo_o.x, (c & 2) ? hi_o.y : lo_o.y, (c & 4) ? hi_o.z : lo_o.z)) + Pp;
+        const f3 u = qrot(Pq, mk3((c & 1) ? th.x : tl.x, (c & 2) ? th.y : tl.y, (c & 4) ? th.z : tl.z)) + Pp;
+        float lo[6] = {w.x, w.y, w.z, u.x, u.y, u.z}, hi[6] = {w.x, w.y, w.z, u.x, u.y, u.z};
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1)
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                lo[k] = fminf(lo[k], __shfl_xor_sync(gmask, lo[k], o));
+                hi[k] = fmaxf(hi[k], __shfl_xor_sync(gmask, hi[k], o));
+            }
+        if (c == 0) {
+            const f3 wl = mk3(lo[0], lo[1], lo[2]), wh = mk3(hi[0], hi[1], hi[2]);
+            float4* out = cache + e * kPoseF4;
+            store_pose(out, Pp, Pq, Pv, Pw, wl, wh);
+            out[4].w = travel_pad(a, Pv, Pw, wl, wh);
+            if (gd.never) {
+                tbox[2 * e] = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+                tbox[2 * e + 1] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            } else {
+                tbox[2 * e] = make_float4(lo[3], lo[4], lo[5], 0.f);
+                tbox[2 * e + 1] = make_float4(hi[3], hi[4], hi[5], 0.f);
+            }
+        }
+    }
+}
+
 // One bin of a frame: every substep of the bin's ropes, state in registers and shared memory.
 template <int BLOCK, int SURF, bool ROPE>
 __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
@@ -263,14 +310,8 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
         }
         float4* cache = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? cache1 : cache0) : cache0;
         float4* tbox = (SURF == SURF_MESHES && a.sdf_moving) ? ((s & 1) ? tbox1 : tbox0) : tbox0;
-        if constexpr (SURF == SURF_MESHES) if (nsdf > 0 && a.sdf_moving) {
-            for (int e = t; e < nPose; e += BLOCK) {
-                const int r = e / nsdf, m = e % nsdf;
-                compute_pose(a, a.ropes[bin.rstart + r].user, m, s, S, h, cache + e * kPoseF4);
-                const PoseV P = load_pose(cache + e * kPoseF4);
-                contact_box(a.grids[m], P.pos, P.q, tbox + 2 * e);
-            }
-        }
+        if constexpr (SURF == SURF_MESHES)
+            if (nsdf > 0 && a.sdf_moving) bin_poses<BLOCK>(a, bin, nsdf, nPose, s, S, h, cache, tbox);
         const float4* mycache = cache + lrope * nsdf * kPoseF4;
         const float4* mytbox = (SURF == SURF_MESHES && a.surf_cull) ? tbox + lrope * nsdf * 2 : nullptr;
 

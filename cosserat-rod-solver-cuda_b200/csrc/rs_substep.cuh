@@ -94,16 +94,15 @@ __device__ __forceinline__ void root_set(const FrameArgs& a, const float* row, f
     if (a.has_q0) q = unit_or_identity(row + 9);
 }
 
-// Pose of (env en, mesh m) at the end of substep s of S: constant linear and angular velocity
-// over the frame, world AABB of the lattice; 5 float4 at `out`.
-__device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, int s, int S, float h, float4* out) {
+// Kinematics of (env en, mesh m) at the end of substep s of S: constant linear and angular
+// velocity over the frame (position, rotor, velocity, angular velocity).
+__device__ __forceinline__ void pose_kinematics(const FrameArgs& a, int en, int m, int s, int S, float h, f3& Pp, float4& Pq,
+                                                f3& Pv, f3& Pw) {
     const Motion M = a.motion[(size_t)en * kMaxSdf + m];
     const float al = float(s + 1) / float(S);
     const float invDt = 1.f / (float(S) * h);
     const f3 p0 = mk3(M.p0x, M.p0y, M.p0z), dp = mk3(M.dpx, M.dpy, M.dpz), rot = mk3(M.rx, M.ry, M.rz);
     const float4 q0 = make_float4(M.qx, M.qy, M.qz, M.qw);
-    f3 Pp, Pv, Pw;
-    float4 Pq;
     const float th = len(rot);
     if (th > 0.f || dp.x != 0.f || dp.y != 0.f || dp.z != 0.f) {
         Pp = p0 + al * dp;
@@ -120,15 +119,31 @@ __device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, 
     } else {  // a target equal to the current pose: exactly the static pose
         Pp = p0; Pq = q0; Pv = zero3(); Pw = zero3();
     }
-    const GridDesc& gd = a.grids[m];
-    const f3 lo_o = mk3(gd.ox, gd.oy, gd.oz);
-    const f3 hi_o = lo_o + mk3(float(gd.nx - 1), float(gd.ny - 1), float(gd.nz - 1)) * gd.h;
-    f3 lo, hi;
+}
+
+// Lattice box [lo_o, hi_o] of grid gd in the object frame.
+__device__ __forceinline__ void lattice_box(const GridDesc& gd, f3& lo_o, f3& hi_o) {
+    lo_o = mk3(gd.ox, gd.oy, gd.oz);
+    hi_o = lo_o + mk3(float(gd.nx - 1), float(gd.ny - 1), float(gd.nz - 1)) * gd.h;
+}
+
+// The broad phase's padding for a mesh's own travel over one substep (contact.cuh:121-136),
+// once per pose instead of once per vertex; static poses keep 0.
+__device__ __forceinline__ float travel_pad(const FrameArgs& a, f3 Pv, f3 Pw, f3 lo, f3 hi) {
+    return a.sdf_moving ? a.h * (len(Pv) + len(Pw) * 0.5f * len(hi - lo)) : 0.f;
+}
+
+// Pose of (env en, mesh m) at the end of substep s of S with the world AABB of the lattice;
+// 5 float4 at `out`.
+__device__ __forceinline__ void compute_pose(const FrameArgs& a, int en, int m, int s, int S, float h, float4* out) {
+    f3 Pp, Pv, Pw;
+    float4 Pq;
+    pose_kinematics(a, en, m, s, S, h, Pp, Pq, Pv, Pw);
+    f3 lo_o, hi_o, lo, hi;
+    lattice_box(a.grids[m], lo_o, hi_o);
     world_box(lo_o, hi_o, Pp, Pq, lo, hi);
     store_pose(out, Pp, Pq, Pv, Pw, lo, hi);
-    // the broad phase's padding for the mesh's own travel over one substep (contact.cuh:121-136),
-    // once per pose instead of once per vertex; static poses keep 0 in this slot
-    out[4].w = a.sdf_moving ? a.h * (len(Pv) + len(Pw) * 0.5f * len(hi - lo)) : 0.f;
+    out[4].w = travel_pad(a, Pv, Pw, lo, hi);
 }
 
 // Surfaces (planes, then candidate meshes in ascending index) at one probe point,
