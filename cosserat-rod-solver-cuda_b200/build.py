@@ -2,8 +2,9 @@
 
 1. libropesim_b200.so: the sm_100a kernels, the C++ driver and the extern "C" boundary
    (include/ropesim_b200.h), compiled by nvcc for `-gencode arch=compute_100a,code=sm_100a`
-   only, IEEE division / square root (no fast math), no compiler FMA contraction (the fused
-   multiply-adds are written out in the sources), static CUDA runtime.
+   only, IEEE division / square root (no fast math; the frame step's rotor norms alone use
+   rsqrtf), no compiler FMA contraction (the fused multiply-adds are written out in the
+   sources), static CUDA runtime.
 2. ropesim/_ropesim*.so: the pybind11 module (RopeSim, RopeBatch, CudaView) linked against (1)
    with an $ORIGIN rpath, so the package directory is self-contained.
 3. The checked build: the same sources with -DROPESIM_CHECKED (every kernel index the topology

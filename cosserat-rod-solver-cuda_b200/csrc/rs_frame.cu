@@ -281,16 +281,18 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
     // exchange form them (inertia, own stretch share, the previous segment's share), so lanes
     // without contact step with the same bits and the sweep builds no Hessian.
     float dd_prev = 0.f, solve_scale = 0.f;
+    const float dd_own = (!ROPE && hasNext) ? ((c.ks * c.invl) * c.invl) * (1.f + damp) : 0.f;
+    if constexpr (!ROPE) sm.fc[t] = dd_own;
+    __syncthreads();  // the loaded rest rotations (and dd_own) are visible to the neighbours
     if constexpr (!ROPE) {
-        const float dd_own = hasNext ? ((c.ks * c.invl) * c.invl) * (1.f + damp) : 0.f;
-        sm.fc[t] = dd_own;
-        __syncthreads();
         dd_prev = hasPrev ? sm.fc[t - 1] : 0.f;
         float hxx = c.Hd;
         if (hasNext) hxx += dd_own;
         if (hasPrev) hxx += dd_prev;
         solve_scale = a.accel / hxx;
     }
+    // rest rotations of the own and the previous segment, constant over the frame
+    const float4 qr_own = sm.qr[t], qr_prev = sm.qr[hasPrev ? t - 1 : t];
 
     int cur = 0;
     if (act) sm.q[0][t] = q;
@@ -420,8 +422,8 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             // ---- frame step over the double-buffered rotors (no barrier needed before it)
             if (!(fl & F_FIX_ORIENT) && hasNext) {
                 const f3 seg = (p1 - p) + (xyz(sm.dx[t + 1]) - dx);
-                q = frame_update(q, seg, c.invl, ks, hasPrev, hasPrev ? sm.q[cur][t - 1] : q, hasPrev ? sm.qr[t - 1] : q,
-                                 (fl & F_NEXT_ORIENT) != 0, (fl & F_NEXT_ORIENT) ? sm.q[cur][t + 1] : q, sm.qr[t]);
+                q = frame_update(q, seg, c.invl, ks, hasPrev, sm.q[cur][hasPrev ? t - 1 : t], qr_prev,
+                                 (fl & F_NEXT_ORIENT) != 0, sm.q[cur][(fl & F_NEXT_ORIENT) ? t + 1 : t], qr_own);
             }
             if (act) sm.q[cur ^ 1][t] = q;
             if constexpr (!ROPE)
