@@ -319,15 +319,15 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                     sn = dot4(q0, nx) > 0.f ? 1.f : -1.f;
                     b = add4(b, scale4(nx, sn));
                 }
-                const float lvv = len(vv), lb = sqrtf(dot4(b, b)), lambda = lvv + lb;
-                const float4 z = add4(qmul_e1(qmul_pure(vv, b)), scale4(b, lambda));
-                const float izl = 1.f / sqrtf(dot4(z, z));
+                float ilvv, ilb, lambda;  // the forward's z (frame_z), so the reverse linearises what ran
+                const float4 z = frame_z(vv, b, ilvv, ilb, lambda);
+                const float izl = rsqrt_nr(dot4(z, z));
                 const float4 qo = scale4(z, izl);
                 const float4 zb = scale4(add4(qb, scale4(qo, -dot4(qo, qb))), izl);
                 float4 bb = scale4(zb, lambda);
                 const float lamb = dot4(zb, b);
-                f3 vvb = (lvv > 0.f) ? vv * (lamb / lvv) : zero3();
-                if (lb > 0.f) bb = add4(bb, scale4(b, lamb / lb));
+                f3 vvb = vv * (lamb * ilvv);
+                bb = add4(bb, scale4(b, lamb * ilb));
                 const float4 Ab = scale4(qmul_e1(zb), -1.f);   // z = A e1  ->  Ā = z̄ e1* = -(z̄ e1)
                 vvb += xyz(qmul(Ab, qconj(b)));
                 bb = add4(bb, scale4(qmul_pure(vv, Ab), -1.f)); // (vv, 0)* Ā = -(vv, 0) Ā

@@ -327,15 +327,15 @@ __global__ void padj_rev_frame_kernel(const FrameArgs* __restrict__ pa, PlainAdj
             sn = dot4(q0, nx) > 0.f ? 1.f : -1.f;
             bq = add4(bq, scale4(nx, sn));
         }
-        const float lvv = len(vv), lb = sqrtf(dot4(bq, bq)), lambda = lvv + lb;
-        const float4 z = add4(qmul_e1(qmul_pure(vv, bq)), scale4(bq, lambda));
-        const float izl = 1.f / sqrtf(dot4(z, z));
+        float ilvv, ilb, lambda;  // the forward's z (frame_z), so the reverse linearises what ran
+        const float4 z = frame_z(vv, bq, ilvv, ilb, lambda);
+        const float izl = rsqrt_nr(dot4(z, z));
         const float4 qo = scale4(z, izl);
         const float4 zb = scale4(add4(qb, scale4(qo, -dot4(qo, qb))), izl);
         float4 bb = scale4(zb, lambda);
         const float lamb = dot4(zb, bq);
-        f3 vvb = (lvv > 0.f) ? vv * (lamb / lvv) : zero3();
-        if (lb > 0.f) bb = add4(bb, scale4(bq, lamb / lb));
+        f3 vvb = vv * (lamb * ilvv);
+        bb = add4(bb, scale4(bq, lamb * ilb));
         const float4 Ab = scale4(qmul_e1(zb), -1.f);
         vvb += xyz(qmul(Ab, qconj(bq)));
         bb = add4(bb, scale4(qmul_pure(vv, Ab), -1.f));

@@ -358,7 +358,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             // ---- position step: own terms, exchange the segment's share, local solve
             f3 f, f2;
             sym3 H, H2;
-            const f3 p1dx = hasNext ? xyz(sm.dx[t + 1]) : zero3();
+            const f3 p1dx = xyz(sm.dx[hasNext ? t + 1 : t]);  // any finite value without a next vertex
             bool touched;
             if constexpr (kRedo) {
                 position_terms<SURF_NONE>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
@@ -378,20 +378,22 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                 }
             }
             __syncthreads();  // B1
-            if (hasPrev) {
+            if constexpr (!ROPE) {
+                const f3 fp = f + xyz(sm.fa[hasPrev ? t - 1 : t]);
+                f = hasPrev ? fp : f;
+            } else if (hasPrev) {
                 const float4 fa = sm.fa[t - 1];
                 f += xyz(fa);
-                if constexpr (ROPE) {
-                    const float4 fb = sm.fb[t - 1];
-                    H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
-                }
+                const float4 fb = sm.fb[t - 1];
+                H.xx += fa.w; H.yy += fb.x; H.zz += fb.y; H.xy += fb.z; H.xz += fb.w; H.yz += sm.fc[t - 1];
             }
             // lanes flagged by the slack redo their terms with contact and take the adjugate solve;
             // the others (and flagged lanes that found no contact) take the frame's diagonal scale
             if constexpr (ROPE) {
                 position_solve_limited(dx, f, H, a.accel, im, hasPrev ? fminf(lim, sm.lim[t - 1]) : lim);
             } else if constexpr (SURF == SURF_NONE) {
-                if (im != 0.f) dx = fma3(f, solve_scale, dx);
+                const f3 nd = fma3(f, solve_scale, dx);  // pinned vertices (im = 0) keep dx
+                dx = im != 0.f ? nd : dx;
             } else {
                 if (touched) {
                     // a flagged lane that finds no contact keeps the sweep's force, so the slack
@@ -410,8 +412,9 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                     } else {
                         dx = fma3(f0, solve_scale, dx);
                     }
-                } else if (im != 0.f) {
-                    dx = fma3(f, solve_scale, dx);
+                } else {
+                    const f3 nd = fma3(f, solve_scale, dx);
+                    dx = im != 0.f ? nd : dx;
                 }
             }
             if (act) sm.dx[t] = f4(dx, 0.f);

