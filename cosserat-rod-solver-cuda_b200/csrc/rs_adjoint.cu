@@ -131,6 +131,22 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
     }
     const float h = a.h, invH = 1.f / h;
     const float damp = a.damping / h;
+    // Without contact terms H is (m / h^2 + k_t / l_t + k_{t-1} / l_{t-1}) I at every iteration of the
+    // frame (the forward's hoisted diagonal): its reciprocal and the mass-weight scales are formed once,
+    // in the order the reverse position step builds H.
+    __syncthreads();  // the neighbours' KC
+    float ihxx = 0.f, wscale = 0.f, kscale = 0.f;
+    if (im != 0.f) {
+        float hxx = c.Hd;
+        if (hasNext) hxx += ks * c.invl * c.invl * (1.f + damp);
+        if (hasPrev) {
+            const float4 kp = KC[t - 1];
+            hxx += kp.x * kp.y * kp.y * (1.f + damp);
+        }
+        ihxx = 1.f / hxx;
+        wscale = -c.fm / im;
+        kscale = -c.kc / im;
+    }
     const f3 gv = mk3(a.gx, a.gy, a.gz);
     const float g2 = dot(gv, gv);
     const int S = a.substeps;
@@ -305,20 +321,15 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 const f3 u = ((p1 - p) + (xyz(Dn[t + 1]) - xyz(Dn[t]))) * c.invl;
                 const f3 vv = u * (-2.f * ks);
                 const float4 q0 = Lq[t];
-                float4 b = zero4(), qp = zero4(), qn = zero4(), rp = zero4(), rn = zero4();
-                float sp = 0.f, sn = 0.f;
-                if (hasPrev) {
-                    qp = Lq[t - 1]; rp = QR[t - 1];
-                    const float4 pr = qmul(qp, rp);
-                    sp = dot4(q0, pr) > 0.f ? 1.f : -1.f;
-                    b = scale4(pr, sp);
-                }
-                if (nextOrient) {
-                    qn = Lq[t + 1]; rn = QR[t];
-                    const float4 nx = qmul(qn, qconj(rn));
-                    sn = dot4(q0, nx) > 0.f ? 1.f : -1.f;
-                    b = add4(b, scale4(nx, sn));
-                }
+                // both neighbour products, the missing ones selected away (as the forward's frame_update)
+                const float4 qp = Lq[hasPrev ? t - 1 : t], rp = QR[hasPrev ? t - 1 : t];
+                const float4 qn = Lq[nextOrient ? t + 1 : t], rn = QR[t];
+                const float4 pr = qmul(qp, rp), nx = qmul(qn, qconj(rn));
+                const float spv = dot4(q0, pr) > 0.f ? 1.f : -1.f, snv = dot4(q0, nx) > 0.f ? 1.f : -1.f;
+                const float sp = hasPrev ? spv : 0.f, sn = nextOrient ? snv : 0.f;
+                float4 b = hasPrev ? scale4(pr, spv) : zero4();
+                const float4 bn = add4(b, scale4(nx, snv));
+                b = nextOrient ? bn : b;
                 float ilvv, ilb, lambda;  // the forward's z (frame_z), so the reverse linearises what ran
                 const float4 z = frame_z(vv, b, ilvv, ilb, lambda);
                 const float izl = rsqrt_nr(dot4(z, z));
@@ -335,14 +346,10 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 su = vvb * (-2.f * ks * c.invl);
                 // b = sp q_{t-1} r_{t-1} + sn q_{t+1} r_t^*: the rotor adjoints b̄ r^(*) also give the
                 // rest-rotor magnitude adjoints, <q^* b̄, r> = <b̄ r^*, q> and <(q^* b̄)^*, r> = <b̄ r, q>
-                if (hasPrev) {
-                    toL = qmul(scale4(bb, sp), qconj(rp));
-                    rhobp += dot4(toL, qp) * KC[t - 1].w;
-                }
-                if (nextOrient) {
-                    toR = qmul(scale4(bb, sn), rn);
-                    rhob += dot4(toR, qn) * irho;
-                }
+                toL = qmul(scale4(bb, sp), qconj(rp));  // zero without the neighbour (sp, sn = 0)
+                rhobp += dot4(toL, qp) * KC[hasPrev ? t - 1 : t].w;
+                toR = qmul(scale4(bb, sn), rn);
+                rhob += dot4(toR, qn) * irho;
             }
             EA[t] = toL;
             EB[t] = toR;
@@ -360,12 +367,14 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 HB1[t] = make_float4(HcB.xz, HcB.yz, 0.f, 0.f);
             }
             __syncthreads();
-            qb = own;
-            if (hasPrev) qb = add4(qb, EB[t - 1]);
-            if (hasNext) qb = add4(qb, EA[t + 1]);
             {
-                f3 dd = -su;
-                if (hasPrev) dd += xyz(EC[t - 1]);
+                const float4 ebp = EB[hasPrev ? t - 1 : t], ean = EA[hasNext ? t + 1 : t];
+                const float4 q1 = add4(own, ebp);
+                qb = hasPrev ? q1 : own;
+                const float4 q2 = add4(qb, ean);
+                qb = hasNext ? q2 : qb;
+                const f3 dp = -su + xyz(EC[hasPrev ? t - 1 : t]);
+                const f3 dd = hasPrev ? dp : -su;
                 db += dd;
                 xb += dd;
             }
@@ -387,14 +396,16 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                     f3 fdummy = zero3();
                     touched = surfaces<SURF>(a, mycache, cand, p, dk, c.kc, h, fdummy, H, nullptr, nullptr);
                 }
-                if (hasNext) {
-                    const float dd = ks * c.invl * c.invl * (1.f + damp);
-                    H.xx += dd; H.yy += dd; H.zz += dd;
-                }
-                if (hasPrev) {
-                    const float4 kp = KC[t - 1];
-                    const float dd = kp.x * kp.y * kp.y * (1.f + damp);
-                    H.xx += dd; H.yy += dd; H.zz += dd;
+                if (SURF != SURF_NONE || ROPE) {  // H beyond its diagonal only where contact can touch it
+                    if (hasNext) {
+                        const float dd = ks * c.invl * c.invl * (1.f + damp);
+                        H.xx += dd; H.yy += dd; H.zz += dd;
+                    }
+                    if (hasPrev) {
+                        const float4 kp = KC[t - 1];
+                        const float dd = kp.x * kp.y * kp.y * (1.f + damp);
+                        H.xx += dd; H.yy += dd; H.zz += dd;
+                    }
                 }
                 f3 gb = db;
                 f3 zk = xyz(Dn[t]);  // the solve's result before the step limit
@@ -419,13 +430,13 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                     }
                     dn = gb;
                 }
-                e = touched ? sym_solve(H, gb) : gb * (1.f / H.xx);
+                e = touched ? sym_solve(H, gb) : gb * ihxx;
                 del = zk - dk;
                 Fb = e * a.accel;
                 trH = -dot(e, del);
                 yb += Fb * c.fm;
                 dn -= Fb * c.fm;
-                float wsum = (dot(y - dk, Fb) + trH) * (-c.fm / im);
+                float wsum = (dot(y - dk, Fb) + trH) * wscale;
                 if constexpr (SURF != SURF_NONE) {
                     for (int pl = 0; pl < a.num_planes; pl++) {
                         const float4 P = a.planes[pl];
@@ -438,11 +449,11 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                                             kb, nb);
                         dn += nrm * gapb;
                         xb += nrm * gapb;
-                        wsum += kb * (-c.kc / im);
+                        wsum += kb * kscale;
                     }
                 }
                 if constexpr (SURF == SURF_MESHES)
-                    wsum += mesh_contact_bwd(a, mycache, cand, p, dk, c.kc, h, Fb, e, del, dn, xb) * (-c.kc / im);
+                    wsum += mesh_contact_bwd(a, mycache, cand, p, dk, c.kc, h, Fb, e, del, dn, xb) * kscale;
                 wb += wsum;
             }
             // segment t's residual c = ((x1 - x) + (d1 - d)) / l - t(q), read before the barrier:

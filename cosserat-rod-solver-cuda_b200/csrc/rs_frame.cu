@@ -198,7 +198,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
     float im = 0.f, lr = 1.f, ks = 0.f;
     float4 q = make_float4(0.f, 0.f, 0.f, 1.f);
     uint32_t fl = 0;
-    int lrope = 0, env = 0;
+    int lrope = 0, env = 0, uidx = 0;  // uidx: caller index (tape rows)
     if (act) {
         const float4 a0 = a.pos[dv], a1 = a.vel[dv], a2 = a.lvel[dv];
         const int4 tp = a.topo[dv];
@@ -208,7 +208,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
         sm.lv[t] = a2;
         q = a.q[dv];
         sm.qr[t] = a.qrest[dv];
-        fl = (uint32_t)tp.x; lrope = tp.y; env = tp.w;
+        fl = (uint32_t)tp.x; lrope = tp.y; env = tp.w; uidx = tp.z;
         if constexpr (kChecked)
             if (!checked_vertex(a, bin, t, tp.z, fl, lrope, env, SURF == SURF_MESHES ? a.num_sdf : 0)) act = false;
     }
@@ -304,7 +304,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
         }
         if (a.tape && act) {  // differentiable frames: this substep's start state, caller order
             // (streaming stores: read once, by the backward, after the frame)
-            float4* tp = a.tape + (size_t)s * 4 * a.n + a.topo[dv].z;
+            float4* tp = a.tape + (size_t)s * 4 * a.n + uidx;
             __stcs(tp, f4(p, __int_as_float((int)(uint32_t)cand)));  // broad-phase mask of this substep
             __stcs(tp + a.n, f4(v, __int_as_float((int)(uint32_t)(cand >> 32))));
             __stcs(tp + 2 * (size_t)a.n, sm.lv[t]);
@@ -419,7 +419,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             }
             if (act) sm.dx[t] = f4(dx, 0.f);
             if constexpr (!ROPE)
-                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + it) * a.n + a.topo[dv].z, f4(dx, 0.f));
+                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + it) * a.n + uidx, f4(dx, 0.f));
             __syncthreads();  // B2
 
             // ---- frame step over the double-buffered rotors (no barrier needed before it)
@@ -430,7 +430,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             }
             if (act) sm.q[cur ^ 1][t] = q;
             if constexpr (!ROPE)
-                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + I + it) * a.n + a.topo[dv].z, q);
+                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + I + it) * a.n + uidx, q);
             cur ^= 1;
         }
         __syncthreads();  // B3
@@ -457,7 +457,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
 
     // ---- write back: device-order state and caller-order views
     if (act) {
-        const int uidx = a.topo[dv].z;
+        // uidx: the caller index loaded with the vertex
         a.pos[dv] = f4(p, im);
         a.vel[dv] = f4(v, lr);
         a.lvel[dv] = f4(xyz(sm.lv[t]), ks);
