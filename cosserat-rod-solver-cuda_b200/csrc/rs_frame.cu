@@ -329,13 +329,18 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
         __syncthreads();  // B0
         const f3 p1 = hasNext ? xyz(sm.p[t + 1]) : zero3();
         // the substep's slack, squared: no plane and no candidate lattice (this substep's poses are
-        // in the cache after B0) can be touched while |dx|^2 < slack2; -1 = evaluate every iteration
+        // in the cache after B0) can be touched while |dx - dx0|^2 < slack2, the ball centred on the
+        // initial guess dx0, which the iterates stay close to (a vertex moving towards a surface is
+        // not flagged for the distance it covers in the substep, only for its corrections);
+        // -1 = evaluate every iteration
         float slack2 = -1.f;
+        const f3 dx0 = dx;
         if constexpr (kRedo)
             if (im != 0.f && a.surf_cull) {
-                float sl = plane_slack(a, p);
+                const f3 pc = p + dx0;
+                float sl = plane_slack(a, pc);
                 if constexpr (SURF == SURF_MESHES)
-                    if (cand && sl > 0.f) sl = fminf(sl, mesh_slack(a, mycache, cand, p));
+                    if (cand && sl > 0.f) sl = fminf(sl, mesh_slack(a, mycache, cand, pc));
                 slack2 = sl > 0.f ? (sl * sl) * 0.99998f : -1.f;
             }
 
@@ -362,7 +367,8 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             bool touched;
             if constexpr (kRedo) {
                 position_terms<SURF_NONE>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
-                touched = im != 0.f && !(dot(dx, dx) < slack2);
+                const f3 dr = dx - dx0;
+                touched = im != 0.f && !(dot(dr, dr) < slack2);
             } else {
                 touched = position_terms<SURF>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2,
                                                btab, mytbox);
@@ -448,7 +454,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
         }
         if constexpr (SURF == SURF_MESHES)
             if (a.forces_on && nsdf > 0)
-                mesh_readout_warp(a, mycache, (act && im != 0.f && !(dot(dx, dx) < slack2)) ? cand : 0ull, p, dx, c.kc,
+                mesh_readout_warp(a, mycache, (act && im != 0.f && !(dot(dx - dx0, dx - dx0) < slack2)) ? cand : 0ull, p, dx, c.kc,
                                   h, env, fv, btab, mytbox);
         if (SURF != SURF_NONE && a.forces_on) facc += fv;
         p += dx;

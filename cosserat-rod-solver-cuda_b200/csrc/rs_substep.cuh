@@ -210,9 +210,10 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
     return touched;
 }
 
-// The smallest sdf_slack over a vertex's candidate meshes at this substep's poses: while the
-// iterate d satisfies |d| < slack, surfaces() finds no mesh contact (persistent kernel: the mesh
-// terms are then skipped without rotating the probe into any lattice).
+// The smallest sdf_slack over a vertex's candidate meshes at this substep's poses, from the
+// probe `pos` (the persistent kernel passes the position plus the substep's initial guess d0):
+// while the iterate d satisfies |d - d0| < slack, surfaces() finds no mesh contact (the mesh terms
+// are then skipped without rotating the probe into any lattice).
 __device__ __forceinline__ float mesh_slack(const FrameArgs& a, const float4* cache, uint64_t cand, f3 pos) {
     float s = INFINITY;
     for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
@@ -223,10 +224,11 @@ __device__ __forceinline__ float mesh_slack(const FrameArgs& a, const float4* ca
     return s;
 }
 
-// How far a vertex's iterate d may move this substep before the probe pos + d could reach a
-// plane's contact band: gap(d) = (n.pos - w) + n.d - R >= (n.pos - w - R) - |d| for a unit
-// normal n, less a 1 mm margin that covers any difference in evaluating the gap expression for
-// coordinates up to ~10 km. INFINITY without planes.
+// How far a vertex's iterate may move from the probe `pos` (the persistent kernel passes the
+// position plus the substep's initial guess d0) before it could reach a plane's contact band:
+// gap(d) = (n.x - w) + n.d - R >= (n.pos - w - R) - |d - d0| for a unit normal n and
+// pos = x + d0, less a 1 mm margin that covers any difference in evaluating the gap expression
+// for coordinates up to ~10 km. INFINITY without planes.
 __device__ __forceinline__ float plane_slack(const FrameArgs& a, f3 pos) {
     float s = INFINITY;
     for (int pl = 0; pl < a.num_planes; pl++) {
