@@ -479,50 +479,73 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 }
                 cp_async_commit();
             }
-            if (hasNext) {
-                const float4 Fn4 = EF[t + 1];
+            if constexpr (!ROPE) {
+                // the stretch terms of segments t and t-1 reversed, without branches: a missing
+                // segment contributes with zero stiffness (its reads stay in the CTA's own slot)
+                const float4 Fn4 = EF[hasNext ? t + 1 : t];
                 const f3 Fn = xyz(Fn4);
-                const float kk = ks * c.invl, dd = kk * c.invl;
+                const float il = hasNext ? c.invl : 0.f;
+                const float kk = ks * il, dd = kk * il;
                 const f3 dF = Fb - Fn;
                 const f3 cb = dF * kk;
-                ksb += dot(cc, dF) * c.invl +
-                       (-damp * (dot(dk, Fb) + dot(dkn, Fn)) + (1.f + damp) * (trH + Fn4.w)) * c.invl * c.invl;
+                ksb += dot(cc, dF) * il + (-damp * (dot(dk, Fb) + dot(dkn, Fn)) + (1.f + damp) * (trH + Fn4.w)) * il * il;
                 qb = add4(qb, scale4(tangent_vjp(qk, cb), -1.f));
-                dn -= cb * c.invl;
-                xb -= cb * c.invl;
+                dn -= cb * il;
+                xb -= cb * il;
                 dn -= Fb * (damp * dd);
-                if constexpr (ROPE) {
-                    if (ncol > 0) {  // the segment's pairs reversed; other vertices' shares by shared-memory atomics
-                        const float4 zn4 = Dn[t + 1];
-                        const f3 lc = xyz(zn4) * (1.f / zn4.w) - dkn;
-                        const f3 ec = xyz(EE[t + 1]);
-                        PairGrad acc{};
-                        float4* cdk = CD + (k & 1) * BLOCK;
-                        for (int q2 = 0; q2 < ncol; q2++) {
-                            const int j = a.cols[(size_t)q2 * n + dv];
-                            PairGrad o{};
-                            collision_bwd(a, damp, p, p1, xyz(X[j]), xyz(X[j + 1]), dk, dkn, xyz(Dk[j]), xyz(Dk[j + 1]),
-                                          Fb, e, del, Fn, ec, lc, o);
-                            acc.x0 += o.x0; acc.d0 += o.d0; acc.x1 += o.x1; acc.d1 += o.d1;
-                            atomic_add3(cdk + j, o.e0);
-                            atomic_add3(cdk + j + 1, o.e1);
-                            atomic_add3(CX + j, o.y0);
-                            atomic_add3(CX + j + 1, o.y1);
+                const float4 kp = KC[hasPrev ? t - 1 : t];
+                const float ilp = hasPrev ? kp.y : 0.f;
+                const float kkp = kp.x * ilp, ddp = kkp * ilp;
+                const f3 cbp = (xyz(EF[hasPrev ? t - 1 : t]) - Fb) * kkp;
+                dn += cbp * ilp;
+                xb += cbp * ilp;
+                dn -= Fb * (damp * ddp);
+            } else {
+                if (hasNext) {
+                    const float4 Fn4 = EF[t + 1];
+                    const f3 Fn = xyz(Fn4);
+                    const float kk = ks * c.invl, dd = kk * c.invl;
+                    const f3 dF = Fb - Fn;
+                    const f3 cb = dF * kk;
+                    ksb += dot(cc, dF) * c.invl +
+                           (-damp * (dot(dk, Fb) + dot(dkn, Fn)) + (1.f + damp) * (trH + Fn4.w)) * c.invl * c.invl;
+                    qb = add4(qb, scale4(tangent_vjp(qk, cb), -1.f));
+                    dn -= cb * c.invl;
+                    xb -= cb * c.invl;
+                    dn -= Fb * (damp * dd);
+                    if constexpr (ROPE) {
+                        if (ncol > 0) {  // the segment's pairs reversed; other vertices' shares by shared-memory atomics
+                            const float4 zn4 = Dn[t + 1];
+                            const f3 lc = xyz(zn4) * (1.f / zn4.w) - dkn;
+                            const f3 ec = xyz(EE[t + 1]);
+                            PairGrad acc{};
+                            float4* cdk = CD + (k & 1) * BLOCK;
+                            for (int q2 = 0; q2 < ncol; q2++) {
+                                const int j = a.cols[(size_t)q2 * n + dv];
+                                PairGrad o{};
+                                collision_bwd(a, damp, p, p1, xyz(X[j]), xyz(X[j + 1]), dk, dkn, xyz(Dk[j]), xyz(Dk[j + 1]),
+                                              Fb, e, del, Fn, ec, lc, o);
+                                acc.x0 += o.x0; acc.d0 += o.d0; acc.x1 += o.x1; acc.d1 += o.d1;
+                                atomic_add3(cdk + j, o.e0);
+                                atomic_add3(cdk + j + 1, o.e1);
+                                atomic_add3(CX + j, o.y0);
+                                atomic_add3(CX + j + 1, o.y1);
+                            }
+                            dn += acc.d0;
+                            xb += acc.x0;
+                            atomic_add3(cdk + t + 1, acc.d1);
+                            atomic_add3(CX + t + 1, acc.x1);
                         }
-                        dn += acc.d0;
-                        xb += acc.x0;
-                        atomic_add3(cdk + t + 1, acc.d1);
-                        atomic_add3(CX + t + 1, acc.x1);
                     }
                 }
-            }
-            if (hasPrev) {
-                const float4 kp = KC[t - 1];
-                const float kkp = kp.x * kp.y, ddp = kkp * kp.y;
-                const f3 cbp = (xyz(EF[t - 1]) - Fb) * kkp;
-                dn += cbp * kp.y;
-                xb += cbp * kp.y;
-                dn -= Fb * (damp * ddp);
+                if (hasPrev) {
+                    const float4 kp = KC[t - 1];
+                    const float kkp = kp.x * kp.y, ddp = kkp * kp.y;
+                    const f3 cbp = (xyz(EF[t - 1]) - Fb) * kkp;
+                    dn += cbp * kp.y;
+                    xb += cbp * kp.y;
+                    dn -= Fb * (damp * ddp);
+                }
             }
             db = dn;
         }

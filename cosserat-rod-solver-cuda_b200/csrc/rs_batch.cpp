@@ -784,6 +784,13 @@ void Batch::tune_after_frame() {
     if (tune_log_.size() < tune_cands_.size()) return;
     auto best = std::min_element(tune_log_.begin(), tune_log_.end(),
                                  [](const std::pair<int, double>& x, const std::pair<int, double>& y) { return x.second < y.second; });
+    // Ties within 3% (the trial frames are different frames of the run) go to the smallest bins:
+    // they spread a frame over more CTAs, and the adjoint, which runs on the forward's bins, gains
+    // from that (1024 64-vertex ropes: 42.1 against 45.0 ms per 30 reverses in 64- and 256-thread
+    // bins at equal forward time).
+    const double limit = best->second * 1.03;
+    for (auto it = tune_log_.begin(); it != tune_log_.end(); ++it)
+        if (it->second <= limit && it->first < best->first) best = it;
     tuned_ = true;
     {
         std::lock_guard<std::mutex> g(g_tune_mtx);
