@@ -78,6 +78,7 @@ static py::class_<rso::Sim<T>> bind_sim(py::module_& m, const char* name) {
         .def_property("drag_quad", [](S& s) { return (double)s.dragQuad; }, [](S& s, float v) { s.dragQuad = T(v); })
         .def_property("drag_quad_t", [](S& s) { return (double)s.dragQuadT; }, [](S& s, float v) { s.dragQuadT = T(v); })
         .def_property("damping", [](S& s) { return (double)s.damping; }, [](S& s, float v) { s.damping = T(v); })
+        .def_property("inplace_frames", [](S& s) { return s.inplaceFrames; }, [](S& s, bool v) { s.inplaceFrames = v; })
         .def_property("accel_ratio", [](S& s) { return (double)s.accel; }, [](S& s, float v) { s.accel = T(v); })
         .def_property("num_itr", [](S& s) { return s.numItr; }, [](S& s, int v) { s.numItr = v; })
         .def_property("max_h", [](S& s) { return s.maxH; }, [](S& s, float v) { s.maxH = v; })

@@ -204,6 +204,7 @@ public:
     T radius = T(1e-4), barrier = T(8e-4), kCollision = T(1e-5), fricMu = T(0.1), kFriction = 5, detScaler = T(1.2);
     T detRadius = 0, scaledDetRadius = 0, minSegLen = 0, maxSegLen = 0;
     bool ropeContact = false, useStepLimit = false;
+    bool inplaceFrames = false;  // frame sweep in place (frame_sweep)
     int groupRopes = 1;
     std::vector<int> numCols;             // per segment
     std::vector<std::vector<int>> cols;   // per segment candidate list (ascending j)
@@ -796,8 +797,13 @@ public:
             H2 -= op * (wb * wb * f1);
         }
     }
-    // quaternionLambdaItr<SNAPSHOT=true>, cosserat.cu:227-273.
+    // quaternionLambdaItr<SNAPSHOT=true>, cosserat.cu:227-273. With inplaceFrames the sweep reads
+    // the rotors it has already updated (SNAPSHOT=false, cosserat.cu:252-268, reads d_qs while
+    // threads write it): a vertex-order Gauss-Seidel pass, one deterministic realisation of the
+    // reference's default racing sweep (there the order is the warp schedule), kept so that the
+    // difference between the two orderings can be measured.
     void frame_sweep() {
+        const std::vector<Q4<T>>& qs = inplaceFrames ? q : qPrev;
         for (int i = 0; i < n; i++) {
             dx[i] = dxNext[i];
             if ((flags[i] & F_FIX_ORIENT) || !(flags[i] & F_NEXT)) continue;
@@ -807,12 +813,12 @@ public:
             Q4<T> b(0, 0, 0, 0);
             const Q4<T> q0 = qPrev[i];
             if (flags[i] & F_PREV) {
-                const Q4<T> qr = qRest[i - 1], qq = qPrev[i - 1];
+                const Q4<T> qr = qRest[i - 1], qq = qs[i - 1];
                 const T s = dot4(qmul(qq.inv(), q0), qr) > 0 ? T(1) : T(-1);
                 b += qmul(qq, qr) * s;
             }
             if (flags[i] & F_NEXT_ORIENT) {
-                const Q4<T> qr = qRest[i], qq = qPrev[i + 1];
+                const Q4<T> qr = qRest[i], qq = qs[i + 1];
                 const T s = dot4(qmul(q0.inv(), qq), qr) > 0 ? T(1) : T(-1);
                 b += qmul(qq, qr.inv()) * s;
             }
