@@ -151,6 +151,30 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
     const float g2 = dot(gv, gv);
     const int S = a.substeps;
     const size_t n = (size_t)a.n;
+    // Constant over the frame: the neighbour slots (a missing neighbour reads the own slot), the
+    // frame step's -2k and -2k/l, the stretch reverse's 1/l, k/l and k/l² of the own segment (zero
+    // without one) and k/l² of the previous segment, and the damping shares of both.
+    const int tp = hasPrev ? t - 1 : t, tn = nextOrient ? t + 1 : t, tn1 = hasNext ? t + 1 : t;
+    const float m2ks = -2.f * ks, m2ksil = m2ks * c.invl;
+    const float ilo = hasNext ? c.invl : 0.f, ilo2 = ilo * ilo;
+    const float kko = ks * ilo, ddo = kko * ilo;
+    // (the mesh variant reads the previous segment's from KC where they are used: held in
+    // registers they make its lattice path spill)
+    auto prev_seg = [&](float& dd, float& ir) {
+        const float4 kp = KC[tp];
+        const float ilp = hasPrev ? kp.y : 0.f;
+        dd = (kp.x * ilp) * ilp;
+        ir = kp.w;
+    };
+    float ddp = 0.f, irho_p = 0.f;
+    if constexpr (SURF != SURF_MESHES) prev_seg(ddp, irho_p);
+    // The iterate tape also holds each frame step's blend rotor b and its sign tests: b of the next
+    // reverse iteration is loaded one iteration ahead (only this vertex reads it). The mesh variant
+    // recomputes them instead (the prefetched rotor's registers would make its lattice path spill).
+    const bool tb = !ROPE && SURF != SURF_MESHES && g.itape != nullptr;
+    const float4* btape = tb ? g.itape + 2 * (size_t)I * n + uidx : nullptr;  // + (s * 3I + k) * n
+    float4 bnx = zero4();
+    if (tb && act) bnx = __ldcs(btape + ((size_t)(S - 1) * 3 * I + (I - 1)) * n);
 
     // adjoints of the frame-end state
     f3 xb = zero3(), vb = zero3(), lvb = zero3();
@@ -175,8 +199,8 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 cp_async_wait_all();
                 t0 = X[t]; t1 = EA[t]; t2 = EB[t]; t3 = EC[t];
             } else {
-                const float4* tp = g.tape + (size_t)s * 4 * n + uidx;
-                t0 = __ldcs(tp); t1 = __ldcs(tp + n); t2 = __ldcs(tp + 2 * n); t3 = __ldcs(tp + 3 * n);
+                const float4* ts = g.tape + (size_t)s * 4 * n + uidx;
+                t0 = __ldcs(ts); t1 = __ldcs(ts + n); t2 = __ldcs(ts + 2 * n); t3 = __ldcs(ts + 3 * n);
             }
             p = xyz(t0); v = xyz(t1); lvin = xyz(t2); q = t3;
             cand = (uint64_t)(uint32_t)__float_as_int(t0.w) | ((uint64_t)(uint32_t)__float_as_int(t1.w) << 32);
@@ -195,6 +219,7 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
         if constexpr (ROPE) RP[t] = make_float4(a.sdet_radius + len(y), INFINITY, __int_as_float((int)fl), 0.f);
         __syncthreads();
         const f3 p1 = hasNext ? xyz(X[t + 1]) : zero3();
+        const f3 p1mp = p1 - p;
 
         // ---- rope-rope detection and step limit (the frame kernel's, from the same inputs)
         int ncol = 0;
@@ -216,8 +241,8 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
         if (!ROPE && g.itape) {
             if (s == S - 1 && act) {
                 for (int k = 0; k < I; k++) {
-                    cp_async16(LD + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)(s * 2 * I + k) * n + uidx);
-                    cp_async16(LQ + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)(s * 2 * I + I + k) * n + uidx);
+                    cp_async16(LD + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)(s * 3 * I + k) * n + uidx);
+                    cp_async16(LQ + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)(s * 3 * I + I + k) * n + uidx);
                 }
                 cp_async_commit();
             }
@@ -313,43 +338,58 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             const float4* Lq = LQ + (size_t)k * BLOCK;
             const float4* Dk = LD + (size_t)k * BLOCK;
             const float4* Dn = LD + (size_t)(k + 1) * BLOCK;
+            const float4* Dq = LQ + (size_t)(k + 1) * BLOCK;
             // frame step k: q^{k+1}_t = normalize(vv b e1 + (|vv| + |b|) b)
             float4 own = qb, toL = zero4(), toR = zero4();
             f3 su = zero3();
+            const float4 bk = bnx;
+            if (tb && act && (k > 0 || s > 0))
+                bnx = __ldcs(btape + ((size_t)(k > 0 ? s : s - 1) * 3 * I + (k > 0 ? k - 1 : I - 1)) * n);
             if (upd) {
                 own = zero4();
-                const f3 u = ((p1 - p) + (xyz(Dn[t + 1]) - xyz(Dn[t]))) * c.invl;
-                const f3 vv = u * (-2.f * ks);
-                const float4 q0 = Lq[t];
-                // both neighbour products, the missing ones selected away (as the forward's frame_update)
-                const float4 qp = Lq[hasPrev ? t - 1 : t], rp = QR[hasPrev ? t - 1 : t];
-                const float4 qn = Lq[nextOrient ? t + 1 : t], rn = QR[t];
-                const float4 pr = qmul(qp, rp), nx = qmul(qn, qconj(rn));
-                const float spv = dot4(q0, pr) > 0.f ? 1.f : -1.f, snv = dot4(q0, nx) > 0.f ? 1.f : -1.f;
+                const f3 u = (p1mp + (xyz(Dn[t + 1]) - xyz(Dn[t]))) * c.invl;
+                const f3 vv = u * m2ks;
+                const float4 qp = Lq[tp], rp = QR[tp];
+                const float4 qn = Lq[tn], rn = QR[t];
+                float spv, snv;
+                float4 b;
+                if (tb) {  // the forward's b and sign tests, from the iterate tape
+                    frame_signs_decode(Dn[t].w, spv, snv);
+                    b = bk;
+                } else {   // both neighbour products, the missing ones selected away (as frame_update)
+                    const float4 q0 = Lq[t];
+                    const float4 pr = qmul(qp, rp), nx = qmul(qn, qconj(rn));
+                    spv = dot4(q0, pr) > 0.f ? 1.f : -1.f;
+                    snv = dot4(q0, nx) > 0.f ? 1.f : -1.f;
+                    b = hasPrev ? scale4(pr, spv) : zero4();
+                    const float4 bn = add4(b, scale4(nx, snv));
+                    b = nextOrient ? bn : b;
+                }
                 const float sp = hasPrev ? spv : 0.f, sn = nextOrient ? snv : 0.f;
-                float4 b = hasPrev ? scale4(pr, spv) : zero4();
-                const float4 bn = add4(b, scale4(nx, snv));
-                b = nextOrient ? bn : b;
                 float ilvv, ilb, lambda;  // the forward's z (frame_z), so the reverse linearises what ran
                 const float4 z = frame_z(vv, b, ilvv, ilb, lambda);
                 const float izl = rsqrt_nr(dot4(z, z));
-                const float4 qo = scale4(z, izl);
-                const float4 zb = scale4(add4(qb, scale4(qo, -dot4(qo, qb))), izl);
-                float4 bb = scale4(zb, lambda);
+                const float4 qo = Dq[t];  // q^{k+1} = z / |z|, as the forward stored it
+                const float4 zb = scale4(fma4(qo, -dot4(qo, qb), qb), izl);
                 const float lamb = dot4(zb, b);
                 f3 vvb = vv * (lamb * ilvv);
-                bb = add4(bb, scale4(b, lamb * ilb));
+                float4 bb = fma4(b, lamb * ilb, scale4(zb, lambda));
                 const float4 Ab = scale4(qmul_e1(zb), -1.f);   // z = A e1  ->  Ā = z̄ e1* = -(z̄ e1)
-                vvb += xyz(qmul(Ab, qconj(b)));
-                bb = add4(bb, scale4(qmul_pure(vv, Ab), -1.f)); // (vv, 0)* Ā = -(vv, 0) Ā
-                ksb += -2.f * dot(u, vvb);
-                su = vvb * (-2.f * ks * c.invl);
+                vvb = qmul_vec_add(Ab, qconj(b), vvb);           // A = (vv, 0) b: vv̄ += vec(Ā b*)
+                {                                                // b̄ += (vv, 0)* Ā = -(vv, 0) Ā
+                    const f3 Av = xyz(Ab);
+                    const f3 r = fma3(vv, -Ab.w, cross_add(Av, vv, xyz(bb)));
+                    bb = make_float4(r.x, r.y, r.z, dot_add(vv, Av, bb.w));
+                }
+                ksb = fmaf(-2.f, dot(u, vvb), ksb);
+                su = vvb * m2ksil;
                 // b = sp q_{t-1} r_{t-1} + sn q_{t+1} r_t^*: the rotor adjoints b̄ r^(*) also give the
                 // rest-rotor magnitude adjoints, <q^* b̄, r> = <b̄ r^*, q> and <(q^* b̄)^*, r> = <b̄ r, q>
                 toL = qmul(scale4(bb, sp), qconj(rp));  // zero without the neighbour (sp, sn = 0)
-                rhobp += dot4(toL, qp) * KC[hasPrev ? t - 1 : t].w;
+                if constexpr (SURF == SURF_MESHES) prev_seg(ddp, irho_p);
+                rhobp = fmaf(dot4(toL, qp), irho_p, rhobp);
                 toR = qmul(scale4(bb, sn), rn);
-                rhob += dot4(toR, qn) * irho;
+                rhob = fmaf(dot4(toR, qn), irho, rhob);
             }
             EA[t] = toL;
             EB[t] = toR;
@@ -368,12 +408,12 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             }
             __syncthreads();
             {
-                const float4 ebp = EB[hasPrev ? t - 1 : t], ean = EA[hasNext ? t + 1 : t];
+                const float4 ebp = EB[tp], ean = EA[tn1];
                 const float4 q1 = add4(own, ebp);
                 qb = hasPrev ? q1 : own;
                 const float4 q2 = add4(qb, ean);
                 qb = hasNext ? q2 : qb;
-                const f3 dp = -su + xyz(EC[hasPrev ? t - 1 : t]);
+                const f3 dp = -su + xyz(EC[tp]);
                 const f3 dd = hasPrev ? dp : -su;
                 db += dd;
                 xb += dd;
@@ -434,9 +474,9 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
                 del = zk - dk;
                 Fb = e * a.accel;
                 trH = -dot(e, del);
-                yb += Fb * c.fm;
-                dn -= Fb * c.fm;
-                float wsum = (dot(y - dk, Fb) + trH) * wscale;
+                yb = fma3(Fb, c.fm, yb);
+                dn = fma3(Fb, -c.fm, dn);
+                float wsum = dot_add(y - dk, Fb, trH) * wscale;
                 if constexpr (SURF != SURF_NONE) {
                     for (int pl = 0; pl < a.num_planes; pl++) {
                         const float4 P = a.planes[pl];
@@ -460,7 +500,7 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             // after it a neighbour may already be writing the next substep's iterates
             const float4 qk = Lq[t];
             const f3 dkn = hasNext ? xyz(Dk[t + 1]) : zero3();
-            const f3 cc = hasNext ? ((p1 - p) + (dkn - dk)) * c.invl - qtangent(qk) : zero3();
+            const f3 cc = hasNext ? fma3(p1mp + (dkn - dk), c.invl, -qtangent(qk)) : zero3();
             EF[t] = f4(Fb, trH);
             if constexpr (ROPE) EE[t] = f4(e, 0.f);
             __syncthreads();
@@ -468,38 +508,33 @@ __global__ void __launch_bounds__(BLOCK, ROPE ? (BLOCK >= 256 ? 1 : 256 / BLOCK)
             // after the last reverse iteration the exchange slots X, EA, EB, EC are free as well
             // and take the previous substep's start state
             if (!ROPE && g.itape && s > 0 && act) {
-                cp_async16(LD + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)((s - 1) * 2 * I + k) * n + uidx);
-                cp_async16(LQ + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)((s - 1) * 2 * I + I + k) * n + uidx);
+                cp_async16(LD + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)((s - 1) * 3 * I + k) * n + uidx);
+                cp_async16(LQ + (size_t)(k + 1) * BLOCK + t, g.itape + (size_t)((s - 1) * 3 * I + I + k) * n + uidx);
                 if (k == 0) {
-                    const float4* tp = g.tape + (size_t)(s - 1) * 4 * n + uidx;
-                    cp_async16(X + t, tp);
-                    cp_async16(EA + t, tp + n);
-                    cp_async16(EB + t, tp + 2 * n);
-                    cp_async16(EC + t, tp + 3 * n);
+                    const float4* ts = g.tape + (size_t)(s - 1) * 4 * n + uidx;
+                    cp_async16(X + t, ts);
+                    cp_async16(EA + t, ts + n);
+                    cp_async16(EB + t, ts + 2 * n);
+                    cp_async16(EC + t, ts + 3 * n);
                 }
                 cp_async_commit();
             }
             if constexpr (!ROPE) {
                 // the stretch terms of segments t and t-1 reversed, without branches: a missing
                 // segment contributes with zero stiffness (its reads stay in the CTA's own slot)
-                const float4 Fn4 = EF[hasNext ? t + 1 : t];
+                const float4 Fn4 = EF[tn1];
                 const f3 Fn = xyz(Fn4);
-                const float il = hasNext ? c.invl : 0.f;
-                const float kk = ks * il, dd = kk * il;
                 const f3 dF = Fb - Fn;
-                const f3 cb = dF * kk;
-                ksb += dot(cc, dF) * il + (-damp * (dot(dk, Fb) + dot(dkn, Fn)) + (1.f + damp) * (trH + Fn4.w)) * il * il;
-                qb = add4(qb, scale4(tangent_vjp(qk, cb), -1.f));
-                dn -= cb * il;
-                xb -= cb * il;
-                dn -= Fb * (damp * dd);
-                const float4 kp = KC[hasPrev ? t - 1 : t];
-                const float ilp = hasPrev ? kp.y : 0.f;
-                const float kkp = kp.x * ilp, ddp = kkp * ilp;
-                const f3 cbp = (xyz(EF[hasPrev ? t - 1 : t]) - Fb) * kkp;
-                dn += cbp * ilp;
-                xb += cbp * ilp;
-                dn -= Fb * (damp * ddp);
+                const float sx = fmaf(-damp, dot_add(dkn, Fn, dot(dk, Fb)), (1.f + damp) * (trH + Fn4.w));
+                ksb = fmaf(sx, ilo2, fmaf(dot(cc, dF), ilo, ksb));
+                qb = sub4(qb, tangent_vjp(qk, dF * kko));
+                dn = fma3(dF, -ddo, dn);
+                xb = fma3(dF, -ddo, xb);
+                if constexpr (SURF == SURF_MESHES) prev_seg(ddp, irho_p);
+                const f3 dFp = xyz(EF[tp]) - Fb;
+                dn = fma3(dFp, ddp, dn);
+                xb = fma3(dFp, ddp, xb);
+                dn = fma3(Fb, -(damp * ddo + damp * ddp), dn);
             } else {
                 if (hasNext) {
                     const float4 Fn4 = EF[t + 1];

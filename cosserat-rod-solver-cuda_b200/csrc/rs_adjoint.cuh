@@ -21,9 +21,11 @@ __device__ __forceinline__ f3 ld3(const float* a, int u) { return mk3(a[3 * u], 
 __device__ __forceinline__ void st3(float* a, int u, f3 v) { a[3 * u] = v.x; a[3 * u + 1] = v.y; a[3 * u + 2] = v.z; }
 
 // Transposed Jacobian of the tangent t(q) = q e_x q*.
+// The factor 2 is applied to tb first (exact: a power of two), each component is an fmaf chain.
 __device__ __forceinline__ float4 tangent_vjp(float4 q, f3 tb) {
-    return make_float4(2.f * (q.x * tb.x + q.y * tb.y + q.z * tb.z), 2.f * (-q.y * tb.x + q.x * tb.y - q.w * tb.z),
-                       2.f * (-q.z * tb.x + q.w * tb.y + q.x * tb.z), 2.f * (q.w * tb.x + q.z * tb.y - q.y * tb.z));
+    const f3 t2 = tb * 2.f;
+    return make_float4(fmaf(q.z, t2.z, fmaf(q.y, t2.y, q.x * t2.x)), fmaf(-q.w, t2.z, fmaf(q.x, t2.y, -q.y * t2.x)),
+                       fmaf(q.x, t2.z, fmaf(q.w, t2.y, -q.z * t2.x)), fmaf(-q.y, t2.z, fmaf(q.z, t2.y, q.w * t2.x)));
 }
 
 // Contact law (contact.cuh:27-46) reversed: f += n N - ut kt, H += k nnᵀ - kt (nnᵀ - I), with

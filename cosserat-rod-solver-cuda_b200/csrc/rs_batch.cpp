@@ -602,6 +602,9 @@ void Batch::run_frame(int root_mode, bool has_q0, bool has_q1, float dt, int ste
         a.queue = d_queue_; a.order = d_order_; a.bin_cost = d_bin_cost_;
     }
     const bool timed = timing_ || tuning();
+    // a timed frame measures the kernel, not its first-use loading (each trial of the autotuner
+    // is the first launch of its bin size)
+    if (timed && !plain) check(prepare_frame(a, block_), "frame kernel set-up");
     if (timed) check(cudaEventRecord(ev0_, stream_), "event");
     if (plain) run_frame_plain(a);
     else check(launch_frame(a, block_, (int)bins_.size(), stream_), "frame kernel");

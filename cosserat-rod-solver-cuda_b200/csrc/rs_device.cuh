@@ -44,6 +44,12 @@ __device__ __forceinline__ f3 fma3(f3 a, float s, f3 b) { return f3{fmaf(a.x, s,
 __device__ __forceinline__ f3 cross(f3 a, f3 b) {
     return f3{fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x))};
 }
+// c + a x b and c + a.b, accumulated into c by fused multiply-adds
+__device__ __forceinline__ f3 cross_add(f3 a, f3 b, f3 c) {
+    return f3{fmaf(a.y, b.z, fmaf(-a.z, b.y, c.x)), fmaf(a.z, b.x, fmaf(-a.x, b.z, c.y)),
+              fmaf(a.x, b.y, fmaf(-a.y, b.x, c.z))};
+}
+__device__ __forceinline__ float dot_add(f3 a, f3 b, float c) { return fmaf(a.z, b.z, fmaf(a.y, b.y, fmaf(a.x, b.x, c))); }
 __device__ __forceinline__ float len(f3 a) { return sqrtf(dot(a, a)); }
 __device__ __forceinline__ f3 lerp3(f3 a, f3 b, float t) { return fma3(b, t, a * (1.f - t)); }
 __device__ __forceinline__ f3 xyz(float4 v) { return f3{v.x, v.y, v.z}; }
@@ -61,6 +67,16 @@ __device__ __forceinline__ float dot4(float4 a, float4 b) {
 }
 __device__ __forceinline__ float4 scale4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
 __device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ float4 sub4(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+// a * s + c, fused per component
+__device__ __forceinline__ float4 fma4(float4 a, float s, float4 c) {
+    return make_float4(fmaf(a.x, s, c.x), fmaf(a.y, s, c.y), fmaf(a.z, s, c.z), fmaf(a.w, s, c.w));
+}
+// c + vec(a b): the vector part of a rotor product, accumulated into c
+__device__ __forceinline__ f3 qmul_vec_add(float4 a, float4 b, f3 c) {
+    const f3 av = mk3(a.x, a.y, a.z), bv = mk3(b.x, b.y, b.z);
+    return fma3(av, b.w, fma3(bv, a.w, cross_add(av, bv, c)));
+}
 __device__ __forceinline__ float4 normalize4(float4 a) { return scale4(a, 1.f / sqrtf(dot4(a, a))); }
 __device__ __forceinline__ f3 qrot(float4 q, f3 v) {
     const f3 qv = xyz(q);

@@ -424,19 +424,25 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                 }
             }
             if (act) sm.dx[t] = f4(dx, 0.f);
-            if constexpr (!ROPE)
-                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + it) * a.n + uidx, f4(dx, 0.f));
             __syncthreads();  // B2
 
             // ---- frame step over the double-buffered rotors (no barrier needed before it)
+            float4 fb = make_float4(0.f, 0.f, 0.f, 0.f);
+            float fsig = 0.f;
             if (!(fl & F_FIX_ORIENT) && hasNext) {
                 const f3 seg = (p1 - p) + (xyz(sm.dx[t + 1]) - dx);
                 q = frame_update(q, seg, c.invl, ks, hasPrev, sm.q[cur][hasPrev ? t - 1 : t], qr_prev,
-                                 (fl & F_NEXT_ORIENT) != 0, sm.q[cur][(fl & F_NEXT_ORIENT) ? t + 1 : t], qr_own);
+                                 (fl & F_NEXT_ORIENT) != 0, sm.q[cur][(fl & F_NEXT_ORIENT) ? t + 1 : t], qr_own, fb,
+                                 fsig);
             }
             if (act) sm.q[cur ^ 1][t] = q;
             if constexpr (!ROPE)
-                if (a.itape && act) __stcs(a.itape + (size_t)(s * 2 * I + I + it) * a.n + uidx, q);
+                if (a.itape && act) {  // d^{k+1} with the frame step's signs, q^{k+1}, the frame step's b
+                    float4* it4 = a.itape + (size_t)(s * 3 * I + it) * a.n + uidx;
+                    __stcs(it4, f4(dx, fsig));
+                    __stcs(it4 + (size_t)I * a.n, q);
+                    __stcs(it4 + (size_t)2 * I * a.n, fb);
+                }
             cur ^= 1;
         }
         __syncthreads();  // B3
@@ -524,13 +530,24 @@ static int resident_ctas(const void* kernel, int block, size_t dyn_smem) {
 }
 
 // ------------------------------------------------------------------ launch
+// With `prepare` set nothing is launched: the kernel is loaded (lazy module loading defers that
+// to its first use), its shared-memory limit set and its resident-CTA count cached, so that a
+// launch timed afterwards (the autotuner's trial frames) times the kernel and not that set-up.
 template <int BLOCK, int SURF, bool ROPE>
-static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_bytes, cudaStream_t s) {
+static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_bytes, cudaStream_t s, bool prepare) {
     auto k = frame_kernel<BLOCK, SURF, ROPE>;
     const size_t dyn_smem = sizeof(FrameSmem<BLOCK>) + pose_bytes;
     if (dyn_smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
         if (e != cudaSuccess) return e;
+    }
+    if (prepare) {
+        cudaFuncAttributes attr;
+        cudaError_t e = cudaFuncGetAttributes(&attr, k);
+        if (e != cudaSuccess) return e;
+        if (a.queue && resident_ctas(reinterpret_cast<const void*>(k), BLOCK, dyn_smem) <= 0)
+            return cudaErrorInvalidConfiguration;
+        return cudaSuccess;
     }
     int grid = num_bins;
     if (a.queue) {  // the work queue: as many CTAs as can be resident at once
@@ -543,29 +560,37 @@ static cudaError_t launch_frame_t(const FrameArgs& a, int num_bins, size_t pose_
 }
 
 template <int BLOCK, bool ROPE>
-static cudaError_t launch_frame_r(const FrameArgs& a, int num_bins, cudaStream_t s) {
+static cudaError_t launch_frame_r(const FrameArgs& a, int num_bins, cudaStream_t s, bool prepare) {
     if (a.num_sdf > 0)
         return launch_frame_t<BLOCK, SURF_MESHES, ROPE>(
-            a, num_bins, (size_t)2 * a.pose_cache * (kPoseF4 + 2) * sizeof(float4) + (size_t)a.sdf_btab * sizeof(float), s);
-    if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES, ROPE>(a, num_bins, 0, s);
-    return launch_frame_t<BLOCK, SURF_NONE, ROPE>(a, num_bins, 0, s);
+            a, num_bins, (size_t)2 * a.pose_cache * (kPoseF4 + 2) * sizeof(float4) + (size_t)a.sdf_btab * sizeof(float), s,
+            prepare);
+    if (a.num_planes > 0) return launch_frame_t<BLOCK, SURF_PLANES, ROPE>(a, num_bins, 0, s, prepare);
+    return launch_frame_t<BLOCK, SURF_NONE, ROPE>(a, num_bins, 0, s, prepare);
 }
 
 template <int BLOCK>
-static cudaError_t launch_frame_b(const FrameArgs& a, int num_bins, cudaStream_t s) {
-    return a.rope_contact ? launch_frame_r<BLOCK, true>(a, num_bins, s) : launch_frame_r<BLOCK, false>(a, num_bins, s);
+static cudaError_t launch_frame_b(const FrameArgs& a, int num_bins, cudaStream_t s, bool prepare) {
+    return a.rope_contact ? launch_frame_r<BLOCK, true>(a, num_bins, s, prepare)
+                          : launch_frame_r<BLOCK, false>(a, num_bins, s, prepare);
 }
 
-cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s) {
+static cudaError_t launch_frame_any(const FrameArgs& a, int block, int num_bins, cudaStream_t s, bool prepare) {
     switch (block) {
-        case 64: return launch_frame_b<64>(a, num_bins, s);
-        case 128: return launch_frame_b<128>(a, num_bins, s);
-        case 256: return launch_frame_b<256>(a, num_bins, s);
-        case 512: return launch_frame_b<512>(a, num_bins, s);
-        case 1024: return launch_frame_b<1024>(a, num_bins, s);
+        case 64: return launch_frame_b<64>(a, num_bins, s, prepare);
+        case 128: return launch_frame_b<128>(a, num_bins, s, prepare);
+        case 256: return launch_frame_b<256>(a, num_bins, s, prepare);
+        case 512: return launch_frame_b<512>(a, num_bins, s, prepare);
+        case 1024: return launch_frame_b<1024>(a, num_bins, s, prepare);
         default: return cudaErrorInvalidValue;
     }
 }
+
+cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s) {
+    return launch_frame_any(a, block, num_bins, s, false);
+}
+
+cudaError_t prepare_frame(const FrameArgs& a, int block) { return launch_frame_any(a, block, 0, nullptr, true); }
 
 // ------------------------------------------------------------------ static candidate scratch
 // Rope-rope candidate lists for callers that must not allocate device memory: a fixed array

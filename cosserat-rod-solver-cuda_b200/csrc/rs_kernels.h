@@ -11,6 +11,9 @@ namespace rs {
 
 // One persistent launch that runs every substep of one control frame for every bin.
 cudaError_t launch_frame(const FrameArgs& a, int block, int num_bins, cudaStream_t s);
+// Everything launch_frame does on the host before its launch (load the kernel, set its shared
+// memory limit, count its resident CTAs), without launching: run before a timed launch.
+cudaError_t prepare_frame(const FrameArgs& a, int block);
 // Device state -> caller-order views.
 cudaError_t launch_gather(const FrameArgs& a, int n, cudaStream_t s);
 // Restore construction state of device vertex ranges (x = start, y = count).

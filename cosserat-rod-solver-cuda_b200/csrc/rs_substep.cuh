@@ -477,6 +477,14 @@ __device__ __forceinline__ float4 frame_z(f3 vv, float4 b, float& ilvv, float& i
     return make_float4(fmaf(b.x, lambda, m.x), fmaf(b.y, lambda, m.y), fmaf(b.z, lambda, m.z), fmaf(b.w, lambda, m.w));
 }
 
+// The frame step's two sign tests (each +1 or -1) as one exact small float, 2 snv + spv, for the
+// iterate tape; decoded by frame_signs_decode.
+__device__ __forceinline__ float frame_signs_encode(float spv, float snv) { return fmaf(2.f, snv, spv); }
+__device__ __forceinline__ void frame_signs_decode(float code, float& spv, float& snv) {
+    snv = code > 0.f ? 1.f : -1.f;
+    spv = fmaf(-2.f, snv, code);
+}
+
 // Frame step of segment i, cosserat.cu:242-272: vv = -2 k ((p1 - p) + (p1dx - dx)) / l, b from
 // the neighbours' frames and rest rotations, q = normalize(vv b e1 + (|vv| + |b|) b). The
 // reference's sign tests dot((q_{i-1}^-1 q_i), r_{i-1}) and dot((q_i^-1 q_{i+1}), r_i) equal
@@ -488,18 +496,28 @@ __device__ __forceinline__ float4 frame_z(f3 vv, float4 b, float& ilvv, float& i
 // twice the instructions and a branch each; a frame of 4096 64-vertex ropes 2.75 -> 2.35 ms with
 // the rest of this step's diet).
 __device__ __forceinline__ float4 frame_update(float4 q, f3 seg, float invl, float ks, bool hasPrev, float4 qprev,
-                                               float4 qrprev, bool hasNextOrient, float4 qnext, float4 qrown) {
+                                               float4 qrprev, bool hasNextOrient, float4 qnext, float4 qrown,
+                                               float4& b_out, float& signs) {
     const f3 vv = (seg * invl) * (-2.f * ks);
     const float4 pr = qmul(qprev, qrprev);
     const float4 nx = qmul(qnext, qconj(qrown));
-    const float4 prs = scale4(pr, dot4(q, pr) > 0.f ? 1.f : -1.f);
-    const float4 nxs = scale4(nx, dot4(q, nx) > 0.f ? 1.f : -1.f);
+    const float spv = dot4(q, pr) > 0.f ? 1.f : -1.f, snv = dot4(q, nx) > 0.f ? 1.f : -1.f;
+    const float4 prs = scale4(pr, spv);
+    const float4 nxs = scale4(nx, snv);
     float4 b = hasPrev ? prs : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 bn = add4(b, nxs);
     b = hasNextOrient ? bn : b;
+    b_out = b;
+    signs = frame_signs_encode(spv, snv);
     float ilvv, ilb, lambda;
     const float4 z = frame_z(vv, b, ilvv, ilb, lambda);
     return scale4(z, rsqrt_nr(dot4(z, z)));
+}
+__device__ __forceinline__ float4 frame_update(float4 q, f3 seg, float invl, float ks, bool hasPrev, float4 qprev,
+                                               float4 qrprev, bool hasNextOrient, float4 qnext, float4 qrown) {
+    float4 b;
+    float signs;
+    return frame_update(q, seg, invl, ks, hasPrev, qprev, qrprev, hasNextOrient, qnext, qrown, b, signs);
 }
 
 // New velocity of a free vertex: dx / h, quadratic drag split by the segment tangent `tg`

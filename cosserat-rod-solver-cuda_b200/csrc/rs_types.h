@@ -181,8 +181,9 @@ struct FrameArgs {
     // tape[(s * 4 + f) * n + u] for f = x, v, lv (previous substep's start velocity), q and the
     // caller-order index u
     float4* tape;
-    // and, when set (no rope-rope contact), every iterate: d^{k+1} at itape[(s * 2I + k) * n + u]
-    // and q^{k+1} at itape[(s * 2I + I + k) * n + u], k = 0 .. I-1
+    // and, when set (no rope-rope contact), every iterate of frame step k = 0 .. I-1: d^{k+1} at
+    // itape[(s * 3I + k) * n + u] (.w: the step's two sign tests, frame_signs_encode), q^{k+1} at
+    // itape[(s * 3I + I + k) * n + u] and the step's blend rotor b at itape[(s * 3I + 2I + k) * n + u]
     float4* itape;
 };
 
@@ -190,7 +191,7 @@ struct FrameArgs {
 // null upstream adjoints read as zero.
 struct AdjArgs {
     const float4* tape;                          // [S][4][n] caller order, written by a frame launch
-    const float4* itape;                         // [S][2I][n] caller order iterates, or null (recompute)
+    const float4* itape;                         // [S][3I][n] caller order iterates, or null (recompute)
     const float *g_pos, *g_vel, *g_lvel, *g_q;   // adjoints of the frame-end state [n,3] x3, [n,4]
     float *o_pos, *o_vel, *o_lvel, *o_q;         // adjoints of the frame-start state
     float *o_ea, *o_ei, *o_mass;                 // [n] adjoints of EA, EI (segment i -> i+1), mass

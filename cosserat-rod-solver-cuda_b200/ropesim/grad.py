@@ -89,11 +89,12 @@ class Frame(torch.autograd.Function):
             p0, v0, p1 = (_check(t, (R, 3), k) for t, k in ((p0, "p0"), (v0, "v0"), (p1, "p1")))
         out = [torch.empty(n, k, device="cuda", dtype=torch.float32) for k in (3, 3, 3, 4)]
         # the frame's substep tape (64 B per vertex-substep) lets the backward skip the replay;
-        # the iterate tape (32 B per vertex-substep-iteration) also skips the recomputation
+        # the iterate tape (48 B per vertex-substep-iteration: d, q and the frame step's blend
+        # rotor b) also skips the recomputation
         ctx.tape = torch.empty(16 * int(substeps) * n, device="cuda", dtype=torch.float32) if tape else None
         ctx.itape = None
         if tape == "iterates":
-            ctx.itape = torch.empty(8 * int(batch.num_itr) * int(substeps) * n, device="cuda", dtype=torch.float32)
+            ctx.itape = torch.empty(12 * int(batch.num_itr) * int(substeps) * n, device="cuda", dtype=torch.float32)
         cur, ext = _streams(batch)
         ext.wait_stream(cur)
         ptrs = [_ptr(t) for t in (pos, vel, lvel, q, ea, ei, mass, p0, v0, p1)] + [_ptr(t) for t in out]
@@ -144,7 +145,7 @@ def frame(batch, st, params, p0, v0, p1, dt, substeps, tape=True):
 
     tape=True keeps the frame's substep tape in device memory until the backward (64 B per
     vertex-substep: 420 MB for 65,536 vertices x 100 substeps), so the backward does not replay
-    the frame; tape="iterates" also keeps every iterate (32 B per vertex-substep-iteration: 1.7 GB
+    the frame; tape="iterates" also keeps every iterate (48 B per vertex-substep-iteration: 2.5 GB
     more at that size and 8 iterations), so the backward does not recompute them either (used on
     the persistent engine without rope-rope contact; elsewhere the backward recomputes);
     tape=False keeps only the frame-start state and replays the frame in the backward."""

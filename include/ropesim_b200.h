@@ -269,11 +269,11 @@ RS_API int rs_batch_backward_async(rs_batch* b, const rs_backward_io* io, float 
  * state and the parameters (NULL = keep), steps with the program rows p0 / v0 / p1 [R,3] (all
  * three NULL: a free frame, as rs_batch_step_free), writes the end state to out_* and, when
  * tape != NULL (16 * substeps * n floats), the substep tape for rs_batch_backward. With itape
- * != NULL as well (8 * num_itr * substeps * n floats: every iterate d^k, q^k of every substep)
- * the backward reads the iterates instead of recomputing them; without rope-rope contact and on
- * the persistent engine only (elsewhere it is ignored and the backward recomputes). *last_h
- * receives the frame's lastH (RS_P_H before the frame). Queued on the handle's stream without
- * host synchronization. */
+ * != NULL as well (12 * num_itr * substeps * n floats: every iterate d^k, q^k of every substep and
+ * each frame step's blend rotor and sign tests) the backward reads the iterates instead of
+ * recomputing them; without rope-rope contact and on the persistent engine only (elsewhere it is
+ * ignored and the backward recomputes). *last_h receives the frame's lastH (RS_P_H before the
+ * frame). Queued on the handle's stream without host synchronization. */
 typedef struct rs_frame_io {
     const float *pos, *vel, *lvel, *q;
     const float *ea, *ei, *mass;
