@@ -38,24 +38,24 @@ __device__ __forceinline__ void surface_contact_bwd(f3 n, float gap, f3 d, float
     const float N = -k * gap;
     const f3 ut = d - n * dot(n, d);
     const float ul = len(ut);
-    const float vt = ul / h;
+    const float w = eps * h, x = ul / w;  // the forward's slip ratio (surface_contact)
     float Nb = dot(n, Fb);
     kb = nHn;
     float kt, mu = 0.f, xr = 0.f;
-    if (vt <= eps) kt = muS * N / (eps * h);
+    if (x <= 1.f) kt = muS * N / w;
     else {
-        xr = vt / eps - 1.f;
+        xr = x - 1.f;
         const float sw = 1.f - fminf(1.f, xr);
         mu = sw * muS + (1.f - sw) * muK;
         kt = mu * N / ul;
     }
     f3 utb = Fb * (-kt);
     const float ktb = -dot(ut, Fb) - (nHn - trHb);
-    if (vt <= eps) Nb += ktb * muS / (eps * h);
+    if (x <= 1.f) Nb += ktb * muS / w;
     else {
         Nb += ktb * mu / ul;
         float ulb = -ktb * mu * N / (ul * ul);
-        if (xr < 1.f) ulb -= ktb * (muS - muK) * N / ul / (eps * h);
+        if (xr < 1.f) ulb -= ktb * (muS - muK) * N / ul / w;
         utb += ut * (ulb / ul);
     }
     db += utb - n * dot(n, utb);
@@ -103,16 +103,17 @@ __device__ __forceinline__ float mesh_contact_bwd(const FrameArgs& a, const floa
         if (!sdf_sample_hess(G, po, phi, gr, hxy, hxz, hyz)) continue;
         const float gap = phi - a.c_radius;
         if (gap >= 0.f) continue;
-        const float gl = len(gr);
-        if (!(gl > 0.f)) continue;
-        const f3 gh = gr / gl;
+        const float g2 = dot(gr, gr);
+        if (!(g2 > 0.f)) continue;
+        const float il = rsqrt_nr(g2);  // the forward's normalisation (sdf_contact_at)
+        const f3 gh = gr * il;
         const f3 nrm = qrot(P.q, gh);
         float gapb, kb;
         f3 nb;
         surface_contact_bwd(nrm, gap, d, kc, h, G.muS, G.muK, a.c_vslip, Fb, e, del, db, gapb, kb, nb);
         kbs += kb;
         const f3 ghb = qrot(qconj(P.q), nb);
-        const f3 grb = (ghb - gh * dot(gh, ghb)) / gl;
+        const f3 grb = (ghb - gh * dot(gh, ghb)) * il;
         const float inv2 = G.invH * G.invH;
         const f3 pob = gr * gapb + mk3(hxy * grb.y + hxz * grb.z, hxy * grb.x + hyz * grb.z, hxz * grb.x + hyz * grb.y) * inv2;
         const f3 wv = qrot(P.q, pob);

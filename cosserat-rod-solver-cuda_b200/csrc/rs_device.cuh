@@ -2,7 +2,9 @@
 // local solve, the surface contact law and the trilinear SDF sample.
 //
 // Every function keeps the operation order of the reference routine it cites so that a
-// single-precision run tracks the reference within rounding (IEEE div/sqrt, no fast math).
+// single-precision run tracks the reference within rounding (IEEE div/sqrt, no fast math), with
+// two exceptions on the contact path: the lattice normal is normalised by rsqrt_nr (about 1 ulp)
+// and the contact law forms its slip ratio with one division instead of two.
 //
 // The engine is compiled with -fmad=false: the compiler fuses nothing, and every fused
 // multiply-add is written out here (fmaf, one rounding). A sum of products is evaluated as
@@ -43,6 +45,11 @@ __device__ __forceinline__ float dot(f3 a, f3 b) { return fmaf(a.z, b.z, fmaf(a.
 __device__ __forceinline__ f3 fma3(f3 a, float s, f3 b) { return f3{fmaf(a.x, s, b.x), fmaf(a.y, s, b.y), fmaf(a.z, s, b.z)}; }
 __device__ __forceinline__ f3 cross(f3 a, f3 b) {
     return f3{fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x))};
+}
+// Reciprocal square root: rsqrtf (within 2 ulp) and one Newton step, within about 1 ulp.
+__device__ __forceinline__ float rsqrt_nr(float x) {
+    const float y = rsqrtf(x);
+    return fmaf(0.5f * y, fmaf(-x * y, y, 1.f), y);
 }
 // c + a x b and c + a.b, accumulated into c by fused multiply-adds
 __device__ __forceinline__ f3 cross_add(f3 a, f3 b, f3 c) {
@@ -149,11 +156,14 @@ __device__ __forceinline__ void surface_contact(f3 n, float gap, f3 d, float k, 
     sym_add_scaled_outer(H, n, k);
     const f3 ut = fma3(n, -dot(n, d), d);
     const float ul = len(ut);
-    const float vt = ul / h;
+    // the slip speed over the regularisation speed, (ul / h) / vslip, as one division by the
+    // slip length vslip h (which the static branch divides by as well)
+    const float w = vslip * h;
+    const float xr = ul / w;
     float kt;
-    if (vt <= vslip) kt = muS * N / (vslip * h);
+    if (xr <= 1.f) kt = muS * N / w;
     else {
-        const float s = 1.f - fminf(1.f, vt / vslip - 1.f);
+        const float s = 1.f - fminf(1.f, xr - 1.f);
         kt = fmaf(s, muS, (1.f - s) * muK) * N / ul;
     }
     f = fma3(ut, -kt, f);
@@ -273,9 +283,12 @@ __device__ __forceinline__ bool sdf_contact_at(const rs::GridDesc& g, const Pose
     if (!sdf_sample(g, po, phi, gr)) return false;
     gap = phi - R;
     if (gap >= 0.f) return false;
-    const float gl = len(gr);
-    if (!(gl > 0.f)) return false;
-    n = qrot(P.q, gr / gl);
+    const float g2 = dot(gr, gr);
+    if (!(g2 > 0.f)) return false;
+    // the unit normal by the reciprocal square root with one Newton step (within about 1 ulp),
+    // not a square root and three divisions: this sits on the critical path of every lane in
+    // contact, which its CTA waits for at the next barrier
+    n = qrot(P.q, gr * rsqrt_nr(g2));
     dRel = d;
     if (moving) dRel = fma3(P.vel + cross(P.om, pos - P.pos), -h, dRel);
     return true;

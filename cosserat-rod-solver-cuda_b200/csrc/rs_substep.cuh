@@ -458,12 +458,6 @@ __device__ __forceinline__ void collision_sectors(const FrameArgs& a, int ncol, 
     if (ncol > 1) { f += fo; f2 += f2o; sym_add(H, Ho); sym_add(H2, H2o); }
 }
 
-// Reciprocal square root: rsqrtf (within 2 ulp) and one Newton step, within about 1 ulp.
-__device__ __forceinline__ float rsqrt_nr(float x) {
-    const float y = rsqrtf(x);
-    return fmaf(0.5f * y, fmaf(-x * y, y, 1.f), y);
-}
-
 // The frame step's unnormalised rotor z = vv b e1 + (|vv| + |b|) b, with lambda = |vv| + |b| and
 // the reciprocal norms 1/|vv|, 1/|b| (0 for a zero vector) the reverse needs. The norms use the
 // hardware reciprocal square root: z is normalised right after, so their rounding (within 2 ulp)
