@@ -386,33 +386,40 @@ def c3_legs(args, world, rank, local, dev, dist, extras):
     value = job_rate(world, nv * S * K, total_ms * 1e-3)
     pos_ok = bool(torch.isfinite(torch.as_tensor(b.positions())).all())
 
-    # ---- end to end: pinned host poses and programs in, positions out, through the public API
-    e2e_value = None
-    if not args.no_e2e:
-        hs = [torch.as_tensor(x[W + K:]).pin_memory() for x in inputs]
-        out = torch.empty((nv, 3), dtype=torch.float32).pin_memory()
-        view = torch.as_tensor(b.positions()).reshape(nv, 3)
-
-        def e2e_frame(i):
-            T = tuple(h[i].to(dev, non_blocking=True) for h in hs)
-            frame(b, W + K + i, T)
-            out.copy_(view)
-
-        for i in range(W):
-            e2e_frame(i)
-        torch.cuda.synchronize()
-        barrier(dist)
-        t0 = time.perf_counter()
-        for i in range(W, W + K):
-            e2e_frame(i)
-        torch.cuda.synchronize()
-        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
-        e2e_value = job_rate(world, nv * S * K, e2e_s)
-    h2d = R * M3 * 7 * 4 + R * 9 * 4
-    d2h = nv * 3 * 4
     layout = list(b.layout())
     del b, Td
     torch.cuda.empty_cache()
+
+    # ---- end to end: pinned host poses and programs in, positions out, through the public API,
+    # on the same frames: a second batch of the same scene takes the W warm-up frames through the
+    # host path too (stepping is deterministic, so it reaches the device-timed run's frame-W state),
+    # then the K timed frames
+    e2e_value = None
+    if not args.no_e2e:
+        b2 = Sc.bench_c3_build(ropesim, scene)
+        hs = [torch.as_tensor(x[:W + K]).pin_memory() for x in inputs]
+        out = torch.empty((nv, 3), dtype=torch.float32).pin_memory()
+        view = torch.as_tensor(b2.positions()).reshape(nv, 3)
+
+        def e2e_frame(f):
+            T = tuple(h[f].to(dev, non_blocking=True) for h in hs)
+            frame(b2, f, T)
+            out.copy_(view)
+
+        for f in range(W):
+            e2e_frame(f)
+        torch.cuda.synchronize()
+        barrier(dist)
+        t0 = time.perf_counter()
+        for f in range(W, W + K):
+            e2e_frame(f)
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+        e2e_value = job_rate(world, nv * S * K, e2e_s)
+        del b2
+        torch.cuda.empty_cache()
+    h2d = R * M3 * 7 * 4 + R * 9 * 4
+    d2h = nv * 3 * 4
 
     res = {"value": value, "ms_per_step": total_ms / K, "kernel_ms_per_frame": float(np.mean(kernel_ms)),
            "R": R, "nv": nv, "layout": layout, "finite": pos_ok, "clocks": sampler.summary(),

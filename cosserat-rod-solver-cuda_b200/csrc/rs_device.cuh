@@ -170,31 +170,48 @@ __device__ __forceinline__ void surface_contact(f3 n, float gap, f3 d, float k, 
     sym_sub_scaled_outer_minus_I(H, n, kt);
 }
 
-// Trilinear phi and its exact gradient at object-frame point p, contact.cuh:57-76.
-__device__ __forceinline__ bool sdf_sample(const rs::GridDesc& g, f3 p, float& phi, f3& grad) {
-    const f3 o = mk3(g.ox, g.oy, g.oz);
-    const f3 u = (p - o) * g.invH;
+// Trilinear phi and its exact gradient at object-frame point p, contact.cuh:57-76, in three parts
+// (the contact test finds the cell once for its block bound and its sample): the cell of p (false
+// outside the lattice and on its upper faces), the cell's eight nodes, the interpolation.
+__device__ __forceinline__ bool sdf_cell(const rs::GridDesc& g, f3 p, int& i, int& j, int& k) {
+    const f3 u = (p - mk3(g.ox, g.oy, g.oz)) * g.invH;
     if (!(u.x >= 0.f && u.y >= 0.f && u.z >= 0.f && u.x < float(g.nx - 1) && u.y < float(g.ny - 1) &&
           u.z < float(g.nz - 1)))
         return false;
-    const int i = (int)u.x, j = (int)u.y, k = (int)u.z;
+    i = (int)u.x; j = (int)u.y; k = (int)u.z;
     if (rs::kChecked && !(i >= 0 && j >= 0 && k >= 0 && i <= g.nx - 2 && j <= g.ny - 2 && k <= g.nz - 2)) {
         check_fail(g.status, rs::CHK_LATTICE);
         return false;
     }
-    const f3 fr = (p - fma3(mk3(float(i), float(j), float(k)), g.h, o)) * g.invH;
-    const float fx = fminf(fmaxf(fr.x, 0.f), 1.f), fy = fminf(fmaxf(fr.y, 0.f), 1.f), fz = fminf(fmaxf(fr.z, 0.f), 1.f);
+    return true;
+}
+struct CellNodes {
+    float c000, c001, c010, c011, c100, c101, c110, c111;
+};
+__device__ __forceinline__ CellNodes sdf_nodes(const rs::GridDesc& g, int i, int j, int k) {
     const int sy = g.nz, sx = g.ny * g.nz;
     const float* c = g.v + (size_t)i * sx + (size_t)j * sy + k;
-    const float c000 = __ldg(c), c001 = __ldg(c + 1), c010 = __ldg(c + sy), c011 = __ldg(c + sy + 1);
-    const float c100 = __ldg(c + sx), c101 = __ldg(c + sx + 1), c110 = __ldg(c + sx + sy), c111 = __ldg(c + sx + sy + 1);
-    const float dx00 = c100 - c000, dx01 = c101 - c001, dx10 = c110 - c010, dx11 = c111 - c011;
-    const float c00 = fmaf(fx, dx00, c000), c01 = fmaf(fx, dx01, c001), c10 = fmaf(fx, dx10, c010), c11 = fmaf(fx, dx11, c011);
+    return CellNodes{__ldg(c), __ldg(c + 1), __ldg(c + sy), __ldg(c + sy + 1),
+                     __ldg(c + sx), __ldg(c + sx + 1), __ldg(c + sx + sy), __ldg(c + sx + sy + 1)};
+}
+__device__ __forceinline__ void sdf_interp(const rs::GridDesc& g, f3 p, int i, int j, int k, const CellNodes& n,
+                                           float& phi, f3& grad) {
+    const f3 o = mk3(g.ox, g.oy, g.oz);
+    const f3 fr = (p - fma3(mk3(float(i), float(j), float(k)), g.h, o)) * g.invH;
+    const float fx = fminf(fmaxf(fr.x, 0.f), 1.f), fy = fminf(fmaxf(fr.y, 0.f), 1.f), fz = fminf(fmaxf(fr.z, 0.f), 1.f);
+    const float dx00 = n.c100 - n.c000, dx01 = n.c101 - n.c001, dx10 = n.c110 - n.c010, dx11 = n.c111 - n.c011;
+    const float c00 = fmaf(fx, dx00, n.c000), c01 = fmaf(fx, dx01, n.c001), c10 = fmaf(fx, dx10, n.c010),
+                c11 = fmaf(fx, dx11, n.c011);
     const float dy0 = c10 - c00, dy1 = c11 - c01;
     const float c0 = fmaf(fy, dy0, c00), c1 = fmaf(fy, dy1, c01);
     phi = fmaf(fz, c1 - c0, c0);
     const float gx0 = fmaf(fy, dx10 - dx00, dx00), gx1 = fmaf(fy, dx11 - dx01, dx01);
     grad = mk3(fmaf(fz, gx1 - gx0, gx0), fmaf(fz, dy1 - dy0, dy0), c1 - c0) * g.invH;
+}
+__device__ __forceinline__ bool sdf_sample(const rs::GridDesc& g, f3 p, float& phi, f3& grad) {
+    int i, j, k;
+    if (!sdf_cell(g, p, i, j, k)) return false;
+    sdf_interp(g, p, i, j, k, sdf_nodes(g, i, j, k), phi, grad);
     return true;
 }
 
@@ -237,20 +254,19 @@ __device__ __forceinline__ void world_box(f3 lo_o, f3 hi_o, f3 pos, float4 q, f3
 
 // Exact early out: the trilinear field inside a lattice block is at least the block's smallest
 // node value, so a block whose bound clears the radius (by more than the rounding of the
-// interpolation, 1e-5) cannot produce gap < 0.
+// interpolation, 1e-5) cannot produce gap < 0. The bound of the block holding cell (i, j, k);
+// false (no bound: the sample decides) when a checked build finds the index out of range.
 // `btab`: the CTA's shared-memory copy of the bound tables (nullptr: read them from L2).
-__device__ __forceinline__ bool sdf_block_clear(const rs::GridDesc& g, const float* btab, f3 p, float R) {
-    const f3 u = (p - mk3(g.ox, g.oy, g.oz)) * g.invH;
-    if (!(u.x >= 0.f && u.y >= 0.f && u.z >= 0.f && u.x < float(g.nx - 1) && u.y < float(g.ny - 1) &&
-          u.z < float(g.nz - 1)))
-        return true;  // outside the lattice: sdf_sample reports no contact either
-    const int bi = (int)u.x / rs::kSdfBlock, bj = (int)u.y / rs::kSdfBlock, bk = (int)u.z / rs::kSdfBlock;
+__device__ __forceinline__ bool sdf_block_bound(const rs::GridDesc& g, const float* btab, int i, int j, int k,
+                                                float& bound) {
+    const int bi = i / rs::kSdfBlock, bj = j / rs::kSdfBlock, bk = k / rs::kSdfBlock;
     const int idx = (bi * g.by + bj) * g.bz + bk;
     if (rs::kChecked && !(bi >= 0 && bj >= 0 && bk >= 0 && bj < g.by && bk < g.bz && idx < g.bcount)) {
         check_fail(g.status, rs::CHK_BLOCK);
-        return false;  // not cleared: the sample (itself checked) decides
+        return false;
     }
-    return (btab ? btab[g.boff + idx] : __ldg(g.bmin + idx)) - R > 1e-5f;
+    bound = btab ? btab[g.boff + idx] : __ldg(g.bmin + idx);
+    return true;
 }
 
 // How far the probe (pos - P.pos) + d of a vertex can move (|d|) before it could touch lattice g
@@ -279,8 +295,11 @@ __device__ __forceinline__ bool sdf_contact_at(const rs::GridDesc& g, const Pose
     float phi;
     f3 gr;
     const f3 po = qrot(qconj(P.q), (pos - P.pos) + d);
-    if (skip && sdf_block_clear(g, btab, po, R)) return false;
-    if (!sdf_sample(g, po, phi, gr)) return false;
+    int i, j, k;
+    if (!sdf_cell(g, po, i, j, k)) return false;  // the cell once, for the block bound and the sample
+    float bound = 0.f;
+    if (skip && sdf_block_bound(g, btab, i, j, k, bound) && bound - R > 1e-5f) return false;
+    sdf_interp(g, po, i, j, k, sdf_nodes(g, i, j, k), phi, gr);
     gap = phi - R;
     if (gap >= 0.f) return false;
     const float g2 = dot(gr, gr);

@@ -181,12 +181,12 @@ __device__ __forceinline__ bool surfaces(const FrameArgs& a, const float4* cache
     if constexpr (SURF == SURF_MESHES) {
     for (uint64_t mm = cand; mm; mm &= mm - 1ull) {
         const int m = __ffsll((long long)mm) - 1;
+        const PoseV P = load_pose(cache + m * kPoseF4);  // loaded with the contact box, not after its test
         if (tbox) {
             const float4 lo = tbox[2 * m], hi = tbox[2 * m + 1];
             const f3 pr = pos + d;
             if (!(pr.x >= lo.x && pr.x <= hi.x && pr.y >= lo.y && pr.y <= hi.y && pr.z >= lo.z && pr.z <= hi.z)) continue;
         }
-        const PoseV P = load_pose(cache + m * kPoseF4);
         f3 n, dRel;
         float gap;
         if (!sdf_contact_at(a.grids[m], P, pos, d, h, a.c_radius, a.sdf_moving != 0, a.sdf_skip != 0, btab, n, gap, dRel))
