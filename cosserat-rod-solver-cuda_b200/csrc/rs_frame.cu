@@ -36,7 +36,8 @@ struct FrameSmem {
     float4 p[BLOCK];      // positions at the substep start
     float4 q[2][BLOCK];   // frame rotors, double buffered across frame steps
     float4 fa[BLOCK];     // segment force on the next vertex (xyz) + H2.xx (= dd without rope contact)
-    float4 fb[BLOCK];     // H2.yy, H2.zz, H2.xy, H2.xz (rope contact only)
+    float4 fb[BLOCK];     // H2.yy, H2.zz, H2.xy, H2.xz (rope contact); without rope contact and
+                          // meshes the displacement iterate of odd substeps (dx holds the even ones)
     float4 qr[BLOCK];     // rest rotation of segment i (vertex i reads slots i-1 and i)
     float4 lv[BLOCK];     // velocity at the previous substep's start (initial-guess extrapolation)
     float fc[BLOCK];      // H2.yz (rope contact only)
@@ -316,6 +317,12 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             if (nsdf > 0 && a.sdf_moving) bin_poses<BLOCK>(a, bin, nsdf, nPose, s, S, h, cache, tbox);
         const float4* mycache = cache + lrope * nsdf * kPoseF4;
         const float4* mytbox = (SURF == SURF_MESHES && a.surf_cull) ? tbox + lrope * nsdf * 2 : nullptr;
+        // Without rope contact and meshes the displacement iterates alternate between two buffers by
+        // substep, so a lane that has finished the substep may write the next one's initial guess
+        // while its neighbour still reads this one's in the last frame step: no barrier ends the
+        // substep (B3 below).
+        constexpr bool kNoB3 = !ROPE && SURF != SURF_MESHES;
+        float4* const sdx = (kNoB3 && (s & 1)) ? sm.fb : sm.dx;
 
         // ---- inertial prediction and initial guess
         f3 dx, y;
@@ -323,7 +330,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
         if (act) {
             sm.lv[t] = f4(v, 0.f);
             sm.p[t] = f4(p, 0.f);
-            sm.dx[t] = f4(dx, 0.f);
+            sdx[t] = f4(dx, 0.f);
             if constexpr (ROPE) sm.pad[t] = a.sdet_radius + len(y);
         }
         __syncthreads();  // B0
@@ -363,7 +370,7 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
             // ---- position step: own terms, exchange the segment's share, local solve
             f3 f, f2;
             sym3 H, H2;
-            const f3 p1dx = xyz(sm.dx[hasNext ? t + 1 : t]);  // any finite value without a next vertex
+            const f3 p1dx = xyz(sdx[hasNext ? t + 1 : t]);  // any finite value without a next vertex
             bool touched;
             if constexpr (kRedo) {
                 position_terms<SURF_NONE>(a, mycache, cand, c, hasNext, p, p1, dx, p1dx, y, q, damp, f, H, f2, H2);
@@ -423,14 +430,14 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                     dx = im != 0.f ? nd : dx;
                 }
             }
-            if (act) sm.dx[t] = f4(dx, 0.f);
+            if (act) sdx[t] = f4(dx, 0.f);
             __syncthreads();  // B2
 
             // ---- frame step over the double-buffered rotors (no barrier needed before it)
             float4 fb = make_float4(0.f, 0.f, 0.f, 0.f);
             float fsig = 0.f;
             if (!(fl & F_FIX_ORIENT) && hasNext) {
-                const f3 seg = (p1 - p) + (xyz(sm.dx[t + 1]) - dx);
+                const f3 seg = (p1 - p) + (xyz(sdx[t + 1]) - dx);
                 q = frame_update(q, seg, c.invl, ks, hasPrev, sm.q[cur][hasPrev ? t - 1 : t], qr_prev,
                                  (fl & F_NEXT_ORIENT) != 0, sm.q[cur][(fl & F_NEXT_ORIENT) ? t + 1 : t], qr_own, fb,
                                  fsig);
@@ -445,7 +452,13 @@ __device__ __forceinline__ void frame_bin(const FrameArgs& a, const Bin bin) {
                 }
             cur ^= 1;
         }
-        __syncthreads();  // B3
+        // B3: rope contact reads other vertices' positions and iterates, and quadratic drag the
+        // previous vertex's rotor, which the next substep's root program may overwrite; without them
+        // every shared slot the rest of the substep and the next one's start write is the lane's own
+        // or double-buffered (iterates by substep, rotors by frame step), and the next substep's
+        // first barrier orders the reads that follow. Planes-only 4096 x 64 frame 2.37 -> 2.33 ms;
+        // the mesh kernel keeps the barrier (20.5 -> 20.9 ms without it, A/B on one B200).
+        if (!kNoB3 || a.drag_quad > 0.f) __syncthreads();  // B3
 
         // ---- velocity, drag, readout (planes, then meshes warp-cooperatively), advection, broad phase
         f3 fv = zero3();
