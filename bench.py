@@ -688,7 +688,8 @@ def c4_legs(args, rollouts_warm=3, rollouts=3, R=1024):
 
         timed(fwd, rollouts_warm)
         ms = timed(fwd, rollouts)
-        out[engine] = {"ms_per_rollout": float(np.mean(ms)), "value": nv * S4 * F * len(ms) / (sum(ms) * 1e-3)}
+        out[engine] = {"ms_per_rollout": float(np.mean(ms)), "value": nv * S4 * F * len(ms) / (sum(ms) * 1e-3),
+                       "bins": list(b.layout())}
         if engine == "persistent":
             par0 = rg.parameters(b)
             grads = {}
