@@ -142,7 +142,7 @@ def _quantiles(d):
     return [float(np.percentile(d, q)) for q in QUANTILES]
 
 
-def _judge(name, gpu, o64, o32, r64, r32, sel, starts):
+def _assess(name, gpu, o64, o32, r64, r32, sel, starts):
     """Deviations per (frame, rope); the assertions of the module docstring; a summary dict."""
     loc = np.concatenate([[0], np.cumsum(np.diff(starts)[sel])])
     g = np.stack([s[0] for s in gpu[1:]])  # GPU positions after each frame
@@ -211,7 +211,7 @@ def test_config2_bench_sample_parity():
 
     o64, r64 = _replay(build, ostep, sel, starts, gpu, "f64")
     o32, r32 = _replay(build, ostep, sel, starts, gpu, "f32")
-    _judge("config2", gpu, o64, o32, r64, r32, sel, starts)
+    _assess("config2", gpu, o64, o32, r64, r32, sel, starts)
 
 
 def test_config3_bench_sample_parity():
@@ -253,4 +253,4 @@ def test_config3_bench_sample_parity():
 
     o64, r64 = _replay(build, ostep, sel, starts, gpu, "f64")
     o32, r32 = _replay(build, ostep, sel, starts, gpu, "f32")
-    _judge("config3", gpu, o64, o32, r64, r32, sel, starts)
+    _assess("config3", gpu, o64, o32, r64, r32, sel, starts)
